@@ -1,0 +1,162 @@
+// Device-side building blocks: exact FP64 arithmetic, warp/block/grid reductions and
+// the sliced-ELL row kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "internal.cuh"
+
+namespace gipb200 {
+
+// GIP's CPU loops round every product and every sum (no FMA contraction); these keep the
+// same IEEE operations on the device.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+
+template <typename T>
+__device__ __forceinline__ T ld_stream(const T* p) {
+  return __ldcs(p);
+}
+
+struct SumOp {
+  __device__ static double identity() { return 0.0; }
+  __device__ static double apply(double a, double b) { return dadd(a, b); }
+};
+struct MaxOp {  // of non-negative values (infinity norm)
+  __device__ static double identity() { return 0.0; }
+  __device__ static double apply(double a, double b) { return (b > a) ? b : a; }
+};
+struct MinOp {
+  __device__ static double identity() { return 1e20; }
+  __device__ static double apply(double a, double b) { return (b < a) ? b : a; }
+};
+
+template <class Op>
+__device__ __forceinline__ double warp_reduce(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = Op::apply(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Reduces K values per thread over the grid.  Every block writes its K partials; the
+// last block to finish reduces them in block order and calls fin(total[]) on thread 0.
+// Returns true in the block that ran fin (all its threads).
+template <class Op, int K, class Fin>
+__device__ __forceinline__ bool grid_reduce(const double (&v)[K], ReduceScratch rs, Fin fin) {
+  __shared__ double sh[K][32];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double w = warp_reduce<Op>(v[k]);
+    if (lane == 0) sh[k][warp] = w;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double w = (lane < nwarps) ? sh[k][lane] : Op::identity();
+      w = warp_reduce<Op>(w);
+      if (lane == 0) rs.partials[k * kMaxReduceBlocks + blockIdx.x] = w;
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned t = atomicAdd(rs.ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  double tot[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double a = Op::identity();
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+      a = Op::apply(a, __ldcg(&rs.partials[k * kMaxReduceBlocks + b]));
+    a = warp_reduce<Op>(a);
+    if (lane == 0) sh[k][warp] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double a = Op::identity();
+      for (int w = 0; w < nwarps; ++w) a = Op::apply(a, sh[k][w]);
+      tot[k] = a;
+    }
+    fin(tot);
+    *rs.ticket = 0u;
+    __threadfence();
+  }
+  return true;
+}
+
+// One row of a SELL-32 matrix, summed slot by slot in CSR order with GIP's rounding.
+// `any` reports whether the row has at least one stored nonzero.
+template <typename V, typename X, int CH = 8>
+__device__ __forceinline__ void sell_row_f64(const SellView<V>& A, const X* __restrict__ x,
+                                             int s, int lane, double& sum, bool& any) {
+  const long long base = A.sptr[s];
+  const int len = (int)((A.sptr[s + 1] - base) >> 5);
+  const int* cp = A.col + base + lane;
+  const V* vp = A.val + base + lane;
+  for (int j0 = 0; j0 < len; j0 += CH) {
+    int c[CH];
+    V v[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+      if (j0 + t < len) {
+        c[t] = ld_stream(cp + (size_t)(j0 + t) * 32);
+        v[t] = ld_stream(vp + (size_t)(j0 + t) * 32);
+      } else {
+        c[t] = -1;
+        v[t] = V(0);
+      }
+    }
+    double xv[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) xv[t] = (c[t] >= 0) ? (double)__ldg(x + c[t]) : 0.0;
+#pragma unroll
+    for (int t = 0; t < CH; ++t)
+      if (c[t] >= 0) {
+        sum = dadd(sum, dmul(xv[t], (double)v[t]));
+        any = true;
+      }
+  }
+}
+
+// FP32 row: FP32 storage and FP32 accumulation (the inner solver of the mixed form).
+template <int CH = 8>
+__device__ __forceinline__ float sell_row_f32(const SellView<float>& A, const float* __restrict__ x,
+                                              int s, int lane) {
+  const long long base = A.sptr[s];
+  const int len = (int)((A.sptr[s + 1] - base) >> 5);
+  const int* cp = A.col + base + lane;
+  const float* vp = A.val + base + lane;
+  float sum = 0.f;
+  for (int j0 = 0; j0 < len; j0 += CH) {
+    int c[CH];
+    float v[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+      if (j0 + t < len) {
+        c[t] = ld_stream(cp + (size_t)(j0 + t) * 32);
+        v[t] = ld_stream(vp + (size_t)(j0 + t) * 32);
+      } else {
+        c[t] = -1;
+        v[t] = 0.f;
+      }
+    }
+    float xv[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) xv[t] = (c[t] >= 0) ? __ldg(x + c[t]) : 0.f;
+#pragma unroll
+    for (int t = 0; t < CH; ++t) sum = fmaf(xv[t], v[t], sum);
+  }
+  return sum;
+}
+
+}  // namespace gipb200

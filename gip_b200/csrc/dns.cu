@@ -1,0 +1,692 @@
+// Device-resident fractional-step timestep: GIP_DNS::integrate (src/Algorithms/GIP_DNS.h:
+// 99-113) with its five phases fused into a handful of kernels, dt/sigma/time and the
+// per-step history kept on the device, and each step capturable in one CUDA graph.
+//
+// Every output element is produced with the IEEE operations and the order of GIP's CPU
+// code (GIP_DNS.h:309-414 over GIP_MatrixMulticore / GIP_VectorMulticore), including
+// GIP's rule that an empty CSR row leaves its output untouched; only the reductions of
+// the PCG dot products are ordered differently.
+#include <math.h>
+
+#include <algorithm>
+#include <string>
+
+#include "device.cuh"
+#include "pcg.cuh"
+
+namespace gipb200 {
+
+struct DnsScalars {
+  double dt, sigma, time;
+  int step;
+  int started;
+};
+
+struct DnsHistory {
+  double* time;
+  double* dt;
+  double* massr;
+  int* iters;
+  double* rr;
+  int capacity;
+};
+
+// ------------------------------------------------------------------ row helpers
+// D and C share D's sparsity (GIP loads C from D's file, GIP_DNS.h:150-151): one pass
+// over the slots yields D u, D v, D w, C u, C v, C w, each summed in CSR order.
+__device__ __forceinline__ void dc_row(const SellView<double>& D, const double* __restrict__ cval,
+                                       const double* __restrict__ u, const double* __restrict__ v,
+                                       const double* __restrict__ w, int s, int lane,
+                                       double (&sd)[3], double (&sc)[3], bool& any) {
+  const long long base = D.sptr[s];
+  const int len = (int)((D.sptr[s + 1] - base) >> 5);
+  for (int j = 0; j < len; ++j) {
+    const long long k = base + 32LL * j + lane;
+    const int c = ld_stream(D.col + k);
+    if (c < 0) continue;
+    const double dv = ld_stream(D.val + k);
+    const double cv = ld_stream(cval + k);
+    const double xu = __ldg(u + c), xv = __ldg(v + c), xw = __ldg(w + c);
+    sd[0] = dadd(sd[0], dmul(xu, dv));
+    sd[1] = dadd(sd[1], dmul(xv, dv));
+    sd[2] = dadd(sd[2], dmul(xw, dv));
+    sc[0] = dadd(sc[0], dmul(xu, cv));
+    sc[1] = dadd(sc[1], dmul(xv, cv));
+    sc[2] = dadd(sc[2], dmul(xw, cv));
+    any = true;
+  }
+}
+
+// y = alpha*sum + beta*y as GIP_MatrixMulticore::spmv(x,b,alpha,beta) (:85-103)
+__device__ __forceinline__ double axpby_row(double alpha, double sum, double beta, double y) {
+  return dadd(dmul(alpha, sum), dmul(beta, y));
+}
+
+// ------------------------------------------------------------------ PredictorVelocity
+// ax = D u; ax = -C u + ax  (and v, w)   -- GIP_DNS.h:313-318
+__global__ void __launch_bounds__(256) k_dns_convdiff(SellView<double> D,
+                                                      const double* __restrict__ cval,
+                                                      const double* __restrict__ u,
+                                                      const double* __restrict__ v,
+                                                      const double* __restrict__ w,
+                                                      double* __restrict__ ax, double* __restrict__ ay,
+                                                      double* __restrict__ az) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int s = gw; s < D.nslices; s += nw) {
+    double sd[3] = {0.0, 0.0, 0.0}, sc[3] = {0.0, 0.0, 0.0};
+    bool any = false;
+    dc_row(D, cval, u, v, w, s, lane, sd, sc, any);
+    const int i = s * 32 + lane;
+    if (i < D.nrows && any) {
+      ax[i] = axpby_row(-1.0, sc[0], 1.0, sd[0]);
+      ay[i] = axpby_row(-1.0, sc[1], 1.0, sd[1]);
+      az[i] = axpby_row(-1.0, sc[2], 1.0, sd[2]);
+    }
+  }
+}
+
+// u += 1.5dt ax; u += -0.5dt ax0; ax0 = ax (and v, w) over the inner cells -- :320-336
+__global__ void __launch_bounds__(256) k_dns_ab2(int n, double* __restrict__ u, double* __restrict__ v,
+                                                 double* __restrict__ w, const double* __restrict__ ax,
+                                                 const double* __restrict__ ay,
+                                                 const double* __restrict__ az,
+                                                 double* __restrict__ ax0, double* __restrict__ ay0,
+                                                 double* __restrict__ az0, const DnsScalars* S) {
+  const double dt = S->dt;
+  const double a1 = dmul(1.5, dt);
+  const double a2 = dmul(-0.5, dt);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double x = ax[i], y = ay[i], z = az[i];
+    u[i] = dadd(dadd(u[i], dmul(a1, x)), dmul(a2, ax0[i]));
+    v[i] = dadd(dadd(v[i], dmul(a1, y)), dmul(a2, ay0[i]));
+    w[i] = dadd(dadd(w[i], dmul(a1, z)), dmul(a2, az0[i]));
+    ax0[i] = x;
+    ay0[i] = y;
+    az0[i] = z;
+  }
+}
+
+// ------------------------------------------------------------------ PoissonEquation rhs
+// rhs = Mx u; rhs = My v + rhs; rhs = sigma Mz w + sigma rhs   -- GIP_DNS.h:343-345
+__global__ void __launch_bounds__(256) k_dns_rhs(SellView<double> Mx, SellView<double> My,
+                                                 SellView<double> Mz, const double* __restrict__ u,
+                                                 const double* __restrict__ v,
+                                                 const double* __restrict__ w,
+                                                 double* __restrict__ rhs, const DnsScalars* S) {
+  const double sigma = S->sigma;
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int ns = max(Mx.nslices, max(My.nslices, Mz.nslices));
+  for (int s = gw; s < ns; s += nw) {
+    const int i = s * 32 + lane;
+    double sx = 0, sy = 0, sz = 0;
+    bool ax = false, ay = false, az = false;
+    if (s < Mx.nslices) sell_row_f64(Mx, u, s, lane, sx, ax);
+    if (s < My.nslices) sell_row_f64(My, v, s, lane, sy, ay);
+    if (s < Mz.nslices) sell_row_f64(Mz, w, s, lane, sz, az);
+    ax = ax && i < Mx.nrows;
+    ay = ay && i < My.nrows;
+    az = az && i < Mz.nrows;
+    if (ax || ay || az) {
+      double r = rhs[i];
+      if (ax) r = sx;
+      if (ay) r = axpby_row(1.0, sy, 1.0, r);
+      if (az) r = axpby_row(sigma, sz, sigma, r);
+      rhs[i] = r;
+    }
+  }
+}
+
+// p0 = p (inner); p = p0 (owned)   -- GIP_DNS.h:350-351
+__global__ void k_dns_pcopy(int n_inner, int n_owned, double* __restrict__ p, double* __restrict__ p0) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_owned; i += gridDim.x * blockDim.x) {
+    if (i < n_inner)
+      p0[i] = p[i];
+    else
+      p[i] = p0[i];
+  }
+}
+
+// ------------------------------------------------------------------ VelocityCorrection
+// gp = G p (x,y,z); u -= gp/(rho sigma) over the inner cells   -- GIP_DNS.h:359-370
+__global__ void __launch_bounds__(256) k_dns_gradcorr(SellView<double> Gx, SellView<double> Gy,
+                                                      SellView<double> Gz, const double* __restrict__ p,
+                                                      double* __restrict__ gpx, double* __restrict__ gpy,
+                                                      double* __restrict__ gpz, double* __restrict__ u,
+                                                      double* __restrict__ v, double* __restrict__ w,
+                                                      int n_inner, double rho, const DnsScalars* S) {
+  const double fact = ddiv(-1.0, dmul(rho, S->sigma));
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int ns = max(max(Gx.nslices, Gy.nslices), max(Gz.nslices, (n_inner + 31) / 32));
+  for (int s = gw; s < ns; s += nw) {
+    const int i = s * 32 + lane;
+    double sx = 0, sy = 0, sz = 0;
+    bool ax = false, ay = false, az = false;
+    if (s < Gx.nslices) sell_row_f64(Gx, p, s, lane, sx, ax);
+    if (s < Gy.nslices) sell_row_f64(Gy, p, s, lane, sy, ay);
+    if (s < Gz.nslices) sell_row_f64(Gz, p, s, lane, sz, az);
+    if (ax && i < Gx.nrows) gpx[i] = sx;
+    if (ay && i < Gy.nrows) gpy[i] = sy;
+    if (az && i < Gz.nrows) gpz[i] = sz;
+    if (i < n_inner) {
+      const double gx = (ax && i < Gx.nrows) ? sx : gpx[i];
+      const double gy = (ay && i < Gy.nrows) ? sy : gpy[i];
+      const double gz = (az && i < Gz.nrows) ? sz : gpz[i];
+      u[i] = dadd(u[i], dmul(fact, gx));
+      v[i] = dadd(v[i], dmul(fact, gy));
+      w[i] = dadd(w[i], dmul(fact, gz));
+    }
+  }
+}
+
+// ------------------------------------------------------------------ MassFluxes
+// mf = -dt SO p + dt SF gp + rho SF u, as seven ordered SpMV updates -- GIP_DNS.h:381-390
+__global__ void __launch_bounds__(256) k_dns_massflux(
+    SellView<double> SO, SellView<double> SFx, SellView<double> SFy, SellView<double> SFz,
+    const double* __restrict__ p, const double* __restrict__ gpx, const double* __restrict__ gpy,
+    const double* __restrict__ gpz, const double* __restrict__ u, const double* __restrict__ v,
+    const double* __restrict__ w, double* __restrict__ mf, double rho, const DnsScalars* S) {
+  const double sigma = S->sigma;
+  const double fact1 = ddiv(-1.0, sigma);
+  const double fact2 = ddiv(1.0, sigma);
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int ns = max(max(SO.nslices, SFx.nslices), max(SFy.nslices, SFz.nslices));
+  for (int s = gw; s < ns; s += nw) {
+    const int f = s * 32 + lane;
+    double so = 0, gx = 0, gy = 0, gz = 0, ux = 0, uy = 0, uz = 0;
+    bool a0 = false, ax = false, ay = false, az = false, bx = false, by = false, bz = false;
+    if (s < SO.nslices) sell_row_f64(SO, p, s, lane, so, a0);
+    if (s < SFx.nslices) {
+      sell_row_f64(SFx, gpx, s, lane, gx, ax);
+      sell_row_f64(SFx, u, s, lane, ux, bx);
+    }
+    if (s < SFy.nslices) {
+      sell_row_f64(SFy, gpy, s, lane, gy, ay);
+      sell_row_f64(SFy, v, s, lane, uy, by);
+    }
+    if (s < SFz.nslices) {
+      sell_row_f64(SFz, gpz, s, lane, gz, az);
+      sell_row_f64(SFz, w, s, lane, uz, bz);
+    }
+    a0 = a0 && f < SO.nrows;
+    ax = ax && f < SFx.nrows;
+    ay = ay && f < SFy.nrows;
+    az = az && f < SFz.nrows;
+    if (a0 || ax || ay || az) {
+      double m = mf[f];
+      if (a0) m = axpby_row(fact1, so, 0.0, m);
+      if (ax) m = axpby_row(fact2, gx, 1.0, m);
+      if (ay) m = axpby_row(fact2, gy, 1.0, m);
+      if (az) m = axpby_row(fact2, gz, 1.0, m);
+      if (ax) m = axpby_row(rho, ux, 1.0, m);
+      if (ay) m = axpby_row(rho, uy, 1.0, m);
+      if (az) m = axpby_row(rho, uz, 1.0, m);
+      mf[f] = m;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ CFLCondition
+struct MassrFinish {
+  const DnsScalars* S;
+  DnsHistory H;
+  __device__ void operator()(const double* t) const {
+    const int k = S->step;
+    if (k < H.capacity) H.massr[k] = t[0];
+  }
+};
+
+// temp = Mres mf; massr = max |temp| over the inner cells   -- GIP_DNS.h:399-400
+__global__ void __launch_bounds__(256) k_dns_massr(SellView<double> Mres, const double* __restrict__ mf,
+                                                   double* __restrict__ temp, int n_inner,
+                                                   const DnsScalars* S, DnsHistory H,
+                                                   ReduceScratch rs) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int ns = max(Mres.nslices, (n_inner + 31) / 32);
+  double acc[1] = {0.0};
+  for (int s = gw; s < ns; s += nw) {
+    const int i = s * 32 + lane;
+    double sum = 0;
+    bool any = false;
+    if (s < Mres.nslices) sell_row_f64(Mres, mf, s, lane, sum, any);
+    any = any && i < Mres.nrows;
+    if (any) temp[i] = sum;
+    if (i < n_inner) {
+      const double a = fabs(any ? sum : temp[i]);
+      if (a > acc[0]) acc[0] = a;
+    }
+  }
+  grid_reduce<MaxOp, 1>(acc, rs, MassrFinish{S, H});
+}
+
+__device__ __forceinline__ double cfl_candidate(double ut, double vt, double wt, double dx,
+                                                double gamma, double rho, double dt) {
+  const double convCoef = 0.25;
+  double normit = (fabs(ut) > fabs(vt)) ? fabs(ut) : fabs(vt);
+  if (normit < fabs(wt)) normit = fabs(wt);
+  if (!(ddiv(dx, normit) < 1e-17)) {
+    const double c = ddiv(dmul(convCoef, dx), normit);
+    if (dt > c) dt = c;
+  }
+  if (!(ddiv(dmul(dmul(dx, dx), rho), gamma) < 1e-17)) {
+    const double c = ddiv(dmul(dmul(dmul(0.2, dx), dx), rho), gamma);
+    if (dt > c) dt = c;
+  }
+  return dt;
+}
+
+struct CflStepFinish {
+  DnsScalars* S;
+  DnsHistory H;
+  const PcgScalars* P;
+  int mode;  // 0: initial dt only (GIP_DNS.h:102-103); 1: end of a step (:402-408)
+  int pcg_mixed;
+  __device__ void operator()(const double* t) const {
+    const double fin = t[0];
+    const double dtn = (dmul(0.8, fin) > 1e-1) ? 1e-1 : dmul(0.8, fin);
+    if (mode == 1) {
+      const int k = S->step;
+      const double tnew = dadd(S->time, S->dt);
+      S->time = tnew;
+      if (k < H.capacity) {
+        H.time[k] = tnew;
+        H.dt[k] = S->dt;
+        H.iters[k] = pcg_mixed ? P->total_inner : P->iter;
+        H.rr[k] = P->rr;
+      }
+      S->step = k + 1;
+    }
+    S->dt = dtn;
+    S->sigma = ddiv(1.0, dtn);
+    S->started = 1;
+  }
+};
+
+__global__ void __launch_bounds__(256) k_dns_cfl(int n, const double* __restrict__ u,
+                                                 const double* __restrict__ v,
+                                                 const double* __restrict__ w,
+                                                 const double* __restrict__ dxs, double gamma,
+                                                 double rho, DnsScalars* S, DnsHistory H,
+                                                 const PcgScalars* P, int mode, int pcg_mixed,
+                                                 ReduceScratch rs) {
+  double acc[1] = {1e20};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    acc[0] = cfl_candidate(u[i], v[i], w[i], dxs[i], gamma, rho, acc[0]);
+  grid_reduce<MinOp, 1>(acc, rs, CflStepFinish{S, H, P, mode, pcg_mixed});
+}
+
+// ------------------------------------------------------------------ engine
+struct Dns {
+  int N = 0, NO = 0, NF = 0;
+  gipb200_dns_params prm{};
+  Sell D, Ec, L, Lb, Mx, My, Mz, Mres, Gx, Gy, Gz, SFx, SFy, SFz, SO;
+  DevBuf<double> cval;
+  DevBuf<double> u, v, w, dxs, ax, ay, az, ax0, ay0, az0, rhs, p, p0, gpx, gpy, gpz, temp, mf;
+  Pcg pcg;
+  DevBuf<DnsScalars> sc;
+  DevBuf<double> h_time, h_dt, h_massr, h_rr;
+  DevBuf<int> h_iters;
+  int capacity = 0;
+  DevBuf<double> partials;
+  DevBuf<unsigned> ticket;
+  ReduceScratch rs{};
+  int steps_enqueued = 0;
+  bool started = false;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int blocks_cells = 1, blocks_faces = 1, blocks_owned = 1, blocks_vec = 1;
+  long long launches = 0;        // kernels launched (graph launches count their kernels)
+  long long graph_kernels = 0;   // kernels in the captured step graph
+
+  ~Dns() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+  }
+  DnsHistory history() const {
+    return {h_time.p, h_dt.p, h_massr.p, h_iters.p, h_rr.p, capacity};
+  }
+  int grow_history(int need, cudaStream_t s);
+  int enqueue_step(cudaStream_t s, bool host_sync);
+  int enqueue_initial_dt(cudaStream_t s);
+  double* field(const std::string& name, int* n);
+};
+
+int Dns::grow_history(int need, cudaStream_t s) {
+  if (need <= capacity) return GIPB200_OK;
+  int cap = std::max(need, std::max(1024, capacity * 2));
+  DevBuf<double> t, d, m, r;
+  DevBuf<int> it;
+  GIPB_TRY(t.alloc(cap));
+  GIPB_TRY(d.alloc(cap));
+  GIPB_TRY(m.alloc(cap));
+  GIPB_TRY(r.alloc(cap));
+  GIPB_TRY(it.alloc(cap));
+  if (capacity > 0) {
+    GIPB_CUDA(cudaMemcpyAsync(t.p, h_time.p, capacity * 8, cudaMemcpyDeviceToDevice, s));
+    GIPB_CUDA(cudaMemcpyAsync(d.p, h_dt.p, capacity * 8, cudaMemcpyDeviceToDevice, s));
+    GIPB_CUDA(cudaMemcpyAsync(m.p, h_massr.p, capacity * 8, cudaMemcpyDeviceToDevice, s));
+    GIPB_CUDA(cudaMemcpyAsync(r.p, h_rr.p, capacity * 8, cudaMemcpyDeviceToDevice, s));
+    GIPB_CUDA(cudaMemcpyAsync(it.p, h_iters.p, capacity * 4, cudaMemcpyDeviceToDevice, s));
+    GIPB_CUDA(cudaStreamSynchronize(s));
+  }
+  std::swap(h_time.p, t.p);
+  std::swap(h_dt.p, d.p);
+  std::swap(h_massr.p, m.p);
+  std::swap(h_rr.p, r.p);
+  std::swap(h_iters.p, it.p);
+  h_time.n = h_dt.n = h_massr.n = h_rr.n = h_iters.n = cap;
+  t.n = d.n = m.n = r.n = it.n = capacity;
+  capacity = cap;
+  // a captured graph refers to the old history arrays
+  if (exec) {
+    cudaGraphExecDestroy(exec);
+    exec = nullptr;
+  }
+  if (graph) {
+    cudaGraphDestroy(graph);
+    graph = nullptr;
+  }
+  return GIPB200_OK;
+}
+
+int Dns::enqueue_initial_dt(cudaStream_t s) {
+  k_dns_cfl<<<blocks_vec, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p,
+                                        history(), pcg.sc.p, 0, 0, rs);
+  GIPB_LAUNCH_CHECK();
+  launches += 1;
+  return GIPB200_OK;
+}
+
+int Dns::enqueue_step(cudaStream_t s, bool host_sync) {
+  const DnsHistory H = history();
+  const long long pcg_before = pcg.launches;
+  // PredictorVelocity: C's values from the face fluxes, then D/C products and AB2
+  GIPB_TRY(launch_csr_spmv(Ec.nrows, Ec.rowptr.p, Ec.csr_col.p, Ec.csr_val.p, mf.p, cval.p, D.pos.p,
+                           0.0, 0.0, 0, s));
+  k_dns_convdiff<<<blocks_cells, 256, 0, s>>>(D.view(), cval.p, u.p, v.p, w.p, ax.p, ay.p, az.p);
+  k_dns_ab2<<<blocks_vec, 256, 0, s>>>(N, u.p, v.p, w.p, ax.p, ay.p, az.p, ax0.p, ay0.p, az0.p, sc.p);
+  // PoissonEquation
+  k_dns_rhs<<<blocks_cells, 256, 0, s>>>(Mx.view(), My.view(), Mz.view(), u.p, v.p, w.p, rhs.p, sc.p);
+  GIPB_LAUNCH_CHECK();
+  GIPB_TRY(pcg.enqueue(rhs.p, p.p, p0.p, s, host_sync));
+  k_dns_pcopy<<<blocks_owned, 256, 0, s>>>(N, NO, p.p, p0.p);
+  GIPB_LAUNCH_CHECK();
+  GIPB_TRY(launch_sell_spmv(Lb, Lb.val.p, p0.p, p.p, 1.0, 1.0, 1, s));
+  // VelocityCorrection
+  k_dns_gradcorr<<<blocks_owned, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p, gpx.p, gpy.p,
+                                               gpz.p, u.p, v.p, w.p, N, prm.rho, sc.p);
+  // MassFluxes
+  k_dns_massflux<<<blocks_faces, 256, 0, s>>>(SO.view(), SFx.view(), SFy.view(), SFz.view(), p.p,
+                                               gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p, prm.rho,
+                                               sc.p);
+  // CFLCondition
+  k_dns_massr<<<blocks_cells, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
+  k_dns_cfl<<<blocks_vec, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p, H,
+                                        pcg.sc.p, 1, prm.pcg.mode == GIPB200_PCG_MIXED, rs);
+  GIPB_LAUNCH_CHECK();
+  launches += 10 + (pcg.launches - pcg_before);
+  return GIPB200_OK;
+}
+
+double* Dns::field(const std::string& name, int* n) {
+  struct E {
+    const char* nm;
+    DevBuf<double>* b;
+    int sz;
+  } tab[] = {{"u", &u, NO},     {"v", &v, NO},     {"w", &w, NO},     {"dxs", &dxs, NO},
+             {"ax", &ax, NO},   {"ay", &ay, NO},   {"az", &az, NO},   {"ax0", &ax0, NO},
+             {"ay0", &ay0, NO}, {"az0", &az0, NO}, {"rhs", &rhs, NO}, {"p", &p, NO},
+             {"p0", &p0, NO},   {"gpx", &gpx, NO}, {"gpy", &gpy, NO}, {"gpz", &gpz, NO},
+             {"temp", &temp, NO}, {"mf", &mf, NF}};
+  for (auto& e : tab)
+    if (name == e.nm) {
+      *n = e.sz;
+      return e.b->p;
+    }
+  return nullptr;
+}
+
+static int check_op(const gipb200_host_csr& m, const char* name, int rows_max, int col_bound) {
+  if (m.nrows > rows_max)
+    return fail(GIPB200_ERR_ARG, "%s: %d rows exceed %d", name, m.nrows, rows_max);
+  return validate_csr(m.nrows, m.ncols, m.nnz, m.rowptr, m.col, col_bound, name);
+}
+
+static int build_op(Sell* S, const gipb200_host_csr& m) {
+  return sell_build(S, m.nrows, m.ncols, m.nnz, m.rowptr, m.col, m.val, 0);
+}
+
+}  // namespace gipb200
+
+using namespace gipb200;
+
+struct gipb200_dns_s {
+  gipb200::Dns E;
+};
+
+extern "C" {
+
+int gipb200_dns_create(const gipb200_dns_ops* ops, const double* h_u, const double* h_v,
+                       const double* h_w, const double* h_dxs, const gipb200_dns_params* prm,
+                       gipb200_dns* out) {
+  if (!ops || !prm || !out || !h_u || !h_v || !h_w || !h_dxs)
+    return fail(GIPB200_ERR_ARG, "null argument");
+  *out = nullptr;
+  const int N = ops->n_inner, NO = ops->n_owned, NF = ops->n_faces;
+  if (N <= 0 || NO < N || NF < 0) return fail(GIPB200_ERR_ARG, "bad topology sizes");
+  // row/column spaces of GIP_DNS's operators (GIP_DNS.h:143-238)
+  GIPB_TRY(check_op(ops->D, "D", N, NO));
+  GIPB_TRY(check_op(ops->L, "L", N, NO));
+  GIPB_TRY(check_op(ops->Lb, "Lb", NO, NO));
+  GIPB_TRY(check_op(ops->Mx, "Mx", N, NO));
+  GIPB_TRY(check_op(ops->My, "My", N, NO));
+  GIPB_TRY(check_op(ops->Mz, "Mz", N, NO));
+  GIPB_TRY(check_op(ops->Mres, "Mres", N, NF));
+  GIPB_TRY(check_op(ops->Gx, "Gx", NO, NO));
+  GIPB_TRY(check_op(ops->Gy, "Gy", NO, NO));
+  GIPB_TRY(check_op(ops->Gz, "Gz", NO, NO));
+  GIPB_TRY(check_op(ops->SFx, "SFx", NF, NO));
+  GIPB_TRY(check_op(ops->SFy, "SFy", NF, NO));
+  GIPB_TRY(check_op(ops->SFz, "SFz", NF, NO));
+  GIPB_TRY(check_op(ops->SO, "SO", NF, NO));
+  GIPB_TRY(check_op(ops->Ec, "Ec", ops->D.nnz, NF));
+  if (ops->Ec.nrows != ops->D.nnz)
+    return fail(GIPB200_ERR_ARG, "Ec has %d rows, D has %d nonzeros", ops->Ec.nrows, ops->D.nnz);
+  if (prm->pcg.mode < 0 || prm->pcg.mode > 2) return fail(GIPB200_ERR_ARG, "bad PCG mode");
+
+  gipb200_dns D = new (std::nothrow) gipb200_dns_s();
+  if (!D) return fail(GIPB200_ERR_NOMEM, "host allocation failed");
+  Dns& E = D->E;
+  int st = [&]() -> int {
+    E.N = N;
+    E.NO = NO;
+    E.NF = NF;
+    E.prm = *prm;
+    GIPB_TRY(build_op(&E.D, ops->D));
+    GIPB_TRY(build_op(&E.Ec, ops->Ec));
+    GIPB_TRY(build_op(&E.L, ops->L));
+    GIPB_TRY(build_op(&E.Lb, ops->Lb));
+    GIPB_TRY(build_op(&E.Mx, ops->Mx));
+    GIPB_TRY(build_op(&E.My, ops->My));
+    GIPB_TRY(build_op(&E.Mz, ops->Mz));
+    GIPB_TRY(build_op(&E.Mres, ops->Mres));
+    GIPB_TRY(build_op(&E.Gx, ops->Gx));
+    GIPB_TRY(build_op(&E.Gy, ops->Gy));
+    GIPB_TRY(build_op(&E.Gz, ops->Gz));
+    GIPB_TRY(build_op(&E.SFx, ops->SFx));
+    GIPB_TRY(build_op(&E.SFy, ops->SFy));
+    GIPB_TRY(build_op(&E.SFz, ops->SFz));
+    GIPB_TRY(build_op(&E.SO, ops->SO));
+    // C starts with D's values (C.postConstruct reads the D file, GIP_DNS.h:151)
+    GIPB_TRY(E.cval.alloc((size_t)std::max<long long>(E.D.nslots, 1)));
+    GIPB_CUDA(cudaMemcpy(E.cval.p, E.D.val.p, E.cval.n * 8, cudaMemcpyDeviceToDevice));
+    DevBuf<double>* cells[] = {&E.u, &E.v, &E.w, &E.dxs, &E.ax, &E.ay, &E.az, &E.ax0, &E.ay0,
+                               &E.az0, &E.rhs, &E.p, &E.p0, &E.gpx, &E.gpy, &E.gpz, &E.temp};
+    for (auto* b : cells) {
+      GIPB_TRY(b->alloc(NO));
+      GIPB_TRY(b->zero());
+    }
+    GIPB_TRY(E.mf.alloc(std::max(NF, 1)));
+    GIPB_TRY(E.mf.zero());
+    GIPB_CUDA(cudaMemcpy(E.u.p, h_u, (size_t)NO * 8, cudaMemcpyHostToDevice));
+    GIPB_CUDA(cudaMemcpy(E.v.p, h_v, (size_t)NO * 8, cudaMemcpyHostToDevice));
+    GIPB_CUDA(cudaMemcpy(E.w.p, h_w, (size_t)NO * 8, cudaMemcpyHostToDevice));
+    GIPB_CUDA(cudaMemcpy(E.dxs.p, h_dxs, (size_t)NO * 8, cudaMemcpyHostToDevice));
+    GIPB_TRY(E.pcg.init(&E.L, NO, prm->pcg, 0));
+    GIPB_TRY(E.sc.alloc(1));
+    GIPB_TRY(E.sc.zero());
+    GIPB_TRY(reduce_scratch_alloc(&E.partials, &E.ticket, &E.rs));
+    GIPB_TRY(E.grow_history(1024, 0));
+    GIPB_TRY(grid_blocks(256, std::max(N, NO), 1, kMaxReduceBlocks, &E.blocks_cells));
+    GIPB_TRY(grid_blocks(256, std::max(NF, 1), 1, kMaxReduceBlocks, &E.blocks_faces));
+    GIPB_TRY(grid_blocks(256, NO, 1, kMaxReduceBlocks, &E.blocks_owned));
+    GIPB_TRY(grid_blocks(256, N, 4, kMaxReduceBlocks, &E.blocks_vec));
+    GIPB_CUDA(cudaStreamCreateWithFlags(&E.cap_stream, cudaStreamNonBlocking));
+    GIPB_CUDA(cudaDeviceSynchronize());
+    return GIPB200_OK;
+  }();
+  if (st != GIPB200_OK) {
+    delete D;
+    return st;
+  }
+  *out = D;
+  return GIPB200_OK;
+}
+
+int gipb200_dns_destroy(gipb200_dns D) {
+  delete D;
+  return GIPB200_OK;
+}
+
+int gipb200_dns_advance(gipb200_dns Dh, int nsteps, void* stream) {
+  if (!Dh || nsteps < 0) return fail(GIPB200_ERR_ARG, "bad arguments");
+  Dns& E = Dh->E;
+  cudaStream_t s = as_stream(stream);
+  GIPB_TRY(E.grow_history(E.steps_enqueued + nsteps, s));
+  if (!E.started) {
+    GIPB_TRY(E.enqueue_initial_dt(s));
+    E.started = true;
+  }
+  // A graph needs a host-free step: FIXED mode, or TOL/MIXED run to their caps.
+  const bool graphable = E.prm.use_graph && E.prm.pcg.mode == GIPB200_PCG_FIXED;
+  for (int k = 0; k < nsteps; ++k) {
+    if (graphable) {
+      if (!E.exec) {
+        cudaStream_t cs = E.cap_stream;
+        GIPB_CUDA(cudaStreamSynchronize(s));
+        GIPB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        const long long before = E.launches;
+        int st = E.enqueue_step(cs, false);
+        E.graph_kernels = E.launches - before;
+        E.launches = before;
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(cs, &g);
+        if (st != GIPB200_OK) {
+          if (g) cudaGraphDestroy(g);
+          return st;
+        }
+        if (ce != cudaSuccess)
+          return fail(GIPB200_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+        E.graph = g;
+        GIPB_CUDA(cudaGraphInstantiate(&E.exec, E.graph, 0));
+      }
+      GIPB_CUDA(cudaGraphLaunch(E.exec, s));
+      E.launches += E.graph_kernels;
+    } else {
+      GIPB_TRY(E.enqueue_step(s, true));
+    }
+    E.steps_enqueued += 1;
+  }
+  return GIPB200_OK;
+}
+
+int gipb200_dns_history(gipb200_dns Dh, int* steps, double* t, double* dt, double* massr,
+                        int* iters, double* rr) {
+  if (!Dh) return fail(GIPB200_ERR_ARG, "null engine");
+  Dns& E = Dh->E;
+  GIPB_CUDA(cudaDeviceSynchronize());
+  DnsScalars S;
+  GIPB_CUDA(cudaMemcpy(&S, E.sc.p, sizeof(S), cudaMemcpyDeviceToHost));
+  const int n = std::min(S.step, E.capacity);
+  if (steps) *steps = S.step;
+  if (t && n) GIPB_CUDA(cudaMemcpy(t, E.h_time.p, n * 8, cudaMemcpyDeviceToHost));
+  if (dt && n) GIPB_CUDA(cudaMemcpy(dt, E.h_dt.p, n * 8, cudaMemcpyDeviceToHost));
+  if (massr && n) GIPB_CUDA(cudaMemcpy(massr, E.h_massr.p, n * 8, cudaMemcpyDeviceToHost));
+  if (iters && n) GIPB_CUDA(cudaMemcpy(iters, E.h_iters.p, n * 4, cudaMemcpyDeviceToHost));
+  if (rr && n) GIPB_CUDA(cudaMemcpy(rr, E.h_rr.p, n * 8, cudaMemcpyDeviceToHost));
+  return GIPB200_OK;
+}
+
+int gipb200_dns_get_field(gipb200_dns Dh, const char* name, double* h_out, int n) {
+  if (!Dh || !name || !h_out) return fail(GIPB200_ERR_ARG, "null argument");
+  int sz = 0;
+  double* p = Dh->E.field(name, &sz);
+  if (!p) return fail(GIPB200_ERR_ARG, "unknown field '%s'", name);
+  if (n < sz) return fail(GIPB200_ERR_ARG, "buffer of %d for field of %d", n, sz);
+  GIPB_CUDA(cudaDeviceSynchronize());
+  GIPB_CUDA(cudaMemcpy(h_out, p, (size_t)sz * 8, cudaMemcpyDeviceToHost));
+  return GIPB200_OK;
+}
+
+int gipb200_dns_field_ptr(gipb200_dns Dh, const char* name, double** d_ptr, int* n) {
+  if (!Dh || !name || !d_ptr) return fail(GIPB200_ERR_ARG, "null argument");
+  int sz = 0;
+  double* p = Dh->E.field(name, &sz);
+  if (!p) return fail(GIPB200_ERR_ARG, "unknown field '%s'", name);
+  *d_ptr = p;
+  if (n) *n = sz;
+  return GIPB200_OK;
+}
+
+int gipb200_dns_set_field(gipb200_dns Dh, const char* name, const double* h_in, int offset,
+                          int n, void* stream) {
+  if (!Dh || !name || (!h_in && n)) return fail(GIPB200_ERR_ARG, "null argument");
+  int sz = 0;
+  double* p = Dh->E.field(name, &sz);
+  if (!p) return fail(GIPB200_ERR_ARG, "unknown field '%s'", name);
+  if (offset < 0 || n < 0 || (long long)offset + n > sz)
+    return fail(GIPB200_ERR_ARG, "range [%d,%d) outside field of %d", offset, offset + n, sz);
+  if (n)
+    GIPB_CUDA(cudaMemcpyAsync(p + offset, h_in, (size_t)n * 8, cudaMemcpyHostToDevice,
+                              as_stream(stream)));
+  return GIPB200_OK;
+}
+
+int gipb200_dns_launch_count(gipb200_dns Dh, long long* count) {
+  if (!Dh || !count) return fail(GIPB200_ERR_ARG, "null argument");
+  *count = Dh->E.launches;
+  return GIPB200_OK;
+}
+
+int gipb200_dns_kernel_time(gipb200_dns Dh, int kernel, int reps, void* stream, double* avg_ms,
+                            double* bytes) {
+  if (!Dh || !avg_ms || !bytes) return fail(GIPB200_ERR_ARG, "null argument");
+  if (kernel != GIPB200_KERNEL_PCG_SPMV_DOT && kernel != GIPB200_KERNEL_MIXED_SPMV_DOT)
+    return fail(GIPB200_ERR_ARG, "unknown kernel id %d", kernel);
+  return Dh->E.pcg.time_spmv(kernel == GIPB200_KERNEL_MIXED_SPMV_DOT, reps, as_stream(stream),
+                             avg_ms, bytes);
+}
+
+int gipb200_dns_scalars(gipb200_dns Dh, double* dt, double* sigma, double* time) {
+  if (!Dh) return fail(GIPB200_ERR_ARG, "null engine");
+  GIPB_CUDA(cudaDeviceSynchronize());
+  DnsScalars S;
+  GIPB_CUDA(cudaMemcpy(&S, Dh->E.sc.p, sizeof(S), cudaMemcpyDeviceToHost));
+  if (dt) *dt = S.dt;
+  if (sigma) *sigma = S.sigma;
+  if (time) *time = S.time;
+  return GIPB200_OK;
+}
+
+}  // extern "C"

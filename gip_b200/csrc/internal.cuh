@@ -1,0 +1,153 @@
+// Internal declarations shared by the gipb200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gipb200.h"
+
+namespace gipb200 {
+
+// ------------------------------------------------------------------ errors
+int fail(int status, const char* fmt, ...);
+void clear_error();
+
+#define GIPB_CUDA(call)                                                                    \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return ::gipb200::fail(GIPB200_ERR_CUDA, "%s failed: %s (%s:%d)", #call,             \
+                             cudaGetErrorString(e_), __FILE__, __LINE__);                  \
+  } while (0)
+
+#define GIPB_TRY(expr)                   \
+  do {                                   \
+    int s_ = (expr);                     \
+    if (s_ != GIPB200_OK) return s_;     \
+  } while (0)
+
+#define GIPB_LAUNCH_CHECK()                                                                \
+  do {                                                                                     \
+    cudaError_t e_ = cudaGetLastError();                                                   \
+    if (e_ != cudaSuccess)                                                                 \
+      return ::gipb200::fail(GIPB200_ERR_CUDA, "kernel launch failed: %s (%s:%d)",         \
+                             cudaGetErrorString(e_), __FILE__, __LINE__);                  \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ------------------------------------------------------------------ device info
+struct DeviceInfo {
+  int device = -1;
+  int nsm = 0;
+  int l2_bytes = 0;
+};
+int device_info(DeviceInfo* out);  // of the current device, cached per device
+
+// ------------------------------------------------------------------ owning device buffer
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  int alloc(size_t count) {
+    release();
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return fail(GIPB200_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", count * sizeof(T),
+                  cudaGetErrorString(e));
+    }
+    n = count;
+    return GIPB200_OK;
+  }
+  int upload(const T* h, size_t count, cudaStream_t s = 0) {
+    GIPB_TRY(alloc(count));
+    if (count) GIPB_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    return GIPB200_OK;
+  }
+  int zero(cudaStream_t s = 0) {
+    GIPB_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+    return GIPB200_OK;
+  }
+};
+
+// ------------------------------------------------------------------ reduction scratch
+// Block partials plus a ticket counter for single-pass grid reductions.  The last
+// block to arrive sums the partials in block order, so the result depends only on the
+// launch shape, never on scheduling.
+constexpr int kMaxReduceBlocks = 8192;
+constexpr int kMaxReduceWidth = 4;
+struct ReduceScratch {
+  double* partials;   // [kMaxReduceWidth][kMaxReduceBlocks]
+  unsigned* ticket;   // one counter, zero between launches
+};
+int reduce_scratch_alloc(DevBuf<double>* partials, DevBuf<unsigned>* ticket, ReduceScratch* out);
+
+// ------------------------------------------------------------------ sliced ELL (SELL-32)
+// Rows are grouped in slices of 32; slice s stores its rows' nonzeros column-major
+// (slot j of lane l at sptr[s] + 32*j + l), padded to the slice's longest row with
+// col = -1.  Each row keeps its CSR nonzero order, so a lane summing slot by slot
+// adds in exactly the CSR order.
+template <typename V>
+struct SellView {
+  int nrows;
+  int nslices;
+  const long long* __restrict__ sptr;
+  const int* __restrict__ col;
+  const V* __restrict__ val;
+};
+
+struct Sell {
+  int nrows = 0, ncols = 0, nnz = 0, nslices = 0;
+  long long nslots = 0;
+  bool rows_nonempty = true;  // no empty row
+  DevBuf<long long> sptr;
+  DevBuf<int> col;
+  DevBuf<double> val;
+  DevBuf<float> val32;        // optional FP32 copy
+  DevBuf<int> pos;            // CSR nonzero k -> slot index (value-target writes)
+  DevBuf<int> rowptr;         // device CSR copy
+  DevBuf<int> csr_col;
+  DevBuf<double> csr_val;
+  std::vector<int> h_rowptr, h_col;  // host CSR structure (setup only)
+  SellView<double> view() const { return {nrows, nslices, sptr.p, col.p, val.p}; }
+  SellView<double> view_vals(const double* v) const { return {nrows, nslices, sptr.p, col.p, v}; }
+  SellView<float> view32() const { return {nrows, nslices, sptr.p, col.p, val32.p}; }
+};
+
+// Builds SELL-32 (and keeps a device CSR copy) from host CSR arrays.
+int sell_build(Sell* S, int nrows, int ncols, int nnz, const int* h_rowptr, const int* h_col,
+               const double* h_val, cudaStream_t stream);
+// Adds an FP32 value copy.
+int sell_add_fp32(Sell* S, cudaStream_t stream);
+int validate_csr(int nrows, int ncols, int nnz, const int* rowptr, const int* col,
+                 int col_bound, const char* name);
+
+// Generic launches used by several translation units.
+int launch_sell_spmv(const Sell& A, const double* vals, const double* x, double* y, double alpha,
+                     double beta, int mode, cudaStream_t s);
+int launch_csr_spmv(int nrows, const int* rowptr, const int* col, const double* val,
+                    const double* x, double* y, const int* ypos, double alpha, double beta,
+                    int mode, cudaStream_t s);
+int grid_blocks(int threads, int work_items, int per_thread, int max_blocks, int* blocks);
+
+}  // namespace gipb200
+
+struct gipb200_matrix_s {
+  gipb200::Sell S;
+};

@@ -1,0 +1,73 @@
+// Device-resident Jacobi-PCG shared by the PCG handle and the timestep engine.
+#pragma once
+
+#include "internal.cuh"
+
+namespace gipb200 {
+
+// Scalars of one solve, in device memory (kernels read and write them; the host only
+// reads them after the solve).
+struct PcgScalars {
+  double rz;        // r.z (FP64 modes) / scaled r.r (inner solve of MIXED)
+  double pAp;
+  double alpha, beta;
+  double rr;        // r.r (FP64 modes: recursive residual; MIXED: true residual)
+  double bb;        // b.b
+  double rz_target; // MIXED: inner stop level
+  int iter;         // iterations of the current (inner) solve
+  int done;         // FP64 modes: solve finished; MIXED: outer loop finished
+  int inner_done;   // MIXED: current inner solve finished
+  int status;       // GIPB200_OK or GIPB200_ERR_BREAKDOWN / NOT_CONVERGED
+  int outer;        // MIXED: refinement cycles done
+  int total_inner;  // MIXED: inner iterations summed over cycles
+  int pad[2];
+  double rsum;      // MIXED: sum of the FP64 residual (pinned-Neumann deflation)
+  double kappa_c;   // MIXED: sum(r)/pin, the pinned cell's exact correction
+};
+
+struct Pcg {
+  const Sell* L = nullptr;   // not owned
+  int n = 0;                 // unknowns = L rows (GIP's inner range)
+  int n_all = 0;             // vector length (inner + ghost cells)
+  gipb200_pcg_params prm{};
+  DevBuf<double> dinv, p, Ap, r;
+  // MIXED
+  DevBuf<float> lhat;        // S L S values in L's sliced layout (FP32)
+  DevBuf<double> scale;      // S = 1/sqrt(L_ii)
+  DevBuf<float> p32, Ap32, r32, y32;
+  DevBuf<double> rtrue;
+  // Pinned-Neumann structure of L (every row sums to zero except one pinned row p with
+  // sum pin > 0): the FP32 inner solve then runs on the pure-Neumann part and the
+  // constant mode is restored exactly from the pin equation.
+  int pin_row = -1;
+  double pin_val = 0.0;
+  // scalars and reduction scratch
+  DevBuf<PcgScalars> sc;
+  DevBuf<double> partials;
+  DevBuf<unsigned> ticket;
+  ReduceScratch rs{};
+  PcgScalars* h_sc = nullptr;  // pinned
+  int blocks_spmv = 1, blocks_vec = 1;
+  long long launches = 0;      // kernels enqueued by this solver (host count)
+
+  ~Pcg();
+  int init(const Sell* L, int n_all, const gipb200_pcg_params& prm, cudaStream_t s);
+  // Enqueues a whole solve.  FIXED mode never synchronises the host.  TOL and MIXED
+  // poll the device's stop flag every `poll` iterations when host_sync is true; with
+  // host_sync false they run exactly their iteration caps (masked after convergence).
+  int enqueue(const double* b, double* x, const double* x0, cudaStream_t s, bool host_sync);
+  int result(cudaStream_t s, gipb200_pcg_result* out);
+  // Times `reps` launches of the SpMV+dot kernel of the current mode on scratch scalars.
+  int time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* bytes);
+
+ private:
+  int enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t s, bool host_sync);
+  int enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_t s, bool host_sync);
+  int read_flag(cudaStream_t s, int which, int* v);
+};
+
+}  // namespace gipb200
+
+struct gipb200_pcg_s {
+  gipb200::Pcg P;
+};

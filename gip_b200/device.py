@@ -1,0 +1,286 @@
+"""Python front end of the B200 library over its C ABI.
+
+Device vectors are ``torch.float64`` CUDA tensors; the operators and solvers are
+library handles.  Names follow GIP's Specification: ``DeviceMatrix.spmv`` is
+``GIP_Matrix::spmv`` (y = A x, or y = alpha A x + beta y with mode 1, empty rows left
+untouched), ``PcgSolver`` is ``GIP_LinearSolver`` and ``DnsEngine`` is ``GIP_DNS``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, Optional
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .formats import Csr, GipCase
+
+
+def _stream(stream=None) -> C.c_void_p:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+def _dptr(t: Optional[torch.Tensor]) -> C.c_void_p:
+    if t is None:
+        return C.c_void_p(0)
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("expected a contiguous CUDA tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _hptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def _host_csr(m: Csr, keep: list) -> L.HostCsr:
+    rp = np.ascontiguousarray(m.rowptr, np.int32)
+    col = np.ascontiguousarray(m.col, np.int32)
+    val = np.ascontiguousarray(m.val, np.float64)
+    keep += [rp, col, val]
+    return L.HostCsr(m.nrows, m.ncols, m.nnz, _hptr(rp), _hptr(col), _hptr(val))
+
+
+# ----------------------------------------------------------------------------- raw kernels
+def spmv_raw(rowptr: torch.Tensor, col: torch.Tensor, val: torch.Tensor, x: torch.Tensor,
+             y: torch.Tensor, alpha: float = 0.0, beta: float = 0.0, mode: int = 0,
+             stream=None) -> torch.Tensor:
+    L.call("gipb200_dcsr_spmv", rowptr.numel() - 1, _dptr(rowptr), _dptr(col), _dptr(val),
+           _dptr(x), _dptr(y), alpha, beta, mode, _stream(stream))
+    return y
+
+
+def axpy(y: torch.Tensor, x: torch.Tensor, alpha: float, n: Optional[int] = None, stream=None):
+    L.call("gipb200_daxpy", y.numel() if n is None else n, _dptr(y), _dptr(x), alpha,
+           _stream(stream))
+    return y
+
+
+def axpby(y: torch.Tensor, x: torch.Tensor, alpha: float, beta: float, n: Optional[int] = None,
+          stream=None):
+    L.call("gipb200_daxpby", y.numel() if n is None else n, _dptr(y), _dptr(x), alpha, beta,
+           _stream(stream))
+    return y
+
+
+def fill(y: torch.Tensor, value: float, stream=None):
+    L.call("gipb200_dfill", y.numel(), _dptr(y), value, _stream(stream))
+    return y
+
+
+def dot(x: torch.Tensor, y: torch.Tensor, n: Optional[int] = None, stream=None) -> float:
+    out = C.c_double()
+    L.call("gipb200_ddot", x.numel() if n is None else n, _dptr(x), _dptr(y), C.byref(out),
+           _stream(stream))
+    return out.value
+
+
+def norminf(x: torch.Tensor, n: Optional[int] = None, stream=None) -> float:
+    out = C.c_double()
+    L.call("gipb200_dnorminf", x.numel() if n is None else n, _dptr(x), C.byref(out),
+           _stream(stream))
+    return out.value
+
+
+def cfl(u, v, w, dxs, n: int, gamma: float, rho: float, stream=None) -> float:
+    out = C.c_double()
+    L.call("gipb200_cfl", n, _dptr(u), _dptr(v), _dptr(w), _dptr(dxs), gamma, rho, C.byref(out),
+           _stream(stream))
+    return out.value
+
+
+# ----------------------------------------------------------------------------- matrices
+class DeviceMatrix:
+    """A CSR operator resident on the device (``GIP_MatrixCuda`` counterpart)."""
+
+    def __init__(self, m: Csr):
+        lib = L.load()
+        keep: list = []
+        h = _host_csr(m, keep)
+        handle = C.c_void_p()
+        L.check(lib.gipb200_matrix_create(h.nrows, h.ncols, h.nnz, h.rowptr, h.col, h.val,
+                                          C.byref(handle)), "gipb200_matrix_create")
+        self.handle = handle
+        self.nrows, self.ncols, self.nnz = m.nrows, m.ncols, m.nnz
+
+    def info(self) -> dict:
+        r, c, z = C.c_int(), C.c_int(), C.c_int()
+        s = C.c_int64()
+        L.call("gipb200_matrix_info", self.handle, C.byref(r), C.byref(c), C.byref(z), C.byref(s))
+        return {"nrows": r.value, "ncols": c.value, "nnz": z.value, "padded_slots": s.value}
+
+    def _check(self, x: torch.Tensor, ylen: int, y: torch.Tensor) -> None:
+        if x.dtype != torch.float64 or y.dtype != torch.float64:
+            raise TypeError("vectors must be float64")
+        if x.numel() < self.ncols or y.numel() < ylen:
+            raise ValueError(f"vector sizes ({x.numel()}, {y.numel()}) below operator "
+                             f"({self.ncols}, {ylen})")
+
+    def spmv(self, x: torch.Tensor, y: torch.Tensor, alpha: float = 0.0, beta: float = 0.0,
+             mode: int = 0, stream=None) -> torch.Tensor:
+        self._check(x, self.nrows, y)
+        L.call("gipb200_matrix_spmv", self.handle, _dptr(x), _dptr(y), alpha, beta, mode,
+               _stream(stream))
+        return y
+
+    def spmv_values(self, x: torch.Tensor, target: "DeviceMatrix", alpha: float = 0.0,
+                    beta: float = 0.0, mode: int = 0, stream=None) -> None:
+        if x.numel() < self.ncols:
+            raise ValueError("x shorter than the operator's columns")
+        L.call("gipb200_matrix_spmv_values", self.handle, _dptr(x), target.handle, alpha, beta,
+               mode, _stream(stream))
+
+    def values(self) -> np.ndarray:
+        out = np.zeros(self.nnz)
+        L.call("gipb200_matrix_get_values", self.handle, _hptr(out))
+        return out
+
+    def inverse_diagonal(self) -> tuple:
+        d = torch.zeros(self.nrows, dtype=torch.float64, device="cuda")
+        miss = C.c_int()
+        L.call("gipb200_matrix_inverse_diagonal", self.handle, _dptr(d), C.byref(miss))
+        return d, miss.value
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            L.load().gipb200_matrix_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+MODES = {"fixed": L.PCG_FIXED, "tol": L.PCG_TOL, "mixed": L.PCG_MIXED}
+
+
+def pcg_params(mode: str = "fixed", maxit: int = 100, tol: float = 1e-6,
+               inner_tol: float = 1e-3, inner_maxit: int = 2000, max_outer: int = 30) -> L.PcgParams:
+    return L.PcgParams(MODES[mode], maxit, tol, inner_tol, inner_maxit, max_outer)
+
+
+class PcgSolver:
+    """``GIP_LinearSolver`` on the device: Jacobi PCG, FP64 (fixed or tolerance) or
+    mixed FP32-inner / FP64-refinement."""
+
+    def __init__(self, A: DeviceMatrix, n_all: Optional[int] = None, **kw):
+        self.A = A
+        self.n_all = n_all or A.nrows
+        self.params = pcg_params(**kw)
+        handle = C.c_void_p()
+        L.call("gipb200_pcg_create", A.handle, n_all or A.nrows, C.byref(self.params),
+               C.byref(handle))
+        self.handle = handle
+
+    def solve(self, b: torch.Tensor, x: torch.Tensor, x0: torch.Tensor, stream=None) -> dict:
+        n_all = max(self.n_all, self.A.nrows)
+        if b.numel() < self.A.nrows or x.numel() < n_all or x0.numel() < n_all:
+            raise ValueError("b needs the operator's rows, x and x0 need n_all entries")
+        for t in (b, x, x0):
+            if t.dtype != torch.float64:
+                raise TypeError("vectors must be float64")
+        res = L.PcgResult()
+        L.call("gipb200_pcg_solve", self.handle, _dptr(b), _dptr(x), _dptr(x0), _stream(stream),
+               C.byref(res))
+        return {"iterations": res.iterations, "outer": res.outer, "status": res.status,
+                "rr": res.rr, "bb": res.bb}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.load().gipb200_pcg_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ----------------------------------------------------------------------------- timestep
+class DnsEngine:
+    """``GIP_DNS`` on the device: ``advance(n)`` is ``integrate()`` for n timesteps."""
+
+    def __init__(self, case: GipCase, rho: float = 1.0, gamma: float = 1e-3,
+                 pcg_mode: str = "fixed", maxit: int = 100, tol: float = 1e-6,
+                 inner_tol: float = 1e-3, inner_maxit: int = 2000, max_outer: int = 30,
+                 use_graph: bool = True):
+        lib = L.load()
+        keep: list = []
+        ops = L.DnsOps(**{n: _host_csr(case.ops[n], keep) for n in L.DNS_OPS},
+                       n_inner=case.n_inner, n_owned=case.n_owned, n_faces=case.n_faces)
+        f = {k: np.ascontiguousarray(case.fields[k], np.float64) for k in ("u", "v", "w", "dxs")}
+        self.params = L.DnsParams(rho, gamma, pcg_params(pcg_mode, maxit, tol, inner_tol,
+                                                         inner_maxit, max_outer), int(use_graph))
+        handle = C.c_void_p()
+        L.check(lib.gipb200_dns_create(C.byref(ops), _hptr(f["u"]), _hptr(f["v"]), _hptr(f["w"]),
+                                       _hptr(f["dxs"]), C.byref(self.params), C.byref(handle)),
+                "gipb200_dns_create")
+        self.handle = handle
+        self.n_inner, self.n_owned, self.n_faces = case.n_inner, case.n_owned, case.n_faces
+
+    def advance(self, nsteps: int, stream=None) -> None:
+        L.call("gipb200_dns_advance", self.handle, nsteps, _stream(stream))
+
+    def history(self) -> Dict[str, np.ndarray]:
+        steps = C.c_int()
+        L.call("gipb200_dns_history", self.handle, C.byref(steps), None, None, None, None, None)
+        n = steps.value
+        out = {"time": np.zeros(n), "dt": np.zeros(n), "massr": np.zeros(n),
+               "iters": np.zeros(n, np.int32), "rr": np.zeros(n)}
+        L.call("gipb200_dns_history", self.handle, C.byref(steps), _hptr(out["time"]),
+               _hptr(out["dt"]), _hptr(out["massr"]), _hptr(out["iters"]), _hptr(out["rr"]))
+        return out
+
+    def field(self, name: str) -> np.ndarray:
+        n = self.n_faces if name == "mf" else self.n_owned
+        out = np.zeros(n)
+        L.call("gipb200_dns_get_field", self.handle, name.encode(), _hptr(out), n)
+        return out
+
+    def field_ptr(self, name: str) -> tuple:
+        p = C.c_void_p()
+        n = C.c_int()
+        L.call("gipb200_dns_field_ptr", self.handle, name.encode(), C.byref(p), C.byref(n))
+        return p.value, n.value
+
+    def set_field(self, name: str, values: np.ndarray, offset: int = 0, stream=None) -> None:
+        """Asynchronous host->device copy into a field (keep `values` alive and, for a
+        truly asynchronous copy, pinned, until the stream has passed it)."""
+        if values.dtype != np.float64 or not values.flags.c_contiguous:
+            raise TypeError("values must be a contiguous float64 array")
+        L.call("gipb200_dns_set_field", self.handle, name.encode(), _hptr(values), offset,
+               values.size, _stream(stream))
+
+    def kernel_time(self, kernel: str = "mixed", reps: int = 20, stream=None) -> tuple:
+        """Mean CUDA-event time (ms) and compulsory bytes of one PCG SpMV+dot launch."""
+        kid = {"fp64": 0, "mixed": 1}[kernel]
+        ms, by = C.c_double(), C.c_double()
+        L.call("gipb200_dns_kernel_time", self.handle, kid, reps, _stream(stream), C.byref(ms),
+               C.byref(by))
+        return ms.value, by.value
+
+    def launch_count(self) -> int:
+        c = C.c_longlong()
+        L.call("gipb200_dns_launch_count", self.handle, C.byref(c))
+        return c.value
+
+    def scalars(self) -> dict:
+        dt, sg, t = C.c_double(), C.c_double(), C.c_double()
+        L.call("gipb200_dns_scalars", self.handle, C.byref(dt), C.byref(sg), C.byref(t))
+        return {"dt": dt.value, "sigma": sg.value, "time": t.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.load().gipb200_dns_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

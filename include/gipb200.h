@@ -1,0 +1,207 @@
+/*
+ * gipb200 -- B200 (sm_100a) kernels and device-resident solvers for GIP's algebraic
+ * fractional-step Navier-Stokes timestep, behind a plain C ABI.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (GIPB200_OK = 0).  On error
+ *    gipb200_last_error() returns a message for the calling thread.
+ *  - Pointers named d_* are device pointers; h_* are host pointers owned by the
+ *    caller.  Handles own their device memory until *_destroy.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream).
+ *  - Integer indices are 0-based int32, values float64, as in GIP's CSR files.
+ *  - SpMV follows GIP's CPU Specification: a row with rowptr[i]==rowptr[i+1] leaves
+ *    y[i] untouched, and every row sums its nonzeros sequentially in stored order, so
+ *    float64 products match GIP's CPU build bit for bit.
+ *
+ * GIP's own device library is `extern "C++"` with void returns and default-stream
+ * blocking reductions (src/Specifications/Cuda/Headers/GIP_gpu.h:4-46); each
+ * declaration below names the routine it replaces.
+ */
+#ifndef GIPB200_H
+#define GIPB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  GIPB200_OK = 0,
+  GIPB200_ERR_ARG = 1,        /* invalid argument or inconsistent sizes            */
+  GIPB200_ERR_CUDA = 2,       /* a CUDA runtime call failed                        */
+  GIPB200_ERR_BREAKDOWN = 3,  /* PCG: p.Ap <= 0 or a non-finite scalar             */
+  GIPB200_ERR_TIMEOUT = 4,    /* a bounded device wait gave up                     */
+  GIPB200_ERR_NOMEM = 5,      /* device or host allocation failed                  */
+  GIPB200_ERR_NOT_CONVERGED = 6,
+  GIPB200_ERR_STATE = 7       /* call not valid in the object's current state       */
+};
+
+/* ------------------------------------------------------------------ library */
+int gipb200_version(void);                 /* major*10000 + minor*100 + patch */
+const char* gipb200_status_string(int status);
+const char* gipb200_last_error(void);
+
+/* GIP_cudaSetDevice (src/Specifications/Cuda/Libs/libgpu.cu:237-240) */
+int gipb200_set_device(int device);
+/* GIP_cudaMallocDouble / GIP_cudaMallocInt (libgpu.cu:18-26) */
+int gipb200_malloc(void** d_ptr, size_t bytes);
+/* GIP_cudaFree (libgpu.cu:52-55) */
+int gipb200_free(void* d_ptr);
+/* GIP_cudaMemcpyDToGpu / IToGpu (libgpu.cu:29-39) */
+int gipb200_memcpy_h2d(void* d_dst, const void* h_src, size_t bytes, void* stream);
+/* GIP_cudaMemcpyDToCpu / IToCpu (libgpu.cu:41-49) */
+int gipb200_memcpy_d2h(void* h_dst, const void* d_src, size_t bytes, void* stream);
+/* GIP_cudaDcopy (libgpu.cu:68-71): d_dst[0:n) = d_src[0:n) */
+int gipb200_dcopy(int n, double* d_dst, const double* d_src, void* stream);
+int gipb200_stream_sync(void* stream);
+
+/* ------------------------------------------------------------------ raw-pointer kernels */
+/* GIP_cudaDCsrSpMV (libgpu.cu:89-96 and 113-120).  mode 0: y = A x; mode 1:
+ * y = alpha A x + beta y.  Empty rows keep y (GIP's CPU semantics, not libgpu's). */
+int gipb200_dcsr_spmv(int nrows, const int* d_rowptr, const int* d_col, const double* d_val,
+                      const double* d_x, double* d_y, double alpha, double beta, int mode,
+                      void* stream);
+/* GIP_cudaDaxpy (libgpu.cu:133-139): y += alpha x */
+int gipb200_daxpy(int n, double* d_y, const double* d_x, double alpha, void* stream);
+/* GIP_cudaDaxpy(alpha,beta) (libgpu.cu:152-158): y = alpha x + beta y */
+int gipb200_daxpby(int n, double* d_y, const double* d_x, double alpha, double beta,
+                   void* stream);
+/* GIP_VectorCuda::operator=(int) (GIP_VectorCuda.cpp:190-195): y[0:n) = value */
+int gipb200_dfill(int n, double* d_y, double value, void* stream);
+/* GIP_cudaDdot (libgpu.cu:160-203): *h_result = sum x[i]*y[i], one pass, deterministic
+ * two-level order; blocks until the result is on the host. */
+int gipb200_ddot(int n, const double* d_x, const double* d_y, double* h_result, void* stream);
+/* GIP_gpuNormi (libgpu.cu:337-393): *h_result = max |x[i]| */
+int gipb200_dnorminf(int n, const double* d_x, double* h_result, void* stream);
+/* GIP_gpuGetCFL (libgpu.cu:244-334) with GIP's CPU expression order
+ * (GIP_NonLinearMulticore.cpp:3-55): *h_dt = min(0.1, 0.8*min_i(...)) over [0,n). */
+int gipb200_cfl(int n, const double* d_u, const double* d_v, const double* d_w,
+                const double* d_dxs, double gamma, double rho, double* h_dt, void* stream);
+
+/* ------------------------------------------------------------------ matrix handles */
+typedef struct gipb200_matrix_s* gipb200_matrix;
+
+/* GIP_MatrixCuda::postConstruct (src/Specifications/Cuda/GIP_MatrixCuda.cpp:14-53):
+ * uploads a host CSR and builds the device layouts (CSR plus 32-row sliced ELL).
+ * Every column index must lie in [0, ncols): x vectors passed to the products must hold
+ * ncols entries (at one rank GIP's operators satisfy this with ncols = cells or faces). */
+int gipb200_matrix_create(int nrows, int ncols, int nnz, const int* h_rowptr, const int* h_col,
+                          const double* h_val, gipb200_matrix* out);
+int gipb200_matrix_destroy(gipb200_matrix A);
+int gipb200_matrix_info(gipb200_matrix A, int* nrows, int* ncols, int* nnz, int64_t* padded_slots);
+/* GIP_MatrixCuda::spmv(x,b[,alpha,beta]) (GIP_MatrixCuda.cpp:83-91) */
+int gipb200_matrix_spmv(gipb200_matrix A, const double* d_x, double* d_y, double alpha,
+                        double beta, int mode, void* stream);
+/* GIP_MatrixCuda::spmv(x,GIP_Matrix*[,alpha,beta]) (GIP_MatrixCuda.cpp:93-100): row k of A
+ * writes value k of `target` (A has one row per nonzero of target). */
+int gipb200_matrix_spmv_values(gipb200_matrix A, const double* d_x, gipb200_matrix target,
+                               double alpha, double beta, int mode, void* stream);
+/* Copies the target's current values (stored order) to the host. */
+int gipb200_matrix_get_values(gipb200_matrix A, double* h_val);
+/* GIP_MatrixCuda::setUpDiagonal (GIP_MatrixCuda.cpp:143-184): d_dinv[i] = 1/A_ii;
+ * *missing = rows without a diagonal entry (their dinv is 0). */
+int gipb200_matrix_inverse_diagonal(gipb200_matrix A, double* d_dinv, int* missing);
+
+/* ------------------------------------------------------------------ PCG */
+typedef struct gipb200_pcg_s* gipb200_pcg;
+
+enum {
+  GIPB200_PCG_FIXED = 0,  /* exactly maxit iterations: GIP_LinearSolver.h:85-116          */
+  GIPB200_PCG_TOL = 1,    /* stop when ||r||_2 <= tol ||b||_2 (r recursive)                */
+  GIPB200_PCG_MIXED = 2   /* FP32 inner PCG inside FP64 iterative refinement, stop at tol  */
+};
+
+typedef struct {
+  int mode;          /* GIPB200_PCG_*                                                */
+  int maxit;         /* FIXED: iterations; TOL/MIXED: cap on (inner) iterations      */
+  double tol;        /* TOL/MIXED: relative 2-norm residual target                   */
+  double inner_tol;  /* MIXED: inner solve reduces its residual by this factor       */
+  int inner_maxit;   /* MIXED: cap per inner solve                                   */
+  int max_outer;     /* MIXED: cap on refinement cycles                              */
+} gipb200_pcg_params;
+
+typedef struct {
+  int iterations;        /* FIXED/TOL: PCG iterations; MIXED: inner iterations summed */
+  int outer;             /* MIXED: refinement cycles                                  */
+  int status;            /* GIPB200_OK / BREAKDOWN / NOT_CONVERGED                    */
+  double rr;             /* r.r at exit (MIXED: true FP64 residual)                   */
+  double bb;             /* b.b                                                       */
+} gipb200_pcg_result;
+
+/* GIP_LinearSolver::setUp (src/Algorithms/GIP_LinearSolver.h:31-42) */
+int gipb200_pcg_create(gipb200_matrix L, int n_all, const gipb200_pcg_params* params,
+                       gipb200_pcg* out);
+int gipb200_pcg_destroy(gipb200_pcg S);
+/* GIP_LinearSolver::solve (GIP_LinearSolver.h:44-117): x (n_all) = PCG(b) from x0. */
+int gipb200_pcg_solve(gipb200_pcg S, const double* d_b, double* d_x, const double* d_x0,
+                      void* stream, gipb200_pcg_result* h_result);
+
+/* ------------------------------------------------------------------ timestep engine */
+typedef struct gipb200_dns_s* gipb200_dns;
+
+typedef struct {
+  int nrows, ncols, nnz;
+  const int* rowptr;
+  const int* col;
+  const double* val;
+} gipb200_host_csr;
+
+/* The operators GIP_DNS loads (src/Algorithms/GIP_DNS.h:143-238), host memory. */
+typedef struct {
+  gipb200_host_csr D, Ec, L, Lb, Mx, My, Mz, Mres, Gx, Gy, Gz, SFx, SFy, SFz, SO;
+  int n_inner, n_owned, n_faces;
+} gipb200_dns_ops;
+
+typedef struct {
+  double rho;                  /* GIP_DNS.h:133 (1.0)                             */
+  double gamma;                /* GIP_DNS.h:137 (1/Re; enters only the CFL limit)  */
+  gipb200_pcg_params pcg;      /* GIP_DNS.h:180-185 (FIXED, maxit 100)             */
+  int use_graph;               /* capture each timestep in a CUDA graph            */
+} gipb200_dns_params;
+
+/* GIP_DNS::setUp (GIP_DNS.h:116-125): uploads operators and the initial fields u,v,w,dxs
+ * (n_owned each); every other GIP_DNS vector starts at 0, C's values at D's. */
+int gipb200_dns_create(const gipb200_dns_ops* ops, const double* h_u, const double* h_v,
+                       const double* h_w, const double* h_dxs, const gipb200_dns_params* params,
+                       gipb200_dns* out);
+int gipb200_dns_destroy(gipb200_dns E);
+/* GIP_DNS::integrate (GIP_DNS.h:99-113): advances nsteps timesteps on `stream`; the first
+ * call also computes the initial dt.  No host synchronisation inside. */
+int gipb200_dns_advance(gipb200_dns E, int nsteps, void* stream);
+/* Per-step history of all steps so far (host arrays of length >= steps taken):
+ * time, dt used, massr (GIP_DNS.h:399-404), PCG iterations, final r.r. */
+int gipb200_dns_history(gipb200_dns E, int* steps_taken, double* h_time, double* h_dt,
+                        double* h_massr, int* h_iters, double* h_rr);
+/* Copies a field to the host: "u","v","w","p","p0","mf","ax0","ay0","az0","gpx",... */
+int gipb200_dns_get_field(gipb200_dns E, const char* name, double* h_out, int n);
+/* Copies h_in[0:n) into a field at `offset` on `stream` (no host synchronisation; the
+ * host buffer must stay valid until the stream reaches the copy).  Used to feed
+ * boundary values (e.g. the lid's ghost velocities) between steps. */
+int gipb200_dns_set_field(gipb200_dns E, const char* name, const double* h_in, int offset, int n,
+                          void* stream);
+/* Device pointer of a field (valid until destroy). */
+int gipb200_dns_field_ptr(gipb200_dns E, const char* name, double** d_ptr, int* n);
+/* Current dt, sigma=1/dt and simulated time. */
+int gipb200_dns_scalars(gipb200_dns E, double* dt, double* sigma, double* time);
+
+/* Number of this library's kernels the engine has launched so far (a graph launch counts
+ * the kernels it holds). */
+int gipb200_dns_launch_count(gipb200_dns E, long long* count);
+
+enum {
+  GIPB200_KERNEL_PCG_SPMV_DOT = 0,  /* FP64 PCG: Ap = L p fused with p.Ap           */
+  GIPB200_KERNEL_MIXED_SPMV_DOT = 1 /* FP32 inner PCG: Ap = (S L S) p fused with p.Ap */
+};
+/* Times `reps` back-to-back launches of one PCG kernel on the engine's resident operator
+ * with CUDA events on `stream`; returns the mean launch time and the kernel's compulsory
+ * bytes per launch (stored values and indices read once, the vector read once, the
+ * product written once).  Leaves the engine's fields untouched. */
+int gipb200_dns_kernel_time(gipb200_dns E, int kernel, int reps, void* stream, double* avg_ms,
+                            double* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GIPB200_H */

@@ -1,0 +1,89 @@
+"""Timestep parity: the device engine against the oracle and GIP's own goldens."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden_lines, have_c100k, rel_err
+from gip_b200 import cavity
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("u", "v", "w", "p", "p0", "mf", "ax0")
+
+
+def _lines(oracle, h):
+    return [oracle.format_line(h["time"][i], h["dt"][i], h["massr"][i], i + 1)
+            for i in range(len(h["time"]))]
+
+
+@pytest.mark.skipif(not have_c100k(), reason="merged C100K set not built")
+@pytest.mark.parametrize("graph", [True, False])
+def test_c100k_readme_golden(gpu, oracle_mod, c100k_case, graph):
+    from gip_b200.device import DnsEngine
+    E = DnsEngine(c100k_case, gamma=1e-3, pcg_mode="fixed", maxit=100, use_graph=graph)
+    E.advance(10)
+    h = E.history()
+    assert _lines(oracle_mod, h) == golden_lines("c100k_readme.txt")
+    d = oracle_mod.OracleDNS(c100k_case, gamma=1e-3)
+    d.run(10)
+    for k in FIELDS:
+        assert rel_err(E.field(k), d.vec[k]) < 1e-10, k
+
+
+@pytest.mark.parametrize("n", [8, 12])
+def test_fields_match_reference_goldens(gpu, n):
+    from gip_b200.device import DnsEngine
+    g = np.load(os.path.join(GOLDEN, f"cavity{n}_ref.npz"))
+    case, _ = cavity.generate(n, re=float(g["re"]))
+    E = DnsEngine(case, gamma=1.0 / float(g["re"]))
+    E.advance(int(g["steps"]))
+    h = E.history()
+    assert h["iters"].tolist() == [100] * int(g["steps"])
+    ref_dt = [float(l.split("[dt::")[1].split("]")[0]) for l in g["lines"]]
+    assert np.allclose(h["dt"], ref_dt, rtol=1e-6)
+    for k in FIELDS:
+        assert rel_err(E.field(k)[: g[k].size], g[k]) < 1e-10, k
+
+
+@pytest.mark.parametrize("n,re,seed", [(10, 100.0, None), (9, 1000.0, 11)])
+def test_engine_matches_oracle_stepwise(gpu, oracle_mod, n, re, seed):
+    from gip_b200.device import DnsEngine
+    case, _ = cavity.generate(n, re=re, permute_seed=seed)
+    E = DnsEngine(case, gamma=1.0 / re)
+    d = oracle_mod.OracleDNS(case, gamma=1.0 / re)
+    for chunk in (3, 4):
+        E.advance(chunk)
+        d.run(chunk)
+        for k in FIELDS:
+            assert rel_err(E.field(k), d.vec[k]) < 1e-10, k
+    h = E.history()
+    assert len(h["time"]) == 7
+    assert E.scalars()["time"] == pytest.approx(d.time, rel=1e-12)
+
+
+def test_engine_tol_mode_iterations(gpu, oracle_mod):
+    from gip_b200.device import DnsEngine
+    case, _ = cavity.generate(16, re=400.0)
+    E = DnsEngine(case, gamma=1.0 / 400, pcg_mode="tol", maxit=3000, tol=1e-8)
+    E.advance(5)
+    d = oracle_mod.OracleDNS(case, gamma=1.0 / 400, cg_maxit=3000, cg_mode=1, cg_tol=1e-8)
+    hr = d.run(5)
+    h = E.history()
+    assert np.all(np.abs(h["iters"] - hr["iters"]) <= 1), (h["iters"], hr["iters"])
+    for k in ("u", "p"):
+        assert rel_err(E.field(k), d.vec[k]) < 1e-7, k
+
+
+def test_engine_mixed_close_to_fp64(gpu, oracle_mod):
+    from gip_b200.device import DnsEngine
+    case, _ = cavity.generate(16, re=400.0)
+    E = DnsEngine(case, gamma=1.0 / 400, pcg_mode="mixed", maxit=3000, tol=1e-8,
+                  inner_tol=1e-3)
+    E.advance(5)
+    d = oracle_mod.OracleDNS(case, gamma=1.0 / 400, cg_maxit=3000, cg_mode=1, cg_tol=1e-10)
+    d.run(5)
+    h = E.history()
+    assert np.all(h["massr"] < 1e-6)
+    for k in ("u", "v", "w"):
+        assert rel_err(E.field(k), d.vec[k]) < 1e-6, k

@@ -1,0 +1,75 @@
+"""PCG parity: fixed iterations (GIP's solver), tolerance mode, mixed precision."""
+import numpy as np
+import pytest
+import torch
+
+from gip_b200 import cavity
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("n,maxit", [(6, 5), (10, 100), (16, 37)])
+def test_pcg_fixed_matches_oracle(gpu, oracle_mod, n, maxit):
+    from gip_b200 import device as dv
+    L, b = cavity.poisson_problem(n, seed=n)
+    x0 = np.random.default_rng(1).standard_normal(L.nrows) * 0.1
+    xr, it, rr = oracle_mod.pcg(L, b, x0, maxit=maxit, mode=0)
+    S = dv.PcgSolver(dv.DeviceMatrix(L), mode="fixed", maxit=maxit)
+    x = _t(np.zeros(L.nrows))
+    res = S.solve(_t(b), x, _t(x0))
+    assert res["iterations"] == it == maxit
+    err = np.abs(x.cpu().numpy() - xr).max() / np.abs(xr).max()
+    assert err < 1e-10, err
+
+
+def test_pcg_fixed_with_ghost_columns(gpu, oracle_mod):
+    # the cavity's L carries stored-zero ghost columns and warm-starts from an n_all x0
+    from gip_b200 import device as dv
+    case, _ = cavity.generate(7, re=100.0)
+    L = case.ops["L"]
+    rng = np.random.default_rng(5)
+    b = rng.standard_normal(L.nrows)
+    x0 = rng.standard_normal(case.n_owned)
+    xr, it, rr = oracle_mod.pcg(L, b, x0, maxit=100, mode=0)
+    S = dv.PcgSolver(dv.DeviceMatrix(L), n_all=case.n_owned, mode="fixed", maxit=100)
+    x = _t(np.zeros(case.n_owned))
+    S.solve(_t(b), x, _t(x0))
+    got = x.cpu().numpy()
+    assert np.array_equal(got[L.nrows:], x0[L.nrows:])  # ghosts keep x0 (GIP_LinearSolver.h:67)
+    assert np.abs(got - xr).max() / np.abs(xr).max() < 1e-10
+
+
+@pytest.mark.parametrize("n,tol", [(12, 1e-6), (20, 1e-8)])
+def test_pcg_tol_iterations_within_one(gpu, oracle_mod, n, tol):
+    from gip_b200 import device as dv
+    L, b = cavity.poisson_problem(n, seed=3)
+    x0 = np.zeros(L.nrows)
+    xr, it, rr = oracle_mod.pcg(L, b, x0, maxit=5000, mode=1, tol=tol)
+    S = dv.PcgSolver(dv.DeviceMatrix(L), mode="tol", maxit=5000, tol=tol)
+    x = _t(np.zeros(L.nrows))
+    res = S.solve(_t(b), x, _t(x0))
+    assert res["status"] == 0
+    assert abs(res["iterations"] - it) <= 1, (res["iterations"], it)
+    r = b - L.to_scipy() @ x.cpu().numpy()
+    assert np.linalg.norm(r) <= 1.5 * tol * np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("n,tol", [(16, 1e-6), (24, 1e-8)])
+def test_pcg_mixed_reaches_fp64_tolerance(gpu, oracle_mod, n, tol):
+    from gip_b200 import device as dv
+    L, b = cavity.poisson_problem(n, seed=4)
+    S = dv.PcgSolver(dv.DeviceMatrix(L), mode="mixed", maxit=5000, tol=tol, inner_tol=1e-3,
+                     inner_maxit=2000, max_outer=40)
+    x = _t(np.zeros(L.nrows))
+    res = S.solve(_t(b), x, _t(np.zeros(L.nrows)))
+    assert res["status"] == 0, res
+    xs = x.cpu().numpy()
+    r = b - L.to_scipy() @ xs
+    assert np.linalg.norm(r) <= tol * np.linalg.norm(b) * 1.0001
+    # against the FP64 oracle solved tighter: solution error is bounded by conditioning
+    xr, _, _ = oracle_mod.pcg(L, b, np.zeros(L.nrows), maxit=20000, mode=1, tol=1e-13)
+    assert np.abs(xs - xr).max() / np.abs(xr).max() < 1e4 * tol
