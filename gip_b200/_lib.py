@@ -44,7 +44,7 @@ class PcgResult(C.Structure):
 
 class DnsParams(C.Structure):
     _fields_ = [("rho", C.c_double), ("gamma", C.c_double), ("pcg", PcgParams),
-                ("use_graph", C.c_int)]
+                ("use_graph", C.c_int), ("reorder", C.c_int)]
 
 
 PCG_FIXED, PCG_TOL, PCG_MIXED = 0, 1, 2
@@ -63,6 +63,10 @@ _SIGNATURES = {
     "gipb200_memcpy_d2h": (_I, [_VP, _VP, C.c_size_t, _VP]),
     "gipb200_dcopy": (_I, [_I, _VP, _VP, _VP]),
     "gipb200_stream_sync": (_I, [_VP]),
+    "gipb200_event_create": (_I, [C.POINTER(_VP)]),
+    "gipb200_event_record": (_I, [_VP, _VP]),
+    "gipb200_event_elapsed_ms": (_I, [_VP, _VP, C.POINTER(C.c_float)]),
+    "gipb200_event_destroy": (_I, [_VP]),
     "gipb200_dcsr_spmv": (_I, [_I, _VP, _VP, _VP, _VP, _VP, _D, _D, _I, _VP]),
     "gipb200_daxpy": (_I, [_I, _VP, _VP, _D, _VP]),
     "gipb200_daxpby": (_I, [_I, _VP, _VP, _D, _D, _VP]),
@@ -88,6 +92,7 @@ _SIGNATURES = {
     "gipb200_dns_history": (_I, [_VP, C.POINTER(_I), _VP, _VP, _VP, _VP, _VP]),
     "gipb200_dns_get_field": (_I, [_VP, C.c_char_p, _VP, _I]),
     "gipb200_dns_field_ptr": (_I, [_VP, C.c_char_p, C.POINTER(_VP), C.POINTER(_I)]),
+    "gipb200_dns_copy_field": (_I, [_VP, C.c_char_p, _VP, _I, _VP]),
     "gipb200_dns_scalars": (_I, [_VP, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
     "gipb200_dns_set_field": (_I, [_VP, C.c_char_p, _VP, _I, _I, _VP]),
     "gipb200_dns_launch_count": (_I, [_VP, C.POINTER(C.c_longlong)]),

@@ -108,6 +108,7 @@ int sell_build(Sell* S, int nrows, int ncols, int nnz, const int* rp, const int*
   std::vector<int> scol((size_t)std::max<long long>(S->nslots, 1), -1);
   std::vector<double> sval((size_t)std::max<long long>(S->nslots, 1), 0.0);
   std::vector<int> pos((size_t)std::max(nnz, 1), 0);
+#pragma omp parallel for schedule(static)
   for (int r = 0; r < nrows; ++r) {
     int s = r >> 5, lane = r & 31;
     for (int k = rp[r]; k < rp[r + 1]; ++k) {
@@ -365,6 +366,28 @@ int gipb200_dcopy(int n, double* d_dst, const double* d_src, void* stream) {
 }
 int gipb200_stream_sync(void* stream) {
   GIPB_CUDA(cudaStreamSynchronize(as_stream(stream)));
+  return GIPB200_OK;
+}
+
+int gipb200_event_create(void** ev) {
+  if (!ev) return fail(GIPB200_ERR_ARG, "null output");
+  cudaEvent_t e;
+  GIPB_CUDA(cudaEventCreate(&e));
+  *ev = (void*)e;
+  return GIPB200_OK;
+}
+int gipb200_event_record(void* ev, void* stream) {
+  GIPB_CUDA(cudaEventRecord((cudaEvent_t)ev, as_stream(stream)));
+  return GIPB200_OK;
+}
+int gipb200_event_elapsed_ms(void* a, void* b, float* ms) {
+  if (!ms) return fail(GIPB200_ERR_ARG, "null output");
+  GIPB_CUDA(cudaEventSynchronize((cudaEvent_t)b));
+  GIPB_CUDA(cudaEventElapsedTime(ms, (cudaEvent_t)a, (cudaEvent_t)b));
+  return GIPB200_OK;
+}
+int gipb200_event_destroy(void* ev) {
+  GIPB_CUDA(cudaEventDestroy((cudaEvent_t)ev));
   return GIPB200_OK;
 }
 

@@ -345,6 +345,10 @@ struct Dns {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int blocks_cells = 1, blocks_faces = 1, blocks_owned = 1, blocks_vec = 1;
+  // internal renumbering (reorder): external index e lives at internal perm[e]
+  bool reordered = false;
+  DevBuf<int> perm_c, perm_f;
+  DevBuf<double> staging;
   long long launches = 0;        // kernels launched (graph launches count their kernels)
   long long graph_kernels = 0;   // kernels in the captured step graph
 
@@ -457,6 +461,87 @@ double* Dns::field(const std::string& name, int* n) {
   return nullptr;
 }
 
+// ------------------------------------------------------------------ locality renumbering
+struct OwnedCsr {
+  int nrows = 0, ncols = 0;
+  std::vector<int> rp, col;
+  std::vector<double> val;
+  gipb200_host_csr view() const {
+    gipb200_host_csr h;
+    h.nrows = nrows;
+    h.ncols = ncols;
+    h.nnz = (int)col.size();
+    h.rowptr = rp.data();
+    h.col = col.data();
+    h.val = val.data();
+    return h;
+  }
+};
+
+// Breadth-first order of the inner cells over L's graph, started from the last cell
+// reached by a first sweep (a pseudo-peripheral cell), neighbours in stored order.
+static void bfs_sweep(const gipb200_host_csr& L, int N, int start, std::vector<int>& order,
+                      std::vector<char>& seen) {
+  size_t head = order.size();
+  order.push_back(start);
+  seen[start] = 1;
+  while (head < order.size()) {
+    const int i = order[head++];
+    if (i >= L.nrows) continue;
+    for (int k = L.rowptr[i]; k < L.rowptr[i + 1]; ++k) {
+      const int j = L.col[k];
+      if (j >= 0 && j < N && !seen[j]) {
+        seen[j] = 1;
+        order.push_back(j);
+      }
+    }
+  }
+}
+
+static std::vector<int> bfs_cells(const gipb200_host_csr& L, int N) {
+  std::vector<int> order;
+  order.reserve(N);
+  std::vector<char> seen(N, 0);
+  bfs_sweep(L, N, 0, order, seen);
+  const int start = order.back();
+  order.clear();
+  std::fill(seen.begin(), seen.end(), 0);
+  bfs_sweep(L, N, start, order, seen);
+  for (int i = 0; i < N; ++i)
+    if (!seen[i]) bfs_sweep(L, N, i, order, seen);
+  return order;  // new -> old
+}
+
+// out row r = m row src[r] (src is a permutation of m's rows); columns through cmap
+static void permute_rows(const gipb200_host_csr& m, const int* src, const int* cmap,
+                         OwnedCsr* out) {
+  out->nrows = m.nrows;
+  out->ncols = m.ncols;
+  out->rp.assign((size_t)m.nrows + 1, 0);
+  for (int r = 0; r < m.nrows; ++r) out->rp[r + 1] = out->rp[r] + (m.rowptr[src[r] + 1] - m.rowptr[src[r]]);
+  out->col.resize((size_t)m.nnz);
+  out->val.resize((size_t)m.nnz);
+#pragma omp parallel for schedule(static)
+  for (int r = 0; r < m.nrows; ++r) {
+    int o = out->rp[r];
+    for (int k = m.rowptr[src[r]]; k < m.rowptr[src[r] + 1]; ++k, ++o) {
+      out->col[o] = cmap ? cmap[m.col[k]] : m.col[k];
+      out->val[o] = m.val ? m.val[k] : 0.0;
+    }
+  }
+}
+
+__global__ void k_gather_field(int n, const int* __restrict__ perm, const double* __restrict__ in,
+                               double* __restrict__ out) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+    out[e] = in[perm[e]];
+}
+__global__ void k_scatter_field(int n, int offset, const int* __restrict__ perm,
+                                const double* __restrict__ in, double* __restrict__ out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    out[perm[offset + k]] = in[k];
+}
+
 static int check_op(const gipb200_host_csr& m, const char* name, int rows_max, int col_bound) {
   if (m.nrows > rows_max)
     return fail(GIPB200_ERR_ARG, "%s: %d rows exceed %d", name, m.nrows, rows_max);
@@ -513,21 +598,117 @@ int gipb200_dns_create(const gipb200_dns_ops* ops, const double* h_u, const doub
     E.NO = NO;
     E.NF = NF;
     E.prm = *prm;
-    GIPB_TRY(build_op(&E.D, ops->D));
-    GIPB_TRY(build_op(&E.Ec, ops->Ec));
-    GIPB_TRY(build_op(&E.L, ops->L));
-    GIPB_TRY(build_op(&E.Lb, ops->Lb));
-    GIPB_TRY(build_op(&E.Mx, ops->Mx));
-    GIPB_TRY(build_op(&E.My, ops->My));
-    GIPB_TRY(build_op(&E.Mz, ops->Mz));
-    GIPB_TRY(build_op(&E.Mres, ops->Mres));
-    GIPB_TRY(build_op(&E.Gx, ops->Gx));
-    GIPB_TRY(build_op(&E.Gy, ops->Gy));
-    GIPB_TRY(build_op(&E.Gz, ops->Gz));
-    GIPB_TRY(build_op(&E.SFx, ops->SFx));
-    GIPB_TRY(build_op(&E.SFy, ops->SFy));
-    GIPB_TRY(build_op(&E.SFz, ops->SFz));
-    GIPB_TRY(build_op(&E.SO, ops->SO));
+    // Renumbering needs every operator's row space complete (cell rows: 0, N or NO rows;
+    // face rows: 0 or NF rows), which GIP's operators satisfy at one rank.
+    const gipb200_host_csr* all_ops[] = {&ops->D, &ops->L, &ops->Lb, &ops->Mx, &ops->My,
+                                         &ops->Mz, &ops->Mres, &ops->Gx, &ops->Gy, &ops->Gz,
+                                         &ops->SFx, &ops->SFy, &ops->SFz, &ops->SO};
+    bool can_reorder = prm->reorder != 0 && ops->D.nrows == N;
+    for (int k = 0; k < 10; ++k) {
+      const int r = all_ops[k]->nrows;
+      can_reorder = can_reorder && (r == 0 || r == N || r == NO);
+    }
+    for (int k = 10; k < 14; ++k) can_reorder = can_reorder && (all_ops[k]->nrows == 0 || all_ops[k]->nrows == NF);
+    gipb200_dns_ops rops = *ops;
+    OwnedCsr own[15];
+    std::vector<double> fu, fv, fw, fdx;
+    const double *pu = h_u, *pv = h_v, *pw = h_w, *pdx = h_dxs;
+    if (can_reorder) {
+      std::vector<int> inv_c = bfs_cells(ops->L, N);  // new -> old (inner)
+      inv_c.resize(NO);
+      for (int g = N; g < NO; ++g) inv_c[g] = g;
+      std::vector<int> perm_c(NO);
+      for (int r = 0; r < NO; ++r) perm_c[inv_c[r]] = r;
+      // faces ordered by the first (renumbered) inner cell that has them
+      std::vector<long long> key(NF);
+      for (int f = 0; f < NF; ++f) key[f] = (long long)NO * NF + f;
+      for (int i = 0; i < ops->Mres.nrows; ++i)
+        for (int k = ops->Mres.rowptr[i]; k < ops->Mres.rowptr[i + 1]; ++k) {
+          const int f = ops->Mres.col[k];
+          const long long kk = (long long)perm_c[i] * NF + f;
+          if (kk < key[f]) key[f] = kk;
+        }
+      std::vector<int> inv_f(NF);
+      for (int f = 0; f < NF; ++f) inv_f[f] = f;
+      std::sort(inv_f.begin(), inv_f.end(), [&](int a, int b) { return key[a] < key[b]; });
+      std::vector<int> perm_f(NF);
+      for (int r = 0; r < NF; ++r) perm_f[inv_f[r]] = r;
+      auto cell_op = [&](const gipb200_host_csr& m, OwnedCsr* o, bool face_cols) {
+        permute_rows(m, inv_c.data(), face_cols ? perm_f.data() : perm_c.data(), o);
+      };
+      auto face_op = [&](const gipb200_host_csr& m, OwnedCsr* o) {
+        permute_rows(m, inv_f.data(), perm_c.data(), o);
+      };
+      cell_op(ops->D, &own[0], false);
+      cell_op(ops->L, &own[1], false);
+      cell_op(ops->Lb, &own[2], false);
+      cell_op(ops->Mx, &own[3], false);
+      cell_op(ops->My, &own[4], false);
+      cell_op(ops->Mz, &own[5], false);
+      cell_op(ops->Mres, &own[6], true);
+      cell_op(ops->Gx, &own[7], false);
+      cell_op(ops->Gy, &own[8], false);
+      cell_op(ops->Gz, &own[9], false);
+      face_op(ops->SFx, &own[10]);
+      face_op(ops->SFy, &own[11]);
+      face_op(ops->SFz, &own[12]);
+      face_op(ops->SO, &own[13]);
+      // Ec rows follow the renumbered D's nonzeros, each kept in its stored order
+      std::vector<int> ec_src;
+      ec_src.reserve((size_t)ops->D.nnz);
+      for (int r = 0; r < N; ++r)
+        for (int k = ops->D.rowptr[inv_c[r]]; k < ops->D.rowptr[inv_c[r] + 1]; ++k) ec_src.push_back(k);
+      permute_rows(ops->Ec, ec_src.data(), perm_f.data(), &own[14]);
+      rops.D = own[0].view();
+      rops.L = own[1].view();
+      rops.Lb = own[2].view();
+      rops.Mx = own[3].view();
+      rops.My = own[4].view();
+      rops.Mz = own[5].view();
+      rops.Mres = own[6].view();
+      rops.Gx = own[7].view();
+      rops.Gy = own[8].view();
+      rops.Gz = own[9].view();
+      rops.SFx = own[10].view();
+      rops.SFy = own[11].view();
+      rops.SFz = own[12].view();
+      rops.SO = own[13].view();
+      rops.Ec = own[14].view();
+      fu.resize(NO);
+      fv.resize(NO);
+      fw.resize(NO);
+      fdx.resize(NO);
+      for (int e = 0; e < NO; ++e) {
+        fu[perm_c[e]] = h_u[e];
+        fv[perm_c[e]] = h_v[e];
+        fw[perm_c[e]] = h_w[e];
+        fdx[perm_c[e]] = h_dxs[e];
+      }
+      pu = fu.data();
+      pv = fv.data();
+      pw = fw.data();
+      pdx = fdx.data();
+      GIPB_TRY(E.perm_c.upload(perm_c.data(), NO));
+      GIPB_TRY(E.perm_f.upload(perm_f.data(), std::max(NF, 1)));
+      GIPB_TRY(E.staging.alloc(std::max(NO, NF)));
+      E.reordered = true;
+    }
+    const gipb200_dns_ops* bops = &rops;
+    GIPB_TRY(build_op(&E.D, bops->D));
+    GIPB_TRY(build_op(&E.Ec, bops->Ec));
+    GIPB_TRY(build_op(&E.L, bops->L));
+    GIPB_TRY(build_op(&E.Lb, bops->Lb));
+    GIPB_TRY(build_op(&E.Mx, bops->Mx));
+    GIPB_TRY(build_op(&E.My, bops->My));
+    GIPB_TRY(build_op(&E.Mz, bops->Mz));
+    GIPB_TRY(build_op(&E.Mres, bops->Mres));
+    GIPB_TRY(build_op(&E.Gx, bops->Gx));
+    GIPB_TRY(build_op(&E.Gy, bops->Gy));
+    GIPB_TRY(build_op(&E.Gz, bops->Gz));
+    GIPB_TRY(build_op(&E.SFx, bops->SFx));
+    GIPB_TRY(build_op(&E.SFy, bops->SFy));
+    GIPB_TRY(build_op(&E.SFz, bops->SFz));
+    GIPB_TRY(build_op(&E.SO, bops->SO));
     // C starts with D's values (C.postConstruct reads the D file, GIP_DNS.h:151)
     GIPB_TRY(E.cval.alloc((size_t)std::max<long long>(E.D.nslots, 1)));
     GIPB_CUDA(cudaMemcpy(E.cval.p, E.D.val.p, E.cval.n * 8, cudaMemcpyDeviceToDevice));
@@ -539,10 +720,10 @@ int gipb200_dns_create(const gipb200_dns_ops* ops, const double* h_u, const doub
     }
     GIPB_TRY(E.mf.alloc(std::max(NF, 1)));
     GIPB_TRY(E.mf.zero());
-    GIPB_CUDA(cudaMemcpy(E.u.p, h_u, (size_t)NO * 8, cudaMemcpyHostToDevice));
-    GIPB_CUDA(cudaMemcpy(E.v.p, h_v, (size_t)NO * 8, cudaMemcpyHostToDevice));
-    GIPB_CUDA(cudaMemcpy(E.w.p, h_w, (size_t)NO * 8, cudaMemcpyHostToDevice));
-    GIPB_CUDA(cudaMemcpy(E.dxs.p, h_dxs, (size_t)NO * 8, cudaMemcpyHostToDevice));
+    GIPB_CUDA(cudaMemcpy(E.u.p, pu, (size_t)NO * 8, cudaMemcpyHostToDevice));
+    GIPB_CUDA(cudaMemcpy(E.v.p, pv, (size_t)NO * 8, cudaMemcpyHostToDevice));
+    GIPB_CUDA(cudaMemcpy(E.w.p, pw, (size_t)NO * 8, cudaMemcpyHostToDevice));
+    GIPB_CUDA(cudaMemcpy(E.dxs.p, pdx, (size_t)NO * 8, cudaMemcpyHostToDevice));
     GIPB_TRY(E.pcg.init(&E.L, NO, prm->pcg, 0));
     GIPB_TRY(E.sc.alloc(1));
     GIPB_TRY(E.sc.zero());
@@ -578,8 +759,9 @@ int gipb200_dns_advance(gipb200_dns Dh, int nsteps, void* stream) {
     GIPB_TRY(E.enqueue_initial_dt(s));
     E.started = true;
   }
-  // A graph needs a host-free step: FIXED mode, or TOL/MIXED run to their caps.
-  const bool graphable = E.prm.use_graph && E.prm.pcg.mode == GIPB200_PCG_FIXED;
+  // Every mode is graphable: FIXED unrolls its iterations, TOL/MIXED loop in
+  // conditional while-nodes that the device stops.
+  const bool graphable = E.prm.use_graph != 0;
   for (int k = 0; k < nsteps; ++k) {
     if (graphable) {
       if (!E.exec) {
@@ -634,8 +816,39 @@ int gipb200_dns_get_field(gipb200_dns Dh, const char* name, double* h_out, int n
   double* p = Dh->E.field(name, &sz);
   if (!p) return fail(GIPB200_ERR_ARG, "unknown field '%s'", name);
   if (n < sz) return fail(GIPB200_ERR_ARG, "buffer of %d for field of %d", n, sz);
+  Dns& E = Dh->E;
   GIPB_CUDA(cudaDeviceSynchronize());
+  if (E.reordered && sz > 0) {
+    const int* perm = (sz == E.NF && std::string(name) == "mf") ? E.perm_f.p : E.perm_c.p;
+    int b;
+    GIPB_TRY(grid_blocks(256, sz, 4, 0, &b));
+    k_gather_field<<<b, 256>>>(sz, perm, p, E.staging.p);
+    GIPB_LAUNCH_CHECK();
+    GIPB_CUDA(cudaMemcpy(h_out, E.staging.p, (size_t)sz * 8, cudaMemcpyDeviceToHost));
+    return GIPB200_OK;
+  }
   GIPB_CUDA(cudaMemcpy(h_out, p, (size_t)sz * 8, cudaMemcpyDeviceToHost));
+  return GIPB200_OK;
+}
+
+int gipb200_dns_copy_field(gipb200_dns Dh, const char* name, double* d_out, int n, void* stream) {
+  if (!Dh || !name || !d_out) return fail(GIPB200_ERR_ARG, "null argument");
+  int sz = 0;
+  double* p = Dh->E.field(name, &sz);
+  if (!p) return fail(GIPB200_ERR_ARG, "unknown field '%s'", name);
+  if (n < sz) return fail(GIPB200_ERR_ARG, "buffer of %d for field of %d", n, sz);
+  Dns& E = Dh->E;
+  cudaStream_t s = as_stream(stream);
+  if (sz == 0) return GIPB200_OK;
+  if (E.reordered) {
+    const int* perm = (std::string(name) == "mf") ? E.perm_f.p : E.perm_c.p;
+    int b;
+    GIPB_TRY(grid_blocks(256, sz, 4, 0, &b));
+    k_gather_field<<<b, 256, 0, s>>>(sz, perm, p, d_out);
+    GIPB_LAUNCH_CHECK();
+  } else {
+    GIPB_CUDA(cudaMemcpyAsync(d_out, p, (size_t)sz * 8, cudaMemcpyDeviceToDevice, s));
+  }
   return GIPB200_OK;
 }
 
@@ -657,9 +870,19 @@ int gipb200_dns_set_field(gipb200_dns Dh, const char* name, const double* h_in, 
   if (!p) return fail(GIPB200_ERR_ARG, "unknown field '%s'", name);
   if (offset < 0 || n < 0 || (long long)offset + n > sz)
     return fail(GIPB200_ERR_ARG, "range [%d,%d) outside field of %d", offset, offset + n, sz);
-  if (n)
-    GIPB_CUDA(cudaMemcpyAsync(p + offset, h_in, (size_t)n * 8, cudaMemcpyHostToDevice,
-                              as_stream(stream)));
+  if (!n) return GIPB200_OK;
+  Dns& E = Dh->E;
+  cudaStream_t s = as_stream(stream);
+  if (E.reordered) {
+    const int* perm = (std::string(name) == "mf") ? E.perm_f.p : E.perm_c.p;
+    GIPB_CUDA(cudaMemcpyAsync(E.staging.p, h_in, (size_t)n * 8, cudaMemcpyHostToDevice, s));
+    int b;
+    GIPB_TRY(grid_blocks(256, n, 4, 0, &b));
+    k_scatter_field<<<b, 256, 0, s>>>(n, offset, perm, E.staging.p, p);
+    GIPB_LAUNCH_CHECK();
+  } else {
+    GIPB_CUDA(cudaMemcpyAsync(p + offset, h_in, (size_t)n * 8, cudaMemcpyHostToDevice, s));
+  }
   return GIPB200_OK;
 }
 

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "device.cuh"
@@ -32,10 +33,17 @@
 namespace gipb200 {
 
 // ------------------------------------------------------------------ FP64 kernels
+// A while-node condition is set by the kernel that decides it: value = keep looping.
+__device__ __forceinline__ void set_loop(int use, cudaGraphConditionalHandle h, int keep) {
+  if (use) cudaGraphSetConditional(h, keep ? 1u : 0u);
+}
+
 struct PcgInitFinish {
   PcgScalars* S;
   int mode, maxit;
   double tol;
+  int use_cond;
+  cudaGraphConditionalHandle cond;
   __device__ void operator()(const double* t) const {
     S->rz = t[0];
     S->rr = t[1];
@@ -44,6 +52,7 @@ struct PcgInitFinish {
     S->status = GIPB200_OK;
     S->done = (maxit <= 0) ? 1 : 0;
     if (mode == GIPB200_PCG_TOL && !(sqrt(t[1]) > tol * sqrt(t[2]))) S->done = 1;
+    set_loop(use_cond, cond, !S->done);
   }
 };
 
@@ -54,7 +63,8 @@ __global__ void __launch_bounds__(256) k_pcg_init(SellView<double> L, const doub
                                                   double* __restrict__ r, double* __restrict__ p,
                                                   double* __restrict__ Ap, PcgScalars* S,
                                                   ReduceScratch rs, int mode, int maxit,
-                                                  double tol) {
+                                                  double tol, int use_cond,
+                                                  cudaGraphConditionalHandle cond) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -77,7 +87,7 @@ __global__ void __launch_bounds__(256) k_pcg_init(SellView<double> L, const doub
       acc[2] = dadd(acc[2], dmul(bi, bi));
     }
   }
-  grid_reduce<SumOp, 3>(acc, rs, PcgInitFinish{S, mode, maxit, tol});
+  grid_reduce<SumOp, 3>(acc, rs, PcgInitFinish{S, mode, maxit, tol, use_cond, cond});
 }
 
 struct AlphaFinish {
@@ -162,7 +172,9 @@ __global__ void __launch_bounds__(256) k_pcg_update(int n, double* __restrict__ 
 __global__ void __launch_bounds__(256) k_pcg_pupdate(int n, double* __restrict__ p,
                                                      const double* __restrict__ r,
                                                      const double* __restrict__ dinv,
-                                                     const PcgScalars* S) {
+                                                     const PcgScalars* S, int use_cond,
+                                                     cudaGraphConditionalHandle cond) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(use_cond, cond, !S->done);
   if (S->done) return;
   const double beta = S->beta;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -181,6 +193,8 @@ struct OuterFinish {
   const double* scale;
   float* r32;
   float* p32;
+  int use_cond;
+  cudaGraphConditionalHandle inner_cond;
   __device__ void operator()(const double* t) const {
     // t[0] = r.r (FP64, true residual), t[1] = scaled r^.r^, t[2] = b.b, t[3] = sum(r)
     if (S->outer == 0) S->bb = t[2];
@@ -209,6 +223,7 @@ struct OuterFinish {
       S->outer += 1;
       S->inner_done = 0;
     }
+    set_loop(use_cond, inner_cond, !S->inner_done);
   }
 };
 
@@ -220,7 +235,9 @@ __global__ void __launch_bounds__(256) k_mx_residual(SellView<double> L, const d
                                                      float* __restrict__ r32, float* __restrict__ p32,
                                                      float* __restrict__ y32, PcgScalars* S,
                                                      ReduceScratch rs, double tol, double inner_tol,
-                                                     int max_outer, int pin_row, double pin_val) {
+                                                     int max_outer, int pin_row, double pin_val,
+                                                     int use_cond,
+                                                     cudaGraphConditionalHandle inner_cond) {
   if (S->done) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -246,7 +263,8 @@ __global__ void __launch_bounds__(256) k_mx_residual(SellView<double> L, const d
     }
   }
   grid_reduce<SumOp, 4>(acc, rs,
-                        OuterFinish{S, tol, inner_tol, max_outer, pin_row, pin_val, scale, r32, p32});
+                        OuterFinish{S, tol, inner_tol, max_outer, pin_row, pin_val, scale, r32, p32,
+                                    use_cond, inner_cond});
 }
 
 struct AlphaFinish32 {
@@ -309,7 +327,9 @@ __global__ void __launch_bounds__(256) k_mx_update(int n, float* __restrict__ y,
 
 __global__ void __launch_bounds__(256) k_mx_pupdate(int n, float* __restrict__ p,
                                                     const float* __restrict__ r,
-                                                    const PcgScalars* S) {
+                                                    const PcgScalars* S, int use_cond,
+                                                    cudaGraphConditionalHandle inner_cond) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(use_cond, inner_cond, !S->inner_done);
   if (S->inner_done) return;
   const float beta = (float)S->beta;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -320,7 +340,9 @@ __global__ void __launch_bounds__(256) k_mx_pupdate(int n, float* __restrict__ p
 __global__ void __launch_bounds__(256) k_mx_correct(int n, double* __restrict__ x,
                                                     const float* __restrict__ y,
                                                     const double* __restrict__ scale,
-                                                    const PcgScalars* S, int pin_row) {
+                                                    const PcgScalars* S, int pin_row, int use_cond,
+                                                    cudaGraphConditionalHandle outer_cond) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(use_cond, outer_cond, !S->done);
   if (S->done) return;
   const double kappa = (pin_row >= 0) ? S->kappa_c - scale[pin_row] * (double)y[pin_row] : 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -380,6 +402,8 @@ __global__ void k_pcg_inv_diag(int nrows, const int* __restrict__ rp, const int*
 // ------------------------------------------------------------------ host side
 Pcg::~Pcg() {
   if (h_sc) cudaFreeHost(h_sc);
+  for (auto& bs : body_stream)
+    if (bs) cudaStreamDestroy(bs);
 }
 
 int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaStream_t s) {
@@ -402,6 +426,7 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
   GIPB_TRY(sc.alloc(1));
   GIPB_TRY(sc.zero(s));
   GIPB_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_sc), sizeof(PcgScalars)));
+  for (auto& bs : body_stream) GIPB_CUDA(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
   GIPB_TRY(grid_blocks(256, L->nslices * 32, 1, kMaxReduceBlocks, &blocks_spmv));
   GIPB_TRY(grid_blocks(256, std::max(n, 1), 4, kMaxReduceBlocks, &blocks_vec));
   if (prm.mode == GIPB200_PCG_MIXED) {
@@ -473,9 +498,132 @@ int Pcg::read_flag(cudaStream_t s, int which, int* v) {
   return GIPB200_OK;
 }
 
+// ------------------------------------------------------------------ conditional while-nodes
+static bool capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess) return false;
+  return st == cudaStreamCaptureStatusActive;
+}
+
+static int make_handle(cudaStream_t cs, unsigned def, unsigned flags,
+                       cudaGraphConditionalHandle* h) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  GIPB_CUDA(cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, nullptr, nullptr));
+  if (st != cudaStreamCaptureStatusActive || !g)
+    return fail(GIPB200_ERR_STATE, "stream is not capturing");
+  GIPB_CUDA(cudaGraphConditionalHandleCreate(h, g, def, flags));
+  return GIPB200_OK;
+}
+
+// Appends a while-node after everything captured so far on `cs`; returns its body graph
+// and makes the node the capture frontier of `cs`.
+static int add_while(cudaStream_t cs, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  GIPB_CUDA(cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd));
+  // the parameter union has no default constructor: zeroed raw storage
+  alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+  memset(raw, 0, sizeof(raw));
+  cudaGraphNodeParams& p = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  GIPB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+  *body = p.conditional.phGraph_out[0];
+  GIPB_CUDA(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
+  return GIPB200_OK;
+}
+
 int Pcg::enqueue(const double* b, double* x, const double* x0, cudaStream_t s, bool host_sync) {
+  if (!host_sync && prm.mode != GIPB200_PCG_FIXED && capturing(s)) {
+    if (!body_stream[0]) {
+      return fail(GIPB200_ERR_STATE, "capture streams missing");
+    }
+    return prm.mode == GIPB200_PCG_MIXED ? enqueue_mixed_graph(b, x, x0, s)
+                                         : enqueue_fp64_graph(b, x, x0, s);
+  }
   if (prm.mode == GIPB200_PCG_MIXED) return enqueue_mixed(b, x, x0, s, host_sync);
   return enqueue_fp64(b, x, x0, s, host_sync);
+}
+
+// TOL mode inside a graph: init, then while(!done) { A; B; C }.  C sets the loop value
+// from the stop flag; the flag is set by a convergence test or the maxit cap, so the
+// loop always ends.
+int Pcg::enqueue_fp64_graph(const double* b, double* x, const double* x0, cudaStream_t s) {
+  cudaGraphConditionalHandle h;
+  GIPB_TRY(make_handle(s, 0, 0, &h));
+  if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
+  GIPB_CUDA(cudaMemcpyAsync(p.p, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
+  if (n > 0) GIPB_CUDA(cudaMemcpyAsync(Ap.p, x0, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+  k_pcg_init<<<blocks_spmv, 256, 0, s>>>(L->view(), x, b, dinv.p, r.p, p.p, Ap.p, sc.p, rs,
+                                          prm.mode, prm.maxit, prm.tol, 1, h);
+  GIPB_LAUNCH_CHECK();
+  cudaGraph_t body;
+  GIPB_TRY(add_while(s, h, &body));
+  cudaStream_t bs = body_stream[0];
+  GIPB_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed));
+  k_pcg_spmv_dot<<<blocks_spmv, 256, 0, bs>>>(L->view(), p.p, Ap.p, sc.p, rs, prm.mode);
+  k_pcg_update<<<blocks_vec, 256, 0, bs>>>(n, x, r.p, p.p, Ap.p, dinv.p, sc.p, rs, prm.mode,
+                                            prm.maxit, prm.tol);
+  k_pcg_pupdate<<<blocks_vec, 256, 0, bs>>>(n, p.p, r.p, dinv.p, sc.p, 1, h);
+  cudaError_t le = cudaGetLastError();
+  cudaGraph_t out = nullptr;
+  GIPB_CUDA(cudaStreamEndCapture(bs, &out));
+  if (le != cudaSuccess) return fail(GIPB200_ERR_CUDA, "launch in loop body: %s", cudaGetErrorString(le));
+  launches += 4;
+  return GIPB200_OK;
+}
+
+// MIXED inside a graph:
+//   while(!done) { residual (sets done / inner_done); while(!inner_done) { A; B; C };
+//                  correct (sets the outer loop value) }
+int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaStream_t s) {
+  cudaGraphConditionalHandle ho;
+  GIPB_TRY(make_handle(s, 1, cudaGraphCondAssignDefault, &ho));
+  if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
+  GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
+  cudaGraph_t outer_body;
+  GIPB_TRY(add_while(s, ho, &outer_body));
+  const SellView<float> A{L->nrows, L->nslices, L->sptr.p, L->col.p, lhat.p};
+  cudaStream_t os = body_stream[0], is = body_stream[1];
+  GIPB_CUDA(cudaStreamBeginCaptureToGraph(os, outer_body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed));
+  int st = [&]() -> int {
+    cudaGraphConditionalHandle hi;
+    GIPB_TRY(make_handle(os, 0, 0, &hi));
+    k_mx_residual<<<blocks_spmv, 256, 0, os>>>(L->view(), x, b, scale.p, rtrue.p, r32.p, p32.p,
+                                                y32.p, sc.p, rs, prm.tol, prm.inner_tol,
+                                                prm.max_outer, pin_row, pin_val, 1, hi);
+    GIPB_LAUNCH_CHECK();
+    cudaGraph_t inner_body;
+    GIPB_TRY(add_while(os, hi, &inner_body));
+    GIPB_CUDA(cudaStreamBeginCaptureToGraph(is, inner_body, nullptr, nullptr, 0,
+                                            cudaStreamCaptureModeRelaxed));
+    k_mx_spmv_dot<<<blocks_spmv, 256, 0, is>>>(A, p32.p, Ap32.p, sc.p, rs);
+    k_mx_update<<<blocks_vec, 256, 0, is>>>(n, y32.p, r32.p, p32.p, Ap32.p, sc.p, rs,
+                                             prm.inner_maxit);
+    k_mx_pupdate<<<blocks_vec, 256, 0, is>>>(n, p32.p, r32.p, sc.p, 1, hi);
+    cudaError_t le = cudaGetLastError();
+    cudaGraph_t out = nullptr;
+    GIPB_CUDA(cudaStreamEndCapture(is, &out));
+    if (le != cudaSuccess)
+      return fail(GIPB200_ERR_CUDA, "launch in inner body: %s", cudaGetErrorString(le));
+    k_mx_correct<<<blocks_vec, 256, 0, os>>>(n, x, y32.p, scale.p, sc.p, pin_row, 1, ho);
+    GIPB_LAUNCH_CHECK();
+    return GIPB200_OK;
+  }();
+  cudaGraph_t out = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(os, &out);
+  if (st != GIPB200_OK) return st;
+  if (ce != cudaSuccess) return fail(GIPB200_ERR_CUDA, "outer body capture: %s", cudaGetErrorString(ce));
+  launches += 5;
+  return GIPB200_OK;
 }
 
 int Pcg::enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t s,
@@ -485,7 +633,7 @@ int Pcg::enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t
   GIPB_CUDA(cudaMemcpyAsync(p.p, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   if (n > 0) GIPB_CUDA(cudaMemcpyAsync(Ap.p, x0, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
   k_pcg_init<<<blocks_spmv, 256, 0, s>>>(L->view(), x, b, dinv.p, r.p, p.p, Ap.p, sc.p, rs,
-                                          prm.mode, prm.maxit, prm.tol);
+                                          prm.mode, prm.maxit, prm.tol, 0, 0);
   GIPB_LAUNCH_CHECK();
   launches += 1;
   const int poll = 16;
@@ -493,7 +641,7 @@ int Pcg::enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t
     k_pcg_spmv_dot<<<blocks_spmv, 256, 0, s>>>(L->view(), p.p, Ap.p, sc.p, rs, prm.mode);
     k_pcg_update<<<blocks_vec, 256, 0, s>>>(n, x, r.p, p.p, Ap.p, dinv.p, sc.p, rs, prm.mode,
                                              prm.maxit, prm.tol);
-    k_pcg_pupdate<<<blocks_vec, 256, 0, s>>>(n, p.p, r.p, dinv.p, sc.p);
+    k_pcg_pupdate<<<blocks_vec, 256, 0, s>>>(n, p.p, r.p, dinv.p, sc.p, 0, 0);
     GIPB_LAUNCH_CHECK();
     launches += 3;
     if (host_sync && prm.mode != GIPB200_PCG_FIXED && (k + 1) % poll == 0) {
@@ -514,7 +662,7 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
   for (int o = 0; o <= prm.max_outer; ++o) {
     k_mx_residual<<<blocks_spmv, 256, 0, s>>>(L->view(), x, b, scale.p, rtrue.p, r32.p, p32.p,
                                                y32.p, sc.p, rs, prm.tol, prm.inner_tol,
-                                               prm.max_outer, pin_row, pin_val);
+                                               prm.max_outer, pin_row, pin_val, 0, 0);
     GIPB_LAUNCH_CHECK();
     launches += 1;
     if (host_sync) {
@@ -526,7 +674,7 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
       k_mx_spmv_dot<<<blocks_spmv, 256, 0, s>>>(A, p32.p, Ap32.p, sc.p, rs);
       k_mx_update<<<blocks_vec, 256, 0, s>>>(n, y32.p, r32.p, p32.p, Ap32.p, sc.p, rs,
                                               prm.inner_maxit);
-      k_mx_pupdate<<<blocks_vec, 256, 0, s>>>(n, p32.p, r32.p, sc.p);
+      k_mx_pupdate<<<blocks_vec, 256, 0, s>>>(n, p32.p, r32.p, sc.p, 0, 0);
       GIPB_LAUNCH_CHECK();
       launches += 3;
       if (host_sync && (k + 1) % poll == 0) {
@@ -535,7 +683,7 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
         if (d) break;
       }
     }
-    k_mx_correct<<<blocks_vec, 256, 0, s>>>(n, x, y32.p, scale.p, sc.p, pin_row);
+    k_mx_correct<<<blocks_vec, 256, 0, s>>>(n, x, y32.p, scale.p, sc.p, pin_row, 0, 0);
     GIPB_LAUNCH_CHECK();
     launches += 1;
   }

@@ -49,6 +49,8 @@ struct Pcg {
   PcgScalars* h_sc = nullptr;  // pinned
   int blocks_spmv = 1, blocks_vec = 1;
   long long launches = 0;      // kernels enqueued by this solver (host count)
+  // streams that capture the bodies of the conditional while-nodes
+  cudaStream_t body_stream[2] = {nullptr, nullptr};
 
   ~Pcg();
   int init(const Sell* L, int n_all, const gipb200_pcg_params& prm, cudaStream_t s);
@@ -64,6 +66,8 @@ struct Pcg {
   int enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t s, bool host_sync);
   int enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_t s, bool host_sync);
   int read_flag(cudaStream_t s, int which, int* v);
+  int enqueue_fp64_graph(const double* b, double* x, const double* x0, cudaStream_t s);
+  int enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaStream_t s);
 };
 
 }  // namespace gipb200

@@ -208,14 +208,15 @@ class DnsEngine:
     def __init__(self, case: GipCase, rho: float = 1.0, gamma: float = 1e-3,
                  pcg_mode: str = "fixed", maxit: int = 100, tol: float = 1e-6,
                  inner_tol: float = 1e-3, inner_maxit: int = 2000, max_outer: int = 30,
-                 use_graph: bool = True):
+                 use_graph: bool = True, reorder: bool = False):
         lib = L.load()
         keep: list = []
         ops = L.DnsOps(**{n: _host_csr(case.ops[n], keep) for n in L.DNS_OPS},
                        n_inner=case.n_inner, n_owned=case.n_owned, n_faces=case.n_faces)
         f = {k: np.ascontiguousarray(case.fields[k], np.float64) for k in ("u", "v", "w", "dxs")}
         self.params = L.DnsParams(rho, gamma, pcg_params(pcg_mode, maxit, tol, inner_tol,
-                                                         inner_maxit, max_outer), int(use_graph))
+                                                         inner_maxit, max_outer), int(use_graph),
+                                  int(reorder))
         handle = C.c_void_p()
         L.check(lib.gipb200_dns_create(C.byref(ops), _hptr(f["u"]), _hptr(f["v"]), _hptr(f["w"]),
                                        _hptr(f["dxs"]), C.byref(self.params), C.byref(handle)),

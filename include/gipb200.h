@@ -56,6 +56,11 @@ int gipb200_memcpy_d2h(void* h_dst, const void* d_src, size_t bytes, void* strea
 /* GIP_cudaDcopy (libgpu.cu:68-71): d_dst[0:n) = d_src[0:n) */
 int gipb200_dcopy(int n, double* d_dst, const double* d_src, void* stream);
 int gipb200_stream_sync(void* stream);
+/* GIP_cudaEventCreate / Record / Synchronize / ElapsedTime / Destroy (libgpu.cu:206-235) */
+int gipb200_event_create(void** event);
+int gipb200_event_record(void* event, void* stream);
+int gipb200_event_elapsed_ms(void* start, void* stop, float* ms); /* waits for stop */
+int gipb200_event_destroy(void* event);
 
 /* ------------------------------------------------------------------ raw-pointer kernels */
 /* GIP_cudaDCsrSpMV (libgpu.cu:89-96 and 113-120).  mode 0: y = A x; mode 1:
@@ -159,6 +164,11 @@ typedef struct {
   double gamma;                /* GIP_DNS.h:137 (1/Re; enters only the CFL limit)  */
   gipb200_pcg_params pcg;      /* GIP_DNS.h:180-185 (FIXED, maxit 100)             */
   int use_graph;               /* capture each timestep in a CUDA graph            */
+  int reorder;                 /* 1: renumber cells (breadth-first from a peripheral cell)
+                                  and faces (by adjacent cell) inside the engine for
+                                  gather locality; every row keeps its nonzero order, so
+                                  each product is unchanged bit for bit.  Fields cross the
+                                  API in the caller's numbering. */
 } gipb200_dns_params;
 
 /* GIP_DNS::setUp (GIP_DNS.h:116-125): uploads operators and the initial fields u,v,w,dxs
@@ -181,8 +191,11 @@ int gipb200_dns_get_field(gipb200_dns E, const char* name, double* h_out, int n)
  * boundary values (e.g. the lid's ghost velocities) between steps. */
 int gipb200_dns_set_field(gipb200_dns E, const char* name, const double* h_in, int offset, int n,
                           void* stream);
-/* Device pointer of a field (valid until destroy). */
+/* Device pointer of a field (valid until destroy), in the engine's internal numbering
+ * (the caller's numbering unless `reorder` is set). */
 int gipb200_dns_field_ptr(gipb200_dns E, const char* name, double** d_ptr, int* n);
+/* Device-to-device copy of a field in the caller's numbering, on `stream`. */
+int gipb200_dns_copy_field(gipb200_dns E, const char* name, double* d_out, int n, void* stream);
 /* Current dt, sigma=1/dt and simulated time. */
 int gipb200_dns_scalars(gipb200_dns E, double* dt, double* sigma, double* time);
 

@@ -18,10 +18,11 @@ def _lines(oracle, h):
 
 
 @pytest.mark.skipif(not have_c100k(), reason="merged C100K set not built")
-@pytest.mark.parametrize("graph", [True, False])
-def test_c100k_readme_golden(gpu, oracle_mod, c100k_case, graph):
+@pytest.mark.parametrize("graph,reorder", [(True, False), (False, False), (True, True)])
+def test_c100k_readme_golden(gpu, oracle_mod, c100k_case, graph, reorder):
     from gip_b200.device import DnsEngine
-    E = DnsEngine(c100k_case, gamma=1e-3, pcg_mode="fixed", maxit=100, use_graph=graph)
+    E = DnsEngine(c100k_case, gamma=1e-3, pcg_mode="fixed", maxit=100, use_graph=graph,
+                  reorder=reorder)
     E.advance(10)
     h = E.history()
     assert _lines(oracle_mod, h) == golden_lines("c100k_readme.txt")
@@ -46,11 +47,12 @@ def test_fields_match_reference_goldens(gpu, n):
         assert rel_err(E.field(k)[: g[k].size], g[k]) < 1e-10, k
 
 
-@pytest.mark.parametrize("n,re,seed", [(10, 100.0, None), (9, 1000.0, 11)])
-def test_engine_matches_oracle_stepwise(gpu, oracle_mod, n, re, seed):
+@pytest.mark.parametrize("n,re,seed,reorder", [(10, 100.0, None, False), (9, 1000.0, 11, False),
+                                               (9, 1000.0, 11, True), (12, 400.0, None, True)])
+def test_engine_matches_oracle_stepwise(gpu, oracle_mod, n, re, seed, reorder):
     from gip_b200.device import DnsEngine
     case, _ = cavity.generate(n, re=re, permute_seed=seed)
-    E = DnsEngine(case, gamma=1.0 / re)
+    E = DnsEngine(case, gamma=1.0 / re, reorder=reorder)
     d = oracle_mod.OracleDNS(case, gamma=1.0 / re)
     for chunk in (3, 4):
         E.advance(chunk)
@@ -62,10 +64,12 @@ def test_engine_matches_oracle_stepwise(gpu, oracle_mod, n, re, seed):
     assert E.scalars()["time"] == pytest.approx(d.time, rel=1e-12)
 
 
-def test_engine_tol_mode_iterations(gpu, oracle_mod):
+@pytest.mark.parametrize("graph,reorder", [(True, False), (False, False), (True, True)])
+def test_engine_tol_mode_iterations(gpu, oracle_mod, graph, reorder):
     from gip_b200.device import DnsEngine
     case, _ = cavity.generate(16, re=400.0)
-    E = DnsEngine(case, gamma=1.0 / 400, pcg_mode="tol", maxit=3000, tol=1e-8)
+    E = DnsEngine(case, gamma=1.0 / 400, pcg_mode="tol", maxit=3000, tol=1e-8, use_graph=graph,
+                  reorder=reorder)
     E.advance(5)
     d = oracle_mod.OracleDNS(case, gamma=1.0 / 400, cg_maxit=3000, cg_mode=1, cg_tol=1e-8)
     hr = d.run(5)
@@ -75,11 +79,12 @@ def test_engine_tol_mode_iterations(gpu, oracle_mod):
         assert rel_err(E.field(k), d.vec[k]) < 1e-7, k
 
 
-def test_engine_mixed_close_to_fp64(gpu, oracle_mod):
+@pytest.mark.parametrize("graph,reorder", [(True, False), (False, False), (True, True)])
+def test_engine_mixed_close_to_fp64(gpu, oracle_mod, graph, reorder):
     from gip_b200.device import DnsEngine
     case, _ = cavity.generate(16, re=400.0)
     E = DnsEngine(case, gamma=1.0 / 400, pcg_mode="mixed", maxit=3000, tol=1e-8,
-                  inner_tol=1e-3)
+                  inner_tol=1e-3, use_graph=graph, reorder=reorder)
     E.advance(5)
     d = oracle_mod.OracleDNS(case, gamma=1.0 / 400, cg_maxit=3000, cg_mode=1, cg_tol=1e-10)
     d.run(5)
@@ -87,3 +92,25 @@ def test_engine_mixed_close_to_fp64(gpu, oracle_mod):
     assert np.all(h["massr"] < 1e-6)
     for k in ("u", "v", "w"):
         assert rel_err(E.field(k), d.vec[k]) < 1e-6, k
+
+
+def test_set_and_copy_field_roundtrip_reordered(gpu):
+    import torch
+    from gip_b200.device import DnsEngine
+    case, meta = cavity.generate(6, re=100.0, permute_seed=2)
+    E = DnsEngine(case, gamma=1e-2, reorder=True)
+    u = E.field("u")
+    assert np.array_equal(u, case.fields["u"])
+    lid = np.full(36, 0.5)
+    off = case.n_inner + 5 * 36
+    E.set_field("u", lid, offset=off)
+    torch.cuda.synchronize()
+    u2 = E.field("u")
+    assert np.array_equal(u2[off:off + 36], lid) and np.array_equal(u2[:off], u[:off])
+    d = torch.zeros(case.n_owned, dtype=torch.float64, device="cuda")
+    from gip_b200 import _lib
+    import ctypes
+    _lib.call("gipb200_dns_copy_field", E.handle, b"u", ctypes.c_void_p(d.data_ptr()),
+              case.n_owned, None)
+    torch.cuda.synchronize()
+    assert np.array_equal(d.cpu().numpy(), u2)
