@@ -47,6 +47,17 @@ class DnsParams(C.Structure):
                 ("use_graph", C.c_int), ("reorder", C.c_int)]
 
 
+class DnsInfo(C.Structure):
+    _fields_ = [("reordered", C.c_int), ("pin_row", C.c_int), ("compressed", C.c_int),
+                ("value_table", C.c_int), ("compressed_fraction", C.c_double),
+                ("slots_L", C.c_longlong), ("nnz_L", C.c_longlong)]
+
+
+class AdjointParams(C.Structure):
+    _fields_ = [("rho", C.c_double), ("gamma", C.c_double), ("nu0", C.c_double),
+                ("tol", C.c_double), ("maxit", C.c_int), ("checkpoint_every", C.c_int)]
+
+
 PCG_FIXED, PCG_TOL, PCG_MIXED = 0, 1, 2
 STATUS_OK, ERR_ARG, ERR_CUDA, ERR_BREAKDOWN, ERR_TIMEOUT, ERR_NOMEM, ERR_NOT_CONVERGED, \
     ERR_STATE = range(8)
@@ -85,11 +96,24 @@ _SIGNATURES = {
     "gipb200_pcg_create": (_I, [_VP, _I, C.POINTER(PcgParams), C.POINTER(_VP)]),
     "gipb200_pcg_destroy": (_I, [_VP]),
     "gipb200_pcg_solve": (_I, [_VP, _VP, _VP, _VP, _VP, C.POINTER(PcgResult)]),
+    "gipb200_adjoint_create": (_I, [C.POINTER(DnsOps), _VP, _VP, _VP, _VP, _VP, _VP, _I,
+                                    C.POINTER(AdjointParams), C.POINTER(_VP)]),
+    "gipb200_adjoint_destroy": (_I, [_VP]),
+    "gipb200_adjoint_forward": (_I, [_VP, _VP, _D, _I, _VP, _I, C.POINTER(_D)]),
+    "gipb200_adjoint_backward": (_I, [_VP, _VP, C.POINTER(_D)]),
+    "gipb200_dns_set_launch": (_I, [_VP, _I, _I]),
+    "gipb200_dns_snapshot": (_I, [_VP, _I, _VP]),
+    "gipb200_dns_get_info": (_I, [_VP, C.POINTER(DnsInfo)]),
+    "gipb200_batch_create": (_I, [_I, _VP, _VP, _VP, _VP, _VP, C.POINTER(DnsParams),
+                                  C.POINTER(_VP)]),
+    "gipb200_batch_destroy": (_I, [_VP]),
+    "gipb200_batch_instance": (_I, [_VP, _I, C.POINTER(_VP)]),
+    "gipb200_batch_advance": (_I, [_VP, _I, _VP]),
     "gipb200_dns_create": (_I, [C.POINTER(DnsOps), _VP, _VP, _VP, _VP, C.POINTER(DnsParams),
                                 C.POINTER(_VP)]),
     "gipb200_dns_destroy": (_I, [_VP]),
     "gipb200_dns_advance": (_I, [_VP, _I, _VP]),
-    "gipb200_dns_history": (_I, [_VP, C.POINTER(_I), _VP, _VP, _VP, _VP, _VP]),
+    "gipb200_dns_history": (_I, [_VP, C.POINTER(_I), _VP, _VP, _VP, _VP, _VP, _VP]),
     "gipb200_dns_get_field": (_I, [_VP, C.c_char_p, _VP, _I]),
     "gipb200_dns_field_ptr": (_I, [_VP, C.c_char_p, C.POINTER(_VP), C.POINTER(_I)]),
     "gipb200_dns_copy_field": (_I, [_VP, C.c_char_p, _VP, _I, _VP]),

@@ -12,24 +12,9 @@
 #include <string>
 
 #include "device.cuh"
-#include "pcg.cuh"
+#include "dns.cuh"
 
 namespace gipb200 {
-
-struct DnsScalars {
-  double dt, sigma, time;
-  int step;
-  int started;
-};
-
-struct DnsHistory {
-  double* time;
-  double* dt;
-  double* massr;
-  int* iters;
-  double* rr;
-  int capacity;
-};
 
 // ------------------------------------------------------------------ row helpers
 // D and C share D's sparsity (GIP loads C from D's file, GIP_DNS.h:150-151): one pass
@@ -290,9 +275,15 @@ struct CflStepFinish {
   const PcgScalars* P;
   int mode;  // 0: initial dt only (GIP_DNS.h:102-103); 1: end of a step (:402-408)
   int pcg_mixed;
+  const double* dt_seq;  // prescribed steps (frozen-dt adjoint runs) or null
+  int dt_seq_len;
   __device__ void operator()(const double* t) const {
     const double fin = t[0];
-    const double dtn = (dmul(0.8, fin) > 1e-1) ? 1e-1 : dmul(0.8, fin);
+    double dtn = (dmul(0.8, fin) > 1e-1) ? 1e-1 : dmul(0.8, fin);
+    if (dt_seq) {
+      const int k = (mode == 1) ? S->step + 1 : S->step;
+      dtn = dt_seq[k < dt_seq_len ? k : dt_seq_len - 1];
+    }
     if (mode == 1) {
       const int k = S->step;
       const double tnew = dadd(S->time, S->dt);
@@ -302,6 +293,7 @@ struct CflStepFinish {
         H.dt[k] = S->dt;
         H.iters[k] = pcg_mixed ? P->total_inner : P->iter;
         H.rr[k] = P->rr;
+        H.outer[k] = pcg_mixed ? P->outer : 0;
       }
       S->step = k + 1;
     }
@@ -317,60 +309,21 @@ __global__ void __launch_bounds__(256) k_dns_cfl(int n, const double* __restrict
                                                  const double* __restrict__ dxs, double gamma,
                                                  double rho, DnsScalars* S, DnsHistory H,
                                                  const PcgScalars* P, int mode, int pcg_mixed,
+                                                 const double* dt_seq, int dt_seq_len,
                                                  ReduceScratch rs) {
   double acc[1] = {1e20};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     acc[0] = cfl_candidate(u[i], v[i], w[i], dxs[i], gamma, rho, acc[0]);
-  grid_reduce<MinOp, 1>(acc, rs, CflStepFinish{S, H, P, mode, pcg_mixed});
+  grid_reduce<MinOp, 1>(acc, rs, CflStepFinish{S, H, P, mode, pcg_mixed, dt_seq, dt_seq_len});
 }
 
 // ------------------------------------------------------------------ engine
-struct Dns {
-  int N = 0, NO = 0, NF = 0;
-  gipb200_dns_params prm{};
-  Sell D, Ec, L, Lb, Mx, My, Mz, Mres, Gx, Gy, Gz, SFx, SFy, SFz, SO;
-  DevBuf<double> cval;
-  DevBuf<double> u, v, w, dxs, ax, ay, az, ax0, ay0, az0, rhs, p, p0, gpx, gpy, gpz, temp, mf;
-  Pcg pcg;
-  DevBuf<DnsScalars> sc;
-  DevBuf<double> h_time, h_dt, h_massr, h_rr;
-  DevBuf<int> h_iters;
-  int capacity = 0;
-  DevBuf<double> partials;
-  DevBuf<unsigned> ticket;
-  ReduceScratch rs{};
-  int steps_enqueued = 0;
-  bool started = false;
-  cudaStream_t cap_stream = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  int blocks_cells = 1, blocks_faces = 1, blocks_owned = 1, blocks_vec = 1;
-  // internal renumbering (reorder): external index e lives at internal perm[e]
-  bool reordered = false;
-  DevBuf<int> perm_c, perm_f;
-  DevBuf<double> staging;
-  long long launches = 0;        // kernels launched (graph launches count their kernels)
-  long long graph_kernels = 0;   // kernels in the captured step graph
-
-  ~Dns() {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    if (cap_stream) cudaStreamDestroy(cap_stream);
-  }
-  DnsHistory history() const {
-    return {h_time.p, h_dt.p, h_massr.p, h_iters.p, h_rr.p, capacity};
-  }
-  int grow_history(int need, cudaStream_t s);
-  int enqueue_step(cudaStream_t s, bool host_sync);
-  int enqueue_initial_dt(cudaStream_t s);
-  double* field(const std::string& name, int* n);
-};
-
 int Dns::grow_history(int need, cudaStream_t s) {
   if (need <= capacity) return GIPB200_OK;
   int cap = std::max(need, std::max(1024, capacity * 2));
   DevBuf<double> t, d, m, r;
-  DevBuf<int> it;
+  DevBuf<int> it, ou;
+  GIPB_TRY(ou.alloc(cap));
   GIPB_TRY(t.alloc(cap));
   GIPB_TRY(d.alloc(cap));
   GIPB_TRY(m.alloc(cap));
@@ -382,6 +335,7 @@ int Dns::grow_history(int need, cudaStream_t s) {
     GIPB_CUDA(cudaMemcpyAsync(m.p, h_massr.p, capacity * 8, cudaMemcpyDeviceToDevice, s));
     GIPB_CUDA(cudaMemcpyAsync(r.p, h_rr.p, capacity * 8, cudaMemcpyDeviceToDevice, s));
     GIPB_CUDA(cudaMemcpyAsync(it.p, h_iters.p, capacity * 4, cudaMemcpyDeviceToDevice, s));
+    GIPB_CUDA(cudaMemcpyAsync(ou.p, h_outer.p, capacity * 4, cudaMemcpyDeviceToDevice, s));
     GIPB_CUDA(cudaStreamSynchronize(s));
   }
   std::swap(h_time.p, t.p);
@@ -389,8 +343,9 @@ int Dns::grow_history(int need, cudaStream_t s) {
   std::swap(h_massr.p, m.p);
   std::swap(h_rr.p, r.p);
   std::swap(h_iters.p, it.p);
-  h_time.n = h_dt.n = h_massr.n = h_rr.n = h_iters.n = cap;
-  t.n = d.n = m.n = r.n = it.n = capacity;
+  std::swap(h_outer.p, ou.p);
+  h_time.n = h_dt.n = h_massr.n = h_rr.n = h_iters.n = h_outer.n = cap;
+  t.n = d.n = m.n = r.n = it.n = ou.n = capacity;
   capacity = cap;
   // a captured graph refers to the old history arrays
   if (exec) {
@@ -406,7 +361,7 @@ int Dns::grow_history(int need, cudaStream_t s) {
 
 int Dns::enqueue_initial_dt(cudaStream_t s) {
   k_dns_cfl<<<blocks_vec, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p,
-                                        history(), pcg.sc.p, 0, 0, rs);
+                                        history(), pcg.sc.p, 0, 0, dt_seq.p, dt_seq_len, rs);
   GIPB_LAUNCH_CHECK();
   launches += 1;
   return GIPB200_OK;
@@ -437,7 +392,8 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync) {
   // CFLCondition
   k_dns_massr<<<blocks_cells, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
   k_dns_cfl<<<blocks_vec, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p, H,
-                                        pcg.sc.p, 1, prm.pcg.mode == GIPB200_PCG_MIXED, rs);
+                                        pcg.sc.p, 1, prm.pcg.mode == GIPB200_PCG_MIXED, dt_seq.p,
+                                        dt_seq_len, rs);
   GIPB_LAUNCH_CHECK();
   launches += 10 + (pcg.launches - pcg_before);
   return GIPB200_OK;
@@ -552,22 +508,7 @@ static int build_op(Sell* S, const gipb200_host_csr& m) {
   return sell_build(S, m.nrows, m.ncols, m.nnz, m.rowptr, m.col, m.val, 0);
 }
 
-}  // namespace gipb200
-
-using namespace gipb200;
-
-struct gipb200_dns_s {
-  gipb200::Dns E;
-};
-
-extern "C" {
-
-int gipb200_dns_create(const gipb200_dns_ops* ops, const double* h_u, const double* h_v,
-                       const double* h_w, const double* h_dxs, const gipb200_dns_params* prm,
-                       gipb200_dns* out) {
-  if (!ops || !prm || !out || !h_u || !h_v || !h_w || !h_dxs)
-    return fail(GIPB200_ERR_ARG, "null argument");
-  *out = nullptr;
+int check_dns_ops(const gipb200_dns_ops* ops) {
   const int N = ops->n_inner, NO = ops->n_owned, NF = ops->n_faces;
   if (N <= 0 || NO < N || NF < 0) return fail(GIPB200_ERR_ARG, "bad topology sizes");
   // row/column spaces of GIP_DNS's operators (GIP_DNS.h:143-238)
@@ -588,12 +529,15 @@ int gipb200_dns_create(const gipb200_dns_ops* ops, const double* h_u, const doub
   GIPB_TRY(check_op(ops->Ec, "Ec", ops->D.nnz, NF));
   if (ops->Ec.nrows != ops->D.nnz)
     return fail(GIPB200_ERR_ARG, "Ec has %d rows, D has %d nonzeros", ops->Ec.nrows, ops->D.nnz);
-  if (prm->pcg.mode < 0 || prm->pcg.mode > 2) return fail(GIPB200_ERR_ARG, "bad PCG mode");
 
-  gipb200_dns D = new (std::nothrow) gipb200_dns_s();
-  if (!D) return fail(GIPB200_ERR_NOMEM, "host allocation failed");
-  Dns& E = D->E;
-  int st = [&]() -> int {
+  return GIPB200_OK;
+}
+
+int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double* h_v,
+             const double* h_w, const double* h_dxs, const gipb200_dns_params* prm) {
+  GIPB_TRY(check_dns_ops(ops));
+  if (prm->pcg.mode < 0 || prm->pcg.mode > 2) return fail(GIPB200_ERR_ARG, "bad PCG mode");
+  const int N = ops->n_inner, NO = ops->n_owned, NF = ops->n_faces;
     E.N = N;
     E.NO = NO;
     E.NF = NF;
@@ -736,24 +680,9 @@ int gipb200_dns_create(const gipb200_dns_ops* ops, const double* h_u, const doub
     GIPB_CUDA(cudaStreamCreateWithFlags(&E.cap_stream, cudaStreamNonBlocking));
     GIPB_CUDA(cudaDeviceSynchronize());
     return GIPB200_OK;
-  }();
-  if (st != GIPB200_OK) {
-    delete D;
-    return st;
-  }
-  *out = D;
-  return GIPB200_OK;
 }
 
-int gipb200_dns_destroy(gipb200_dns D) {
-  delete D;
-  return GIPB200_OK;
-}
-
-int gipb200_dns_advance(gipb200_dns Dh, int nsteps, void* stream) {
-  if (!Dh || nsteps < 0) return fail(GIPB200_ERR_ARG, "bad arguments");
-  Dns& E = Dh->E;
-  cudaStream_t s = as_stream(stream);
+int dns_advance(Dns& E, int nsteps, cudaStream_t s) {
   GIPB_TRY(E.grow_history(E.steps_enqueued + nsteps, s));
   if (!E.started) {
     GIPB_TRY(E.enqueue_initial_dt(s));
@@ -793,8 +722,41 @@ int gipb200_dns_advance(gipb200_dns Dh, int nsteps, void* stream) {
   return GIPB200_OK;
 }
 
+}  // namespace gipb200
+
+using namespace gipb200;
+
+extern "C" {
+
+int gipb200_dns_create(const gipb200_dns_ops* ops, const double* h_u, const double* h_v,
+                       const double* h_w, const double* h_dxs, const gipb200_dns_params* prm,
+                       gipb200_dns* out) {
+  if (!ops || !prm || !out || !h_u || !h_v || !h_w || !h_dxs)
+    return fail(GIPB200_ERR_ARG, "null argument");
+  *out = nullptr;
+  gipb200_dns D = new (std::nothrow) gipb200_dns_s();
+  if (!D) return fail(GIPB200_ERR_NOMEM, "host allocation failed");
+  int st = dns_init(D->E, ops, h_u, h_v, h_w, h_dxs, prm);
+  if (st != GIPB200_OK) {
+    delete D;
+    return st;
+  }
+  *out = D;
+  return GIPB200_OK;
+}
+
+int gipb200_dns_destroy(gipb200_dns D) {
+  delete D;
+  return GIPB200_OK;
+}
+
+int gipb200_dns_advance(gipb200_dns Dh, int nsteps, void* stream) {
+  if (!Dh || nsteps < 0) return fail(GIPB200_ERR_ARG, "bad arguments");
+  return dns_advance(Dh->E, nsteps, as_stream(stream));
+}
+
 int gipb200_dns_history(gipb200_dns Dh, int* steps, double* t, double* dt, double* massr,
-                        int* iters, double* rr) {
+                        int* iters, double* rr, int* outer) {
   if (!Dh) return fail(GIPB200_ERR_ARG, "null engine");
   Dns& E = Dh->E;
   GIPB_CUDA(cudaDeviceSynchronize());
@@ -807,6 +769,7 @@ int gipb200_dns_history(gipb200_dns Dh, int* steps, double* t, double* dt, doubl
   if (massr && n) GIPB_CUDA(cudaMemcpy(massr, E.h_massr.p, n * 8, cudaMemcpyDeviceToHost));
   if (iters && n) GIPB_CUDA(cudaMemcpy(iters, E.h_iters.p, n * 4, cudaMemcpyDeviceToHost));
   if (rr && n) GIPB_CUDA(cudaMemcpy(rr, E.h_rr.p, n * 8, cudaMemcpyDeviceToHost));
+  if (outer && n) GIPB_CUDA(cudaMemcpy(outer, E.h_outer.p, n * 4, cudaMemcpyDeviceToHost));
   return GIPB200_OK;
 }
 
@@ -883,6 +846,65 @@ int gipb200_dns_set_field(gipb200_dns Dh, const char* name, const double* h_in, 
   } else {
     GIPB_CUDA(cudaMemcpyAsync(p + offset, h_in, (size_t)n * 8, cudaMemcpyHostToDevice, s));
   }
+  return GIPB200_OK;
+}
+
+int gipb200_dns_set_launch(gipb200_dns Dh, int spmv_blocks, int vec_blocks) {
+  if (!Dh) return fail(GIPB200_ERR_ARG, "null engine");
+  Dns& E = Dh->E;
+  GIPB_TRY(E.pcg.set_launch(spmv_blocks, vec_blocks));
+  if (E.exec) {
+    cudaGraphExecDestroy(E.exec);
+    E.exec = nullptr;
+  }
+  if (E.graph) {
+    cudaGraphDestroy(E.graph);
+    E.graph = nullptr;
+  }
+  return GIPB200_OK;
+}
+
+int gipb200_dns_get_info(gipb200_dns Dh, gipb200_dns_info* info) {
+  if (!Dh || !info) return fail(GIPB200_ERR_ARG, "null argument");
+  const Dns& E = Dh->E;
+  info->reordered = E.reordered;
+  info->pin_row = E.pcg.pin_row;
+  info->compressed = E.pcg.cop.enabled;
+  info->value_table = E.pcg.cop.dict;
+  info->compressed_fraction = E.pcg.cop.compressed_fraction;
+  info->slots_L = E.L.nslots;
+  info->nnz_L = E.L.nnz;
+  return GIPB200_OK;
+}
+
+int gipb200_dns_snapshot(gipb200_dns Dh, int restore, void* stream) {
+  if (!Dh) return fail(GIPB200_ERR_ARG, "null engine");
+  Dns& E = Dh->E;
+  cudaStream_t s = as_stream(stream);
+  DevBuf<double>* state[] = {&E.u,   &E.v,   &E.w,   &E.ax,  &E.ay,  &E.az,  &E.ax0,
+                             &E.ay0, &E.az0, &E.rhs, &E.p,   &E.p0,  &E.gpx, &E.gpy,
+                             &E.gpz, &E.temp, &E.mf, &E.cval};
+  const int ns = (int)(sizeof(state) / sizeof(state[0]));
+  if (!restore) {
+    if (E.snap.empty()) {
+      for (int k = 0; k < ns; ++k) {
+        DevBuf<double>* b = new DevBuf<double>();
+        E.snap.push_back(b);
+        GIPB_TRY(b->alloc(state[k]->n));
+      }
+      GIPB_TRY(E.snap_sc.alloc(1));
+    }
+    for (int k = 0; k < ns; ++k)
+      GIPB_CUDA(cudaMemcpyAsync(E.snap[k]->p, state[k]->p, state[k]->n * 8, cudaMemcpyDeviceToDevice, s));
+    GIPB_CUDA(cudaMemcpyAsync(E.snap_sc.p, E.sc.p, sizeof(DnsScalars), cudaMemcpyDeviceToDevice, s));
+    E.snap_steps = E.steps_enqueued;
+    return GIPB200_OK;
+  }
+  if (E.snap.empty() || E.snap_steps < 0) return fail(GIPB200_ERR_STATE, "no snapshot taken");
+  for (int k = 0; k < ns; ++k)
+    GIPB_CUDA(cudaMemcpyAsync(state[k]->p, E.snap[k]->p, state[k]->n * 8, cudaMemcpyDeviceToDevice, s));
+  GIPB_CUDA(cudaMemcpyAsync(E.sc.p, E.snap_sc.p, sizeof(DnsScalars), cudaMemcpyDeviceToDevice, s));
+  E.steps_enqueued = E.snap_steps;
   return GIPB200_OK;
 }
 

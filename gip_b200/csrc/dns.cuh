@@ -1,0 +1,85 @@
+// The fused timestep engine shared by the C ABI (dns.cu) and the adjoint (adjoint.cu).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "pcg.cuh"
+
+namespace gipb200 {
+
+struct DnsScalars {
+  double dt, sigma, time;
+  int step;
+  int started;
+};
+
+struct DnsHistory {
+  double* time;
+  double* dt;
+  double* massr;
+  int* iters;
+  double* rr;
+  int* outer;
+  int capacity;
+};
+
+struct Dns {
+  int N = 0, NO = 0, NF = 0;
+  gipb200_dns_params prm{};
+  Sell D, Ec, L, Lb, Mx, My, Mz, Mres, Gx, Gy, Gz, SFx, SFy, SFz, SO;
+  DevBuf<double> cval;
+  DevBuf<double> u, v, w, dxs, ax, ay, az, ax0, ay0, az0, rhs, p, p0, gpx, gpy, gpz, temp, mf;
+  Pcg pcg;
+  DevBuf<DnsScalars> sc;
+  DevBuf<double> h_time, h_dt, h_massr, h_rr;
+  DevBuf<int> h_iters, h_outer;
+  int capacity = 0;
+  DevBuf<double> partials;
+  DevBuf<unsigned> ticket;
+  ReduceScratch rs{};
+  int steps_enqueued = 0;
+  bool started = false;
+  cudaStream_t cap_stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int blocks_cells = 1, blocks_faces = 1, blocks_owned = 1, blocks_vec = 1;
+  // internal renumbering (reorder): external index e lives at internal perm[e]
+  bool reordered = false;
+  DevBuf<int> perm_c, perm_f;
+  DevBuf<double> staging;
+  long long launches = 0;        // kernels launched (graph launches count their kernels)
+  long long graph_kernels = 0;   // kernels in the captured step graph
+  // device-side snapshot of the whole timestep state (checkpoint / resume)
+  std::vector<DevBuf<double>*> snap;
+  DevBuf<DnsScalars> snap_sc;
+  int snap_steps = -1;
+  // prescribed time steps (adjoint runs): dt of step k is dt_seq[min(k, len-1)]
+  DevBuf<double> dt_seq;
+  int dt_seq_len = 0;
+
+  ~Dns() {
+    for (auto* b : snap) delete b;
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+  }
+  DnsHistory history() const {
+    return {h_time.p, h_dt.p, h_massr.p, h_iters.p, h_rr.p, h_outer.p, capacity};
+  }
+  int grow_history(int need, cudaStream_t s);
+  int enqueue_step(cudaStream_t s, bool host_sync);
+  int enqueue_initial_dt(cudaStream_t s);
+  double* field(const std::string& name, int* n);
+};
+
+int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double* h_v,
+             const double* h_w, const double* h_dxs, const gipb200_dns_params* prm);
+int dns_advance(Dns& E, int nsteps, cudaStream_t s);
+int check_dns_ops(const gipb200_dns_ops* ops);
+
+}  // namespace gipb200
+
+struct gipb200_dns_s {
+  gipb200::Dns E;
+};

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -184,61 +185,71 @@ __global__ void __launch_bounds__(256) k_pcg_pupdate(int n, double* __restrict__
 }
 
 // ------------------------------------------------------------------ MIXED kernels
-struct OuterFinish {
+// Reliable-update mixed CG.  The FP32 CG runs on the scaled operator A^ = S L S (pin
+// removed when L is pinned-Neumann) with its search direction kept for the whole solve;
+// the FP64 true residual r = b - L x replaces the FP32 one ("reliable update") whenever
+// the FP32 residual has fallen by the factor delta since the last replacement or
+// predicts convergence.  x accumulates in FP64: x += S y + kappa at each replacement.
+
+struct ResidualFinish {
   PcgScalars* S;
-  double tol, inner_tol;
-  int max_outer;
+  int first;
+  double tol, delta;
+  int maxit, max_updates;
   int pin_row;
   double pin_val;
   const double* scale;
   float* r32;
   float* p32;
   int use_cond;
-  cudaGraphConditionalHandle inner_cond;
+  cudaGraphConditionalHandle loop_cond;
   __device__ void operator()(const double* t) const {
-    // t[0] = r.r (FP64, true residual), t[1] = scaled r^.r^, t[2] = b.b, t[3] = sum(r)
-    if (S->outer == 0) S->bb = t[2];
+    // t[0] = r.r (FP64 true residual), t[1] = r^.r^ before the pin projection,
+    // t[2] = b.b, t[3] = sum(r)
+    if (first) S->bb = t[2];
     S->rr = t[0];
     double rz = t[1];
-    S->rsum = t[3];
     S->kappa_c = 0.0;
     if (pin_row >= 0) {
-      // project the scaled residual: r^_p -= s_p sum(r)
       const float old = __ldcg(r32 + pin_row);
       const float nw = (float)((double)old - scale[pin_row] * t[3]);
       r32[pin_row] = nw;
-      p32[pin_row] = nw;
+      if (first) p32[pin_row] = nw;
       rz = rz - (double)old * (double)old + (double)nw * (double)nw;
       S->kappa_c = t[3] / pin_val;
     }
+    if (!first) {
+      S->beta = rz / S->rz;  // continue the direction with the replaced residual
+      S->outer += 1;
+    }
     S->rz = rz;
-    S->rz_target = rz * inner_tol * inner_tol;
-    S->iter = 0;
+    S->maxr2 = rz;
+    // FP32 level at which the predicted true residual reaches tol*||b|| / 2
+    const double goal = 0.5 * tol * sqrt(S->bb);
+    S->trig = (t[0] > 0.0) ? rz * (goal * goal) / t[0] : 0.0;
+    S->upd = 0;
     const bool conv = !(sqrt(t[0]) > tol * sqrt(S->bb));
-    if (conv || S->outer >= max_outer || !isfinite(t[0])) {
+    if (conv || !isfinite(t[0]) || S->total_inner >= maxit || S->outer >= max_updates) {
       if (!conv) S->status = isfinite(t[0]) ? GIPB200_ERR_NOT_CONVERGED : GIPB200_ERR_BREAKDOWN;
       S->done = 1;
-      S->inner_done = 1;
-    } else {
-      S->outer += 1;
-      S->inner_done = 0;
     }
-    set_loop(use_cond, inner_cond, !S->inner_done);
+    (void)delta;
+    if (first) set_loop(use_cond, loop_cond, !S->done);
   }
 };
 
-// r = b - L x (FP64); r^ = S r (FP32); p = r^; y = 0; (r.r, r^.r^, b.b)
+// r = b - L x (FP64); r^ = S r (FP32); first call: p = r^, y = 0.  Later calls run only
+// when a replacement is due (S->upd).
 __global__ void __launch_bounds__(256) k_mx_residual(SellView<double> L, const double* __restrict__ x,
                                                      const double* __restrict__ b,
                                                      const double* __restrict__ scale,
-                                                     double* __restrict__ rtrue,
                                                      float* __restrict__ r32, float* __restrict__ p32,
                                                      float* __restrict__ y32, PcgScalars* S,
-                                                     ReduceScratch rs, double tol, double inner_tol,
-                                                     int max_outer, int pin_row, double pin_val,
-                                                     int use_cond,
-                                                     cudaGraphConditionalHandle inner_cond) {
-  if (S->done) return;
+                                                     ReduceScratch rs, int first, double tol,
+                                                     double delta, int maxit, int max_updates,
+                                                     int pin_row, double pin_val, int use_cond,
+                                                     cudaGraphConditionalHandle loop_cond) {
+  if (!first && (!S->upd || S->done)) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -251,11 +262,12 @@ __global__ void __launch_bounds__(256) k_mx_residual(SellView<double> L, const d
     if (i < L.nrows) {
       const double bi = b[i];
       const double ri = bi - sum;
-      rtrue[i] = ri;
       const float rh = (float)(ri * scale[i]);
       r32[i] = rh;
-      p32[i] = rh;
-      y32[i] = 0.f;
+      if (first) {
+        p32[i] = rh;
+        y32[i] = 0.f;
+      }
       acc[0] += ri * ri;
       acc[1] += (double)rh * (double)rh;
       acc[2] += bi * bi;
@@ -263,8 +275,8 @@ __global__ void __launch_bounds__(256) k_mx_residual(SellView<double> L, const d
     }
   }
   grid_reduce<SumOp, 4>(acc, rs,
-                        OuterFinish{S, tol, inner_tol, max_outer, pin_row, pin_val, scale, r32, p32,
-                                    use_cond, inner_cond});
+                        ResidualFinish{S, first, tol, delta, maxit, max_updates, pin_row, pin_val,
+                                       scale, r32, p32, use_cond, loop_cond});
 }
 
 struct AlphaFinish32 {
@@ -272,14 +284,16 @@ struct AlphaFinish32 {
   __device__ void operator()(const double* t) const {
     S->pAp = t[0];
     S->alpha = S->rz / t[0];
-    if (!(t[0] > 0.0) || !isfinite(S->alpha)) S->inner_done = 1;  // inner stagnated
+    if (!(t[0] > 0.0) || !isfinite(S->alpha)) {  // FP32 direction lost: force a replacement
+      S->alpha = 0.0;
+    }
   }
 };
 
 __global__ void __launch_bounds__(256) k_mx_spmv_dot(SellView<float> A, const float* __restrict__ p,
                                                      float* __restrict__ Ap, PcgScalars* S,
                                                      ReduceScratch rs) {
-  if (S->inner_done) return;
+  if (S->done) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -295,25 +309,104 @@ __global__ void __launch_bounds__(256) k_mx_spmv_dot(SellView<float> A, const fl
   grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
 }
 
+// Same product as k_mx_spmv_dot from the compressed layout: identical gathers and FMA
+// order, so identical results.
+template <bool DICT>
+__global__ void __launch_bounds__(256) k_mxc_spmv_dot(SellView<float> A,
+                                                      const unsigned short* __restrict__ delta,
+                                                      const unsigned char* __restrict__ vidx,
+                                                      const int* __restrict__ base,
+                                                      const unsigned char* __restrict__ plain,
+                                                      const float* __restrict__ table, int ntable,
+                                                      const float* __restrict__ p,
+                                                      float* __restrict__ Ap, PcgScalars* S,
+                                                      ReduceScratch rs) {
+  if (S->done) return;
+  __shared__ float tab[256];
+  if (DICT) {
+    for (int t = threadIdx.x; t < ntable; t += blockDim.x) tab[t] = table[t];
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  double acc[1] = {0.0};
+  for (int s = gw; s < A.nslices; s += nw) {
+    float sum;
+    if (plain[s]) {
+      sum = sell_row_f32(A, p, s, lane);
+    } else {
+      const long long b0 = A.sptr[s];
+      const int len = (int)((A.sptr[s + 1] - b0) >> 5);
+      const int* bs = base + (b0 >> 5);
+      sum = 0.f;
+      constexpr int CH = 8;
+      for (int j0 = 0; j0 < len; j0 += CH) {
+        int c[CH];
+        float v[CH];
+#pragma unroll
+        for (int t = 0; t < CH; ++t) {
+          if (j0 + t < len) {
+            const long long k = b0 + 32LL * (j0 + t) + lane;
+            c[t] = __ldg(bs + j0 + t) + (int)ld_stream(delta + k);
+            v[t] = DICT ? tab[ld_stream(vidx + k)] : ld_stream(A.val + k);
+          } else {
+            c[t] = -1;
+            v[t] = 0.f;
+          }
+        }
+        float xv[CH];
+#pragma unroll
+        for (int t = 0; t < CH; ++t) xv[t] = (c[t] >= 0) ? __ldg(p + c[t]) : 0.f;
+#pragma unroll
+        for (int t = 0; t < CH; ++t) sum = fmaf(xv[t], v[t], sum);
+      }
+    }
+    const int i = s * 32 + lane;
+    if (i < A.nrows) {
+      Ap[i] = sum;
+      acc[0] += (double)p[i] * (double)sum;
+    }
+  }
+  grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
+}
+
 struct BetaFinish32 {
   PcgScalars* S;
-  int inner_maxit;
+  double delta;
+  int maxit;
+  int pin_row;
+  const double* scale;
+  const float* y32;
+  int use_cond;
+  cudaGraphConditionalHandle upd_cond;
   __device__ void operator()(const double* t) const {
-    const double r0 = S->rz;
-    S->rz = t[0];
-    S->beta = t[0] / r0;
     S->iter += 1;
     S->total_inner += 1;
-    if (!(t[0] > S->rz_target) || S->iter >= inner_maxit) S->inner_done = 1;
+    const double rz_new = t[0];
+    if (rz_new > S->maxr2) S->maxr2 = rz_new;
+    const bool upd = !(rz_new > S->trig) || !(rz_new > delta * delta * S->maxr2) ||
+                     S->alpha == 0.0 || S->total_inner >= maxit || !isfinite(rz_new);
+    if (upd) {
+      S->upd = 1;
+      S->kappa = (pin_row >= 0) ? S->kappa_c - scale[pin_row] * (double)__ldcg(y32 + pin_row) : 0.0;
+    } else {
+      S->beta = rz_new / S->rz;
+      S->rz = rz_new;
+    }
+    set_loop(use_cond, upd_cond, upd);
   }
 };
 
+// y += alpha p; r^ -= alpha A^p; r^.r^; decide on a replacement
 __global__ void __launch_bounds__(256) k_mx_update(int n, float* __restrict__ y,
                                                    float* __restrict__ r,
                                                    const float* __restrict__ p,
                                                    const float* __restrict__ Ap, PcgScalars* S,
-                                                   ReduceScratch rs, int inner_maxit) {
-  if (S->inner_done) return;
+                                                   ReduceScratch rs, double delta, int maxit,
+                                                   int pin_row, const double* __restrict__ scale,
+                                                   int use_cond, cudaGraphConditionalHandle upd_cond) {
+  if (S->done) return;
   const float alpha = (float)S->alpha;
   double acc[1] = {0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -322,31 +415,31 @@ __global__ void __launch_bounds__(256) k_mx_update(int n, float* __restrict__ y,
     r[i] = ri;
     acc[0] += (double)ri * (double)ri;
   }
-  grid_reduce<SumOp, 1>(acc, rs, BetaFinish32{S, inner_maxit});
+  grid_reduce<SumOp, 1>(acc, rs, BetaFinish32{S, delta, maxit, pin_row, scale, y, use_cond, upd_cond});
 }
 
+// x += S y + kappa (FP64); y = 0   -- only when a replacement is due
+__global__ void __launch_bounds__(256) k_mx_apply(int n, double* __restrict__ x, float* __restrict__ y,
+                                                  const double* __restrict__ scale,
+                                                  const PcgScalars* S) {
+  if (!S->upd || S->done) return;
+  const double kappa = S->kappa;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] += scale[i] * (double)y[i] + kappa;
+    y[i] = 0.f;
+  }
+}
+
+// p = r^ + beta p; sets the while-loop value
 __global__ void __launch_bounds__(256) k_mx_pupdate(int n, float* __restrict__ p,
                                                     const float* __restrict__ r,
                                                     const PcgScalars* S, int use_cond,
-                                                    cudaGraphConditionalHandle inner_cond) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(use_cond, inner_cond, !S->inner_done);
-  if (S->inner_done) return;
+                                                    cudaGraphConditionalHandle loop_cond) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(use_cond, loop_cond, !S->done);
+  if (S->done) return;
   const float beta = (float)S->beta;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     p[i] = fmaf(beta, p[i], r[i]);
-}
-
-// x += S y (+ the exact constant when the pinned-Neumann split is active)
-__global__ void __launch_bounds__(256) k_mx_correct(int n, double* __restrict__ x,
-                                                    const float* __restrict__ y,
-                                                    const double* __restrict__ scale,
-                                                    const PcgScalars* S, int pin_row, int use_cond,
-                                                    cudaGraphConditionalHandle outer_cond) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(use_cond, outer_cond, !S->done);
-  if (S->done) return;
-  const double kappa = (pin_row >= 0) ? S->kappa_c - scale[pin_row] * (double)y[pin_row] : 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    x[i] += scale[i] * (double)y[i] + kappa;
 }
 
 // scale = 1/sqrt(L_ii); lhat = S L S (columns outside the unknowns dropped to 0)
@@ -419,8 +512,9 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
   prm = params;
   if (prm.mode != GIPB200_PCG_FIXED && !(prm.tol > 0)) return fail(GIPB200_ERR_ARG, "tol must be > 0");
   if (prm.mode == GIPB200_PCG_MIXED) {
-    if (!(prm.inner_tol > 0 && prm.inner_tol < 1)) return fail(GIPB200_ERR_ARG, "inner_tol in (0,1)");
-    if (prm.inner_maxit <= 0 || prm.max_outer <= 0) return fail(GIPB200_ERR_ARG, "bad inner caps");
+    if (!(prm.inner_tol > 0 && prm.inner_tol < 1))
+      return fail(GIPB200_ERR_ARG, "inner_tol (replacement factor) must be in (0,1)");
+    if (prm.max_outer <= 0) return fail(GIPB200_ERR_ARG, "max_outer must be positive");
   }
   GIPB_TRY(reduce_scratch_alloc(&partials, &ticket, &rs));
   GIPB_TRY(sc.alloc(1));
@@ -437,7 +531,6 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
     GIPB_TRY(Ap32.alloc(n));
     GIPB_TRY(r32.alloc(n));
     GIPB_TRY(y32.alloc(n));
-    GIPB_TRY(rtrue.alloc(n));
     if (n > 0) {
       int b;
       GIPB_TRY(grid_blocks(256, n, 1, 0, &b));
@@ -470,6 +563,7 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
       }
       k_mx_lhat<<<blocks_spmv, 256, 0, s>>>(L->view(), scale.p, n, pin_row, pin_val, lhat.p);
       GIPB_LAUNCH_CHECK();
+      if (prm.mode == GIPB200_PCG_MIXED && !getenv("GIPB200_NO_COMPRESS")) GIPB_TRY(build_compressed(s));
     }
   } else {
     GIPB_TRY(dinv.alloc(n));
@@ -491,12 +585,119 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
   return GIPB200_OK;
 }
 
+int Pcg::build_compressed(cudaStream_t s) {
+  const int ns = L->nslices;
+  const long long nslots = L->nslots;
+  if (ns == 0 || nslots == 0) return GIPB200_OK;
+  std::vector<long long> sptr((size_t)ns + 1);
+  std::vector<int> col((size_t)nslots);
+  std::vector<float> val((size_t)nslots);
+  GIPB_CUDA(cudaMemcpyAsync(sptr.data(), L->sptr.p, sptr.size() * 8, cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaMemcpyAsync(col.data(), L->col.p, col.size() * 4, cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaMemcpyAsync(val.data(), lhat.p, val.size() * 4, cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> base((size_t)(nslots / 32), 0);
+  std::vector<unsigned char> plain((size_t)ns, 0);
+  std::vector<unsigned short> delta((size_t)nslots, 0);
+  long long comp_slots = 0;
+#pragma omp parallel for schedule(static) reduction(+ : comp_slots)
+  for (int sl = 0; sl < ns; ++sl) {
+    const long long b0 = sptr[sl];
+    const int len = (int)((sptr[sl + 1] - b0) >> 5);
+    bool ok = true;
+    for (int j = 0; j < len && ok; ++j) {
+      int lo = 0x7fffffff, hi = -1;
+      for (int l = 0; l < 32; ++l) {
+        const int c = col[b0 + 32LL * j + l];
+        if (c >= 0) {
+          lo = std::min(lo, c);
+          hi = std::max(hi, c);
+        }
+      }
+      if (hi < 0) lo = hi = 0;
+      if (hi - lo > 65535) ok = false;
+      base[(b0 >> 5) + j] = lo;
+      for (int l = 0; l < 32 && ok; ++l) {
+        const int c = col[b0 + 32LL * j + l];
+        delta[b0 + 32LL * j + l] = (unsigned short)(c >= 0 ? c - lo : 0);
+      }
+    }
+    plain[sl] = ok ? 0 : 1;
+    if (ok) comp_slots += 32LL * len;
+  }
+  cop.compressed_fraction = (double)comp_slots / (double)nslots;
+  if (cop.compressed_fraction < 0.5) return GIPB200_OK;  // not worth a second layout
+  // value table (index 0 = 0.0f, shared by padding and stored zeros)
+  std::vector<float> table(1, 0.0f);
+  std::vector<unsigned char> vidx((size_t)nslots, 0);
+  bool dict = true;
+  {
+    std::vector<unsigned> keys;
+    for (long long k = 0; k < nslots && dict; ++k) {
+      const float v = (col[k] >= 0) ? val[k] : 0.0f;
+      if (v == 0.0f) continue;
+      unsigned bits;
+      memcpy(&bits, &v, 4);
+      if (std::find(keys.begin(), keys.end(), bits) == keys.end()) {
+        if (keys.size() >= 255) {
+          dict = false;
+          break;
+        }
+        keys.push_back(bits);
+        table.push_back(v);
+      }
+    }
+    if (dict) {
+#pragma omp parallel for schedule(static)
+      for (long long k = 0; k < nslots; ++k) {
+        const float v = (col[k] >= 0) ? val[k] : 0.0f;
+        unsigned char id = 0;
+        if (v != 0.0f)
+          for (size_t t = 1; t < table.size(); ++t)
+            if (table[t] == v) {
+              id = (unsigned char)t;
+              break;
+            }
+        vidx[k] = id;
+      }
+    }
+  }
+  cop.dict = dict;
+  cop.ntable = (int)table.size();
+  GIPB_TRY(cop.delta.upload(delta.data(), delta.size(), s));
+  GIPB_TRY(cop.base.upload(base.data(), std::max<size_t>(base.size(), 1), s));
+  GIPB_TRY(cop.plain.upload(plain.data(), plain.size(), s));
+  GIPB_TRY(cop.table.upload(table.data(), table.size(), s));
+  if (dict) GIPB_TRY(cop.vidx.upload(vidx.data(), vidx.size(), s));
+  GIPB_CUDA(cudaStreamSynchronize(s));
+  const double slot_bytes = dict ? 3.0 : 6.0;
+  const double comp_nnz = (double)L->nnz * cop.compressed_fraction;
+  cop.bytes_per_launch = comp_nnz * slot_bytes + ((double)L->nnz - comp_nnz) * 8.0 +
+                         (double)base.size() * 4.0 * cop.compressed_fraction +
+                         (double)(ns + 1) * 9.0 + (double)L->nrows * 8.0;
+  cop.enabled = true;
+  return GIPB200_OK;
+}
+
+int Pcg::set_launch(int spmv_blocks, int vec_blocks) {
+  if (spmv_blocks < 0 || vec_blocks < 0 || spmv_blocks > kMaxReduceBlocks ||
+      vec_blocks > kMaxReduceBlocks)
+    return fail(GIPB200_ERR_ARG, "launch blocks must be in [0, %d]", kMaxReduceBlocks);
+  if (spmv_blocks) blocks_spmv = spmv_blocks;
+  else GIPB_TRY(grid_blocks(256, L->nslices * 32, 1, kMaxReduceBlocks, &blocks_spmv));
+  if (vec_blocks) blocks_vec = vec_blocks;
+  else GIPB_TRY(grid_blocks(256, std::max(n, 1), 4, kMaxReduceBlocks, &blocks_vec));
+  return GIPB200_OK;
+}
+
 int Pcg::read_flag(cudaStream_t s, int which, int* v) {
   GIPB_CUDA(cudaMemcpyAsync(h_sc, sc.p, sizeof(PcgScalars), cudaMemcpyDeviceToHost, s));
   GIPB_CUDA(cudaStreamSynchronize(s));
   *v = which == 0 ? h_sc->done : h_sc->inner_done;
   return GIPB200_OK;
 }
+
+static void launch_mx_spmv(const Pcg& P, const SellView<float>& A, cudaStream_t s);
 
 // ------------------------------------------------------------------ conditional while-nodes
 static bool capturing(cudaStream_t s) {
@@ -581,48 +782,68 @@ int Pcg::enqueue_fp64_graph(const double* b, double* x, const double* x0, cudaSt
 }
 
 // MIXED inside a graph:
-//   while(!done) { residual (sets done / inner_done); while(!inner_done) { A; B; C };
-//                  correct (sets the outer loop value) }
+//   residual (first); while(!done) { A; B; if(upd) { apply; residual }; C }
+// B decides a replacement on the device and sets the if-node; C sets the loop value.
+static int add_if(cudaStream_t cs, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  GIPB_CUDA(cudaStreamGetCaptureInfo(cs, &st, nullptr, &g, &deps, &nd));
+  alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+  memset(raw, 0, sizeof(raw));
+  cudaGraphNodeParams& p = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeIf;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  GIPB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+  *body = p.conditional.phGraph_out[0];
+  GIPB_CUDA(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
+  return GIPB200_OK;
+}
+
 int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaStream_t s) {
-  cudaGraphConditionalHandle ho;
-  GIPB_TRY(make_handle(s, 1, cudaGraphCondAssignDefault, &ho));
+  cudaGraphConditionalHandle hl;
+  GIPB_TRY(make_handle(s, 0, 0, &hl));
   if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
-  cudaGraph_t outer_body;
-  GIPB_TRY(add_while(s, ho, &outer_body));
+  GIPB_TRY(launch_mixed_residual(b, x, 1, s, 1, hl));
+  cudaGraph_t loop_body;
+  GIPB_TRY(add_while(s, hl, &loop_body));
   const SellView<float> A{L->nrows, L->nslices, L->sptr.p, L->col.p, lhat.p};
   cudaStream_t os = body_stream[0], is = body_stream[1];
-  GIPB_CUDA(cudaStreamBeginCaptureToGraph(os, outer_body, nullptr, nullptr, 0,
+  GIPB_CUDA(cudaStreamBeginCaptureToGraph(os, loop_body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
   int st = [&]() -> int {
-    cudaGraphConditionalHandle hi;
-    GIPB_TRY(make_handle(os, 0, 0, &hi));
-    k_mx_residual<<<blocks_spmv, 256, 0, os>>>(L->view(), x, b, scale.p, rtrue.p, r32.p, p32.p,
-                                                y32.p, sc.p, rs, prm.tol, prm.inner_tol,
-                                                prm.max_outer, pin_row, pin_val, 1, hi);
+    cudaGraphConditionalHandle hu;
+    GIPB_TRY(make_handle(os, 0, 0, &hu));
+    launch_mx_spmv(*this, A, os);
+    k_mx_update<<<blocks_vec, 256, 0, os>>>(n, y32.p, r32.p, p32.p, Ap32.p, sc.p, rs,
+                                             prm.inner_tol, prm.maxit, pin_row, scale.p, 1, hu);
     GIPB_LAUNCH_CHECK();
-    cudaGraph_t inner_body;
-    GIPB_TRY(add_while(os, hi, &inner_body));
-    GIPB_CUDA(cudaStreamBeginCaptureToGraph(is, inner_body, nullptr, nullptr, 0,
+    cudaGraph_t if_body;
+    GIPB_TRY(add_if(os, hu, &if_body));
+    GIPB_CUDA(cudaStreamBeginCaptureToGraph(is, if_body, nullptr, nullptr, 0,
                                             cudaStreamCaptureModeRelaxed));
-    k_mx_spmv_dot<<<blocks_spmv, 256, 0, is>>>(A, p32.p, Ap32.p, sc.p, rs);
-    k_mx_update<<<blocks_vec, 256, 0, is>>>(n, y32.p, r32.p, p32.p, Ap32.p, sc.p, rs,
-                                             prm.inner_maxit);
-    k_mx_pupdate<<<blocks_vec, 256, 0, is>>>(n, p32.p, r32.p, sc.p, 1, hi);
+    k_mx_apply<<<blocks_vec, 256, 0, is>>>(n, x, y32.p, scale.p, sc.p);
+    int rst = launch_mixed_residual(b, x, 0, is, 0, 0);
     cudaError_t le = cudaGetLastError();
     cudaGraph_t out = nullptr;
     GIPB_CUDA(cudaStreamEndCapture(is, &out));
+    if (rst != GIPB200_OK) return rst;
     if (le != cudaSuccess)
-      return fail(GIPB200_ERR_CUDA, "launch in inner body: %s", cudaGetErrorString(le));
-    k_mx_correct<<<blocks_vec, 256, 0, os>>>(n, x, y32.p, scale.p, sc.p, pin_row, 1, ho);
+      return fail(GIPB200_ERR_CUDA, "launch in replacement body: %s", cudaGetErrorString(le));
+    k_mx_pupdate<<<blocks_vec, 256, 0, os>>>(n, p32.p, r32.p, sc.p, 1, hl);
     GIPB_LAUNCH_CHECK();
     return GIPB200_OK;
   }();
   cudaGraph_t out = nullptr;
   cudaError_t ce = cudaStreamEndCapture(os, &out);
   if (st != GIPB200_OK) return st;
-  if (ce != cudaSuccess) return fail(GIPB200_ERR_CUDA, "outer body capture: %s", cudaGetErrorString(ce));
-  launches += 5;
+  if (ce != cudaSuccess) return fail(GIPB200_ERR_CUDA, "loop body capture: %s", cudaGetErrorString(ce));
+  launches += 4;
   return GIPB200_OK;
 }
 
@@ -653,39 +874,52 @@ int Pcg::enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t
   return GIPB200_OK;
 }
 
+static void launch_mx_spmv(const Pcg& P, const SellView<float>& A, cudaStream_t s) {
+  const CompressedOp& c = P.cop;
+  if (c.enabled && c.dict)
+    k_mxc_spmv_dot<true><<<P.blocks_spmv, 256, 0, s>>>(A, c.delta.p, c.vidx.p, c.base.p, c.plain.p,
+                                                       c.table.p, c.ntable, P.p32.p, P.Ap32.p,
+                                                       P.sc.p, P.rs);
+  else if (c.enabled)
+    k_mxc_spmv_dot<false><<<P.blocks_spmv, 256, 0, s>>>(A, c.delta.p, c.vidx.p, c.base.p, c.plain.p,
+                                                        c.table.p, c.ntable, P.p32.p, P.Ap32.p,
+                                                        P.sc.p, P.rs);
+  else
+    k_mx_spmv_dot<<<P.blocks_spmv, 256, 0, s>>>(A, P.p32.p, P.Ap32.p, P.sc.p, P.rs);
+}
+
+int Pcg::launch_mixed_residual(const double* b, const double* x, int first, cudaStream_t s,
+                               int use_cond, cudaGraphConditionalHandle h) {
+  k_mx_residual<<<blocks_spmv, 256, 0, s>>>(L->view(), x, b, scale.p, r32.p, p32.p, y32.p, sc.p,
+                                             rs, first, prm.tol, prm.inner_tol, prm.maxit,
+                                             prm.max_outer, pin_row, pin_val, use_cond, h);
+  GIPB_LAUNCH_CHECK();
+  launches += 1;
+  return GIPB200_OK;
+}
+
 int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_t s,
                        bool host_sync) {
   if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
   const SellView<float> A{L->nrows, L->nslices, L->sptr.p, L->col.p, lhat.p};
+  GIPB_TRY(launch_mixed_residual(b, x, 1, s, 0, 0));
   const int poll = 16;
-  for (int o = 0; o <= prm.max_outer; ++o) {
-    k_mx_residual<<<blocks_spmv, 256, 0, s>>>(L->view(), x, b, scale.p, rtrue.p, r32.p, p32.p,
-                                               y32.p, sc.p, rs, prm.tol, prm.inner_tol,
-                                               prm.max_outer, pin_row, pin_val, 0, 0);
+  for (int k = 0; k < prm.maxit; ++k) {
+    launch_mx_spmv(*this, A, s);
+    k_mx_update<<<blocks_vec, 256, 0, s>>>(n, y32.p, r32.p, p32.p, Ap32.p, sc.p, rs, prm.inner_tol,
+                                            prm.maxit, pin_row, scale.p, 0, 0);
+    k_mx_apply<<<blocks_vec, 256, 0, s>>>(n, x, y32.p, scale.p, sc.p);
     GIPB_LAUNCH_CHECK();
-    launches += 1;
-    if (host_sync) {
+    GIPB_TRY(launch_mixed_residual(b, x, 0, s, 0, 0));
+    k_mx_pupdate<<<blocks_vec, 256, 0, s>>>(n, p32.p, r32.p, sc.p, 0, 0);
+    GIPB_LAUNCH_CHECK();
+    launches += 4;
+    if (host_sync && (k + 1) % poll == 0) {
       int d;
       GIPB_TRY(read_flag(s, 0, &d));
       if (d) break;
     }
-    for (int k = 0; k < prm.inner_maxit; ++k) {
-      k_mx_spmv_dot<<<blocks_spmv, 256, 0, s>>>(A, p32.p, Ap32.p, sc.p, rs);
-      k_mx_update<<<blocks_vec, 256, 0, s>>>(n, y32.p, r32.p, p32.p, Ap32.p, sc.p, rs,
-                                              prm.inner_maxit);
-      k_mx_pupdate<<<blocks_vec, 256, 0, s>>>(n, p32.p, r32.p, sc.p, 0, 0);
-      GIPB_LAUNCH_CHECK();
-      launches += 3;
-      if (host_sync && (k + 1) % poll == 0) {
-        int d;
-        GIPB_TRY(read_flag(s, 1, &d));
-        if (d) break;
-      }
-    }
-    k_mx_correct<<<blocks_vec, 256, 0, s>>>(n, x, y32.p, scale.p, sc.p, pin_row, 0, 0);
-    GIPB_LAUNCH_CHECK();
-    launches += 1;
   }
   return GIPB200_OK;
 }
@@ -715,7 +949,15 @@ int Pcg::time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* 
   // that would skip work: p.Ap > 0 for the SPD operator and a nonzero p)
   for (int k = 0; k <= reps; ++k) {
     if (k == 1) GIPB_CUDA(cudaEventRecord(e0, s));
-    if (mixed)
+    if (mixed && cop.enabled && cop.dict)
+      k_mxc_spmv_dot<true><<<blocks_spmv, 256, 0, s>>>(A, cop.delta.p, cop.vidx.p, cop.base.p,
+                                                       cop.plain.p, cop.table.p, cop.ntable, p32.p,
+                                                       tAp32.p, tsc.p, rs);
+    else if (mixed && cop.enabled)
+      k_mxc_spmv_dot<false><<<blocks_spmv, 256, 0, s>>>(A, cop.delta.p, cop.vidx.p, cop.base.p,
+                                                        cop.plain.p, cop.table.p, cop.ntable, p32.p,
+                                                        tAp32.p, tsc.p, rs);
+    else if (mixed)
       k_mx_spmv_dot<<<blocks_spmv, 256, 0, s>>>(A, p32.p, tAp32.p, tsc.p, rs);
     else
       k_pcg_spmv_dot<<<blocks_spmv, 256, 0, s>>>(L->view(), p.p, tAp.p, tsc.p, rs,
@@ -733,6 +975,7 @@ int Pcg::time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* 
   const double vbytes = mixed ? 4.0 : 8.0;
   *bytes = (double)L->nnz * (vbytes + 4.0) + (double)(L->nslices + 1) * 8.0 +
            (double)L->nrows * 2.0 * vbytes;
+  if (mixed && cop.enabled) *bytes = cop.bytes_per_launch;
   return GIPB200_OK;
 }
 

@@ -22,7 +22,29 @@ struct PcgScalars {
   int total_inner;  // MIXED: inner iterations summed over cycles
   int pad[2];
   double rsum;      // MIXED: sum of the FP64 residual (pinned-Neumann deflation)
-  double kappa_c;   // MIXED: sum(r)/pin, the pinned cell's exact correction
+  double kappa_c;   // MIXED: sum(r)/pin of the current segment
+  double kappa;     // MIXED: constant added to x at the next replacement
+  double maxr2;     // MIXED: largest FP32 r^.r^ since the last replacement
+  double trig;      // MIXED: FP32 r^.r^ level that predicts convergence
+  int upd;          // MIXED: replace the FP32 residual by the FP64 one now
+  int pad2;
+};
+
+// The FP32 operator of the mixed form, compressed without loss: per slot a 16-bit
+// column delta from a per-(slice, slot) base and, when the operator has at most 255
+// distinct values, an 8-bit index into a value table (index 0 = 0.0f, the padding).
+// Slices whose column spread exceeds 16 bits stay in the plain layout.
+struct CompressedOp {
+  bool enabled = false;
+  bool dict = false;
+  DevBuf<unsigned short> delta;
+  DevBuf<unsigned char> vidx;
+  DevBuf<int> base;            // index (sptr[s] / 32 + j)
+  DevBuf<unsigned char> plain; // per slice
+  DevBuf<float> table;
+  int ntable = 0;
+  double compressed_fraction = 0.0;
+  double bytes_per_launch = 0.0;  // stored bytes the kernel streams (+ vectors)
 };
 
 struct Pcg {
@@ -35,7 +57,8 @@ struct Pcg {
   DevBuf<float> lhat;        // S L S values in L's sliced layout (FP32)
   DevBuf<double> scale;      // S = 1/sqrt(L_ii)
   DevBuf<float> p32, Ap32, r32, y32;
-  DevBuf<double> rtrue;
+  CompressedOp cop;
+  int build_compressed(cudaStream_t s);
   // Pinned-Neumann structure of L (every row sums to zero except one pinned row p with
   // sum pin > 0): the FP32 inner solve then runs on the pure-Neumann part and the
   // constant mode is restored exactly from the pin equation.
@@ -48,6 +71,8 @@ struct Pcg {
   ReduceScratch rs{};
   PcgScalars* h_sc = nullptr;  // pinned
   int blocks_spmv = 1, blocks_vec = 1;
+  // launch shape overrides (autotuning): 0 = default grid
+  int set_launch(int spmv_blocks, int vec_blocks);
   long long launches = 0;      // kernels enqueued by this solver (host count)
   // streams that capture the bodies of the conditional while-nodes
   cudaStream_t body_stream[2] = {nullptr, nullptr};
@@ -68,6 +93,8 @@ struct Pcg {
   int read_flag(cudaStream_t s, int which, int* v);
   int enqueue_fp64_graph(const double* b, double* x, const double* x0, cudaStream_t s);
   int enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaStream_t s);
+  int launch_mixed_residual(const double* b, const double* x, int first, cudaStream_t s,
+                            int use_cond, cudaGraphConditionalHandle h);
 };
 
 }  // namespace gipb200

@@ -205,10 +205,15 @@ class PcgSolver:
 class DnsEngine:
     """``GIP_DNS`` on the device: ``advance(n)`` is ``integrate()`` for n timesteps."""
 
-    def __init__(self, case: GipCase, rho: float = 1.0, gamma: float = 1e-3,
+    def __init__(self, case: Optional[GipCase], rho: float = 1.0, gamma: float = 1e-3,
                  pcg_mode: str = "fixed", maxit: int = 100, tol: float = 1e-6,
                  inner_tol: float = 1e-3, inner_maxit: int = 2000, max_outer: int = 30,
-                 use_graph: bool = True, reorder: bool = False):
+                 use_graph: bool = True, reorder: bool = False, _handle=None, _sizes=None):
+        self._owned = _handle is None
+        if _handle is not None:  # a view of an engine owned elsewhere (a batch instance)
+            self.handle = _handle
+            self.n_inner, self.n_owned, self.n_faces = _sizes
+            return
         lib = L.load()
         keep: list = []
         ops = L.DnsOps(**{n: _host_csr(case.ops[n], keep) for n in L.DNS_OPS},
@@ -229,12 +234,14 @@ class DnsEngine:
 
     def history(self) -> Dict[str, np.ndarray]:
         steps = C.c_int()
-        L.call("gipb200_dns_history", self.handle, C.byref(steps), None, None, None, None, None)
+        L.call("gipb200_dns_history", self.handle, C.byref(steps), None, None, None, None, None,
+               None)
         n = steps.value
         out = {"time": np.zeros(n), "dt": np.zeros(n), "massr": np.zeros(n),
-               "iters": np.zeros(n, np.int32), "rr": np.zeros(n)}
+               "iters": np.zeros(n, np.int32), "rr": np.zeros(n), "outer": np.zeros(n, np.int32)}
         L.call("gipb200_dns_history", self.handle, C.byref(steps), _hptr(out["time"]),
-               _hptr(out["dt"]), _hptr(out["massr"]), _hptr(out["iters"]), _hptr(out["rr"]))
+               _hptr(out["dt"]), _hptr(out["massr"]), _hptr(out["iters"]), _hptr(out["rr"]),
+               _hptr(out["outer"]))
         return out
 
     def field(self, name: str) -> np.ndarray:
@@ -275,9 +282,74 @@ class DnsEngine:
         L.call("gipb200_dns_scalars", self.handle, C.byref(dt), C.byref(sg), C.byref(t))
         return {"dt": dt.value, "sigma": sg.value, "time": t.value}
 
+    def info(self) -> dict:
+        i = L.DnsInfo()
+        L.call("gipb200_dns_get_info", self.handle, C.byref(i))
+        return {k: getattr(i, k) for k, _ in L.DnsInfo._fields_}
+
+    def snapshot(self, restore: bool = False, stream=None) -> None:
+        """Save (or restore) the whole timestep state on the device."""
+        L.call("gipb200_dns_snapshot", self.handle, int(restore), _stream(stream))
+
+    def set_launch(self, spmv_blocks: int = 0, vec_blocks: int = 0) -> None:
+        L.call("gipb200_dns_set_launch", self.handle, spmv_blocks, vec_blocks)
+
+    def close(self):
+        if getattr(self, "handle", None) and getattr(self, "_owned", True):
+            L.load().gipb200_dns_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def dns_params(rho: float = 1.0, gamma: float = 1e-3, pcg_mode: str = "fixed", maxit: int = 100,
+               tol: float = 1e-6, inner_tol: float = 1e-3, inner_maxit: int = 2000,
+               max_outer: int = 30, use_graph: bool = True, reorder: bool = False) -> L.DnsParams:
+    return L.DnsParams(rho, gamma, pcg_params(pcg_mode, maxit, tol, inner_tol, inner_maxit,
+                                              max_outer), int(use_graph), int(reorder))
+
+
+class DnsBatch:
+    """Many independent cases advanced together: one graph launch per timestep whose
+    parallel branches are the instances' steps (each with its own convergence loops)."""
+
+    def __init__(self, cases, params):
+        n = len(cases)
+        keep: list = []
+        ops = [L.DnsOps(**{k: _host_csr(c.ops[k], keep) for k in L.DNS_OPS},
+                        n_inner=c.n_inner, n_owned=c.n_owned, n_faces=c.n_faces) for c in cases]
+        fields = [{k: np.ascontiguousarray(c.fields[k], np.float64)
+                   for k in ("u", "v", "w", "dxs")} for c in cases]
+        keep += fields
+        OpsArr = C.POINTER(L.DnsOps) * n
+        PtrArr = C.c_void_p * n
+        ops_p = OpsArr(*[C.pointer(o) for o in ops])
+        arr = {k: PtrArr(*[f[k].ctypes.data for f in fields]) for k in ("u", "v", "w", "dxs")}
+        prm = (L.DnsParams * n)(*params)
+        h = C.c_void_p()
+        L.call("gipb200_batch_create", n, C.cast(ops_p, C.c_void_p), C.cast(arr["u"], C.c_void_p),
+               C.cast(arr["v"], C.c_void_p), C.cast(arr["w"], C.c_void_p),
+               C.cast(arr["dxs"], C.c_void_p), prm, C.byref(h))
+        self.handle = h
+        self.instances = []
+        for i, c in enumerate(cases):
+            d = C.c_void_p()
+            L.call("gipb200_batch_instance", h, i, C.byref(d))
+            self.instances.append(DnsEngine(None, _handle=d, _sizes=(c.n_inner, c.n_owned,
+                                                                      c.n_faces)))
+
+    def advance(self, nsteps: int, stream=None) -> None:
+        L.call("gipb200_batch_advance", self.handle, nsteps, _stream(stream))
+
     def close(self):
         if getattr(self, "handle", None):
-            L.load().gipb200_dns_destroy(self.handle)
+            for e in self.instances:
+                e.handle = None
+            L.load().gipb200_batch_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

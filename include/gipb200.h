@@ -115,21 +115,23 @@ typedef struct gipb200_pcg_s* gipb200_pcg;
 enum {
   GIPB200_PCG_FIXED = 0,  /* exactly maxit iterations: GIP_LinearSolver.h:85-116          */
   GIPB200_PCG_TOL = 1,    /* stop when ||r||_2 <= tol ||b||_2 (r recursive)                */
-  GIPB200_PCG_MIXED = 2   /* FP32 inner PCG inside FP64 iterative refinement, stop at tol  */
+  GIPB200_PCG_MIXED = 2   /* FP32 PCG with FP64 residual replacement (iterative refinement
+                             that keeps the Krylov direction), stop at tol                  */
 };
 
 typedef struct {
   int mode;          /* GIPB200_PCG_*                                                */
   int maxit;         /* FIXED: iterations; TOL/MIXED: cap on (inner) iterations      */
   double tol;        /* TOL/MIXED: relative 2-norm residual target                   */
-  double inner_tol;  /* MIXED: inner solve reduces its residual by this factor       */
-  int inner_maxit;   /* MIXED: cap per inner solve                                   */
-  int max_outer;     /* MIXED: cap on refinement cycles                              */
+  double inner_tol;  /* MIXED: the FP64 true residual replaces the FP32 one when the
+                        FP32 residual has fallen by this factor (reliable update)   */
+  int inner_maxit;   /* MIXED: unused (kept for layout)                              */
+  int max_outer;     /* MIXED: cap on residual replacements                          */
 } gipb200_pcg_params;
 
 typedef struct {
   int iterations;        /* FIXED/TOL: PCG iterations; MIXED: inner iterations summed */
-  int outer;             /* MIXED: refinement cycles                                  */
+  int outer;             /* MIXED: FP64 residual replacements                         */
   int status;            /* GIPB200_OK / BREAKDOWN / NOT_CONVERGED                    */
   double rr;             /* r.r at exit (MIXED: true FP64 residual)                   */
   double bb;             /* b.b                                                       */
@@ -180,10 +182,11 @@ int gipb200_dns_destroy(gipb200_dns E);
 /* GIP_DNS::integrate (GIP_DNS.h:99-113): advances nsteps timesteps on `stream`; the first
  * call also computes the initial dt.  No host synchronisation inside. */
 int gipb200_dns_advance(gipb200_dns E, int nsteps, void* stream);
-/* Per-step history of all steps so far (host arrays of length >= steps taken):
- * time, dt used, massr (GIP_DNS.h:399-404), PCG iterations, final r.r. */
+/* Per-step history of all steps so far (host arrays of length >= steps taken, any may
+ * be NULL): time, dt used, massr (GIP_DNS.h:399-404), PCG iterations (MIXED: FP32
+ * iterations), final r.r, MIXED residual replacements (FP64 true-residual updates). */
 int gipb200_dns_history(gipb200_dns E, int* steps_taken, double* h_time, double* h_dt,
-                        double* h_massr, int* h_iters, double* h_rr);
+                        double* h_massr, int* h_iters, double* h_rr, int* h_outer);
 /* Copies a field to the host: "u","v","w","p","p0","mf","ax0","ay0","az0","gpx",... */
 int gipb200_dns_get_field(gipb200_dns E, const char* name, double* h_out, int n);
 /* Copies h_in[0:n) into a field at `offset` on `stream` (no host synchronisation; the
@@ -199,6 +202,28 @@ int gipb200_dns_copy_field(gipb200_dns E, const char* name, double* d_out, int n
 /* Current dt, sigma=1/dt and simulated time. */
 int gipb200_dns_scalars(gipb200_dns E, double* dt, double* sigma, double* time);
 
+typedef struct {
+  int reordered;               /* engine runs in its breadth-first numbering            */
+  int pin_row;                 /* MIXED: detected pinned-Neumann row of L (-1: none)     */
+  int compressed;              /* MIXED: FP32 operator stored compressed                 */
+  int value_table;             /* MIXED: values through an 8-bit table                   */
+  double compressed_fraction;  /* MIXED: share of slots in compressed slices             */
+  long long slots_L;           /* sliced slots of L (stored nonzeros plus padding)       */
+  long long nnz_L;
+} gipb200_dns_info;
+int gipb200_dns_get_info(gipb200_dns E, gipb200_dns_info* info);
+
+/* Device-side checkpoint of the whole timestep state (every GIP_DNS vector, C's values,
+ * dt, sigma, time, step counter): restore = 0 saves, 1 restores the last save.  Steps
+ * taken after a restore overwrite the history from the saved step on. */
+int gipb200_dns_snapshot(gipb200_dns E, int restore, void* stream);
+
+/* Launch shape of the PCG kernels (SpMV+dot grid, vector-kernel grid; 0 = default,
+ * at most 8192 blocks of 256 threads).  A different shape changes the order of the
+ * dot-product partial sums (results stay deterministic for a given shape).  The next
+ * step re-captures its graph. */
+int gipb200_dns_set_launch(gipb200_dns E, int spmv_blocks, int vec_blocks);
+
 /* Number of this library's kernels the engine has launched so far (a graph launch counts
  * the kernels it holds). */
 int gipb200_dns_launch_count(gipb200_dns E, long long* count);
@@ -213,6 +238,55 @@ enum {
  * product written once).  Leaves the engine's fields untouched. */
 int gipb200_dns_kernel_time(gipb200_dns E, int kernel, int reps, void* stream, double* avg_ms,
                             double* bytes);
+
+/* ------------------------------------------------------------------ batched cavities */
+/* No counterpart in the reference.  Many independent cases (uneven sizes, own Reynolds
+ * numbers and parameters) advanced together: each timestep is one CUDA graph launch whose
+ * parallel branches are the instances' steps; every branch keeps its own device-decided
+ * PCG loops, so each instance stops at its own convergence (per-instance masks). */
+typedef struct gipb200_batch_s* gipb200_batch;
+int gipb200_batch_create(int n, const gipb200_dns_ops* const* ops, const double* const* h_u,
+                         const double* const* h_v, const double* const* h_w,
+                         const double* const* h_dxs, const gipb200_dns_params* params,
+                         gipb200_batch* out);
+int gipb200_batch_destroy(gipb200_batch B);
+/* Instance i as an engine handle (history, fields, launch shape); owned by the batch. */
+int gipb200_batch_instance(gipb200_batch B, int i, gipb200_dns* out);
+/* nsteps timesteps of every instance, one graph launch each, on `stream`. */
+int gipb200_batch_advance(gipb200_batch B, int nsteps, void* stream);
+
+/* ------------------------------------------------------------------ discrete adjoint */
+/* No counterpart in the reference (GIP has no derivatives).  FP64 discrete adjoint of
+ * the timestep above with the CFL steps frozen: J = 1/2 sum_i vol_i |u_i|^2 over the
+ * inner cells after `nsteps` steps; gradients with respect to the lid's ghost velocities
+ * (u on the listed ghost cells) and the viscosity nu = nu_scale * nu0 (D scales with
+ * nu).  The forward keeps checkpoints every `checkpoint_every` steps; the backward
+ * recomputes each segment and applies the transposed step: transposed SpMVs over CSR
+ * transposes built at creation, one adjoint Poisson solve per step with the same PCG
+ * (L is symmetric), and the convective adjoint dJ/dmf = -Ec^T z. */
+typedef struct gipb200_adjoint_s* gipb200_adjoint;
+
+typedef struct {
+  double rho;            /* density                                                  */
+  double gamma;          /* CFL viscosity parameter (dt is frozen after the forward)  */
+  double nu0;            /* viscosity baked into D                                    */
+  double tol;            /* relative tolerance of every Poisson solve (forward, adjoint) */
+  int maxit;             /* PCG iteration cap                                         */
+  int checkpoint_every;  /* forward checkpoint spacing, in steps                      */
+} gipb200_adjoint_params;
+
+int gipb200_adjoint_create(const gipb200_dns_ops* ops, const double* h_u0, const double* h_v0,
+                           const double* h_w0, const double* h_dxs, const double* h_volume,
+                           const int* h_lid_cells, int n_lid, const gipb200_adjoint_params* prm,
+                           gipb200_adjoint* out);
+int gipb200_adjoint_destroy(gipb200_adjoint A);
+/* Forward from the initial fields with the lid values applied.  dt_given = 1: use the
+ * nsteps steps in h_dt; dt_given = 0: GIP's CFL chooses them and they are written to h_dt
+ * when it is not NULL.  *h_J = kinetic energy after the last step. */
+int gipb200_adjoint_forward(gipb200_adjoint A, const double* h_lid, double nu_scale, int nsteps,
+                            double* h_dt, int dt_given, double* h_J);
+/* Gradients of the last forward's J: h_grad_lid[n_lid], *h_grad_nu. */
+int gipb200_adjoint_backward(gipb200_adjoint A, double* h_grad_lid, double* h_grad_nu);
 
 #ifdef __cplusplus
 }

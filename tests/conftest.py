@@ -15,6 +15,7 @@ REF_BIN = os.path.join(REPO, "oracle", "_ref", "gip_ref_cpu")
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+    config.addinivalue_line("markers", "slow: a full-size configuration check (minutes)")
 
 
 def have_c100k() -> bool:

@@ -79,7 +79,31 @@ def main():
             lines2 = run_ref(td, "CAV", 2, steps, "-", re_)
         np.savez_compressed(os.path.join(HERE, f"cavity{n}_ref.npz"), lines=np.array(lines),
                             lines_np2=np.array(lines2), re=re_, steps=steps, **fields)
+
+    # the first configuration: 48^3, Re 100, 10 steps; GIP at 4 slab ranks and at 1 rank.
+    # Only per-step lines and field checksums are kept (the fields are 110k cells each).
+    import json
+    case, meta = cavity.generate(48, re=100.0)
+    out = {"n": 48, "re": 100.0, "steps": 10}
+    with tempfile.TemporaryDirectory() as td:
+        formats.write_case(td, "CAV48", [case])
+        dump = os.path.join(td, "dump")
+        out["lines_np1"] = run_ref(td, "CAV48", 1, 10, dump, 100.0)
+        out["checksums_np1"] = {k: _checksums(np.fromfile(f"{dump}.{k}.0.f64"), case.n_inner)
+                                for k in ("u", "v", "w", "p", "mf")}
+        parts = formats.split_ranks(case, cavity.slab_partition(meta, 4), 4)
+        formats.write_case(td, "CAV48", parts)
+        out["lines_np4"] = run_ref(td, "CAV48", 4, 10, "-", 100.0)
+    with open(os.path.join(HERE, "cavity48_ref.json"), "w") as f:
+        json.dump(out, f, indent=1)
     print("goldens written to", HERE)
+
+
+def _checksums(x: np.ndarray, n_inner: int) -> dict:
+    """Order-free summaries of a field: L1, L2 and max norms of the inner part."""
+    xi = x[:n_inner]
+    return {"l1": float(np.abs(xi).sum()), "l2": float(np.sqrt((xi * xi).sum())),
+            "max": float(np.abs(xi).max())}
 
 
 if __name__ == "__main__":

@@ -71,3 +71,18 @@ def test_oracle_pcg_fixed_equals_reference_formula(oracle_mod):
     L, b = cavity.poisson_problem(6, seed=2)
     _, it, _ = oracle_mod.pcg(L, b, np.zeros(L.nrows), maxit=17, mode=0)
     assert it == 17
+
+
+def test_torch_adjoint_reference_forward_matches_oracle(oracle_mod):
+    # the torch timestep used as the gradient reference reproduces the oracle's state
+    import torch
+    from adjoint_reference import kinetic_energy
+    case, meta = cavity.generate(6, re=100.0)
+    d = oracle_mod.OracleDNS(case, gamma=1e-2, cg_maxit=5000, cg_mode=1, cg_tol=1e-14)
+    h = d.run(4)
+    N = case.n_inner
+    vol = np.full(N, meta.h ** 3)
+    J_or = 0.5 * (vol * (d.vec["u"][:N] ** 2 + d.vec["v"][:N] ** 2 + d.vec["w"][:N] ** 2)).sum()
+    lid = case.fields["u"][meta.lid_ghosts]
+    J = kinetic_energy(case, meta.lid_ghosts, torch.tensor(lid), torch.tensor(1.0), h["dt"], vol)
+    assert abs(J.item() - J_or) <= 1e-9 * abs(J_or)
