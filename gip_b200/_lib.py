@@ -96,6 +96,8 @@ _SIGNATURES = {
     "gipb200_pcg_create": (_I, [_VP, _I, C.POINTER(PcgParams), C.POINTER(_VP)]),
     "gipb200_pcg_destroy": (_I, [_VP]),
     "gipb200_pcg_solve": (_I, [_VP, _VP, _VP, _VP, _VP, C.POINTER(PcgResult)]),
+    "gipb200_pcg_solve_static": (_I, [_I, _I, _VP, _VP, _VP, _VP, _VP, _VP, _I, _I, _D, _VP,
+                                      _VP]),
     "gipb200_adjoint_create": (_I, [C.POINTER(DnsOps), _VP, _VP, _VP, _VP, _VP, _VP, _I,
                                     C.POINTER(AdjointParams), C.POINTER(_VP)]),
     "gipb200_adjoint_destroy": (_I, [_VP]),

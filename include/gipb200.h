@@ -145,6 +145,23 @@ int gipb200_pcg_destroy(gipb200_pcg S);
 int gipb200_pcg_solve(gipb200_pcg S, const double* d_b, double* d_x, const double* d_x0,
                       void* stream, gipb200_pcg_result* h_result);
 
+/* No counterpart in the reference.  A Jacobi-PCG solve for callers that cannot allocate
+ * device memory at solve time (a framework-owned arena or caching allocator, code that
+ * must not call cudaMalloc because it synchronises the device, embedders without
+ * library handles).  The caller passes a device CSR operator (n rows), b (n), x and x0
+ * (n_all = inner plus ghost cells, ghosts copied from x0), and d_stats (4 doubles out:
+ * iterations, r.r, b.b, status).  mode: GIPB200_PCG_FIXED (exactly maxit iterations, as
+ * GIP's solver) or GIPB200_PCG_TOL (stop at tol; maxit masked iterations are launched).
+ * The solver's vectors and reductions use one file-scope device array of 8 MiB that
+ * every GPU loading the library keeps until exit: n_all above 262144 is rejected with
+ * GIPB200_ERR_ARG.  All calls share that array, so calls that overlap on the GPU race;
+ * serialise them.  The first call on a device (with that device current) resolves the
+ * array's address and clears it; make that first call before any stream capture. */
+int gipb200_pcg_solve_static(int n, int n_all, const int* d_rowptr, const int* d_col,
+                             const double* d_val, const double* d_b, double* d_x,
+                             const double* d_x0, int mode, int maxit, double tol,
+                             double* d_stats, void* stream);
+
 /* ------------------------------------------------------------------ timestep engine */
 typedef struct gipb200_dns_s* gipb200_dns;
 
