@@ -47,6 +47,11 @@ class DnsParams(C.Structure):
                 ("use_graph", C.c_int), ("reorder", C.c_int)]
 
 
+class PcgInfo(C.Structure):
+    _fields_ = [("pin_row", C.c_int), ("compressed", C.c_int), ("value_table", C.c_int),
+                ("compressed_fraction", C.c_double)]
+
+
 class DnsInfo(C.Structure):
     _fields_ = [("reordered", C.c_int), ("pin_row", C.c_int), ("compressed", C.c_int),
                 ("value_table", C.c_int), ("compressed_fraction", C.c_double),
@@ -95,6 +100,8 @@ _SIGNATURES = {
     "gipb200_matrix_inverse_diagonal": (_I, [_VP, _VP, C.POINTER(_I)]),
     "gipb200_pcg_create": (_I, [_VP, _I, C.POINTER(PcgParams), C.POINTER(_VP)]),
     "gipb200_pcg_destroy": (_I, [_VP]),
+    "gipb200_pcg_get_info": (_I, [_VP, C.POINTER(PcgInfo)]),
+    "gipb200_pcg_kernel_time": (_I, [_VP, _I, _VP, C.POINTER(_D), C.POINTER(_D)]),
     "gipb200_pcg_solve": (_I, [_VP, _VP, _VP, _VP, _VP, C.POINTER(PcgResult)]),
     "gipb200_pcg_solve_static": (_I, [_I, _I, _VP, _VP, _VP, _VP, _VP, _VP, _I, _I, _D, _VP,
                                       _VP]),

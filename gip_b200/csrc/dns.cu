@@ -870,7 +870,7 @@ int gipb200_dns_get_info(gipb200_dns Dh, gipb200_dns_info* info) {
   info->reordered = E.reordered;
   info->pin_row = E.pcg.pin_row;
   info->compressed = E.pcg.cop.enabled;
-  info->value_table = E.pcg.cop.dict;
+  info->value_table = E.pcg.cop.index_bits;
   info->compressed_fraction = E.pcg.cop.compressed_fraction;
   info->slots_L = E.L.nslots;
   info->nnz_L = E.L.nnz;

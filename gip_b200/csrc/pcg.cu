@@ -290,7 +290,7 @@ struct AlphaFinish32 {
   }
 };
 
-__global__ void __launch_bounds__(256) k_mx_spmv_dot(SellView<float> A, const float* __restrict__ p,
+__global__ void __launch_bounds__(256, 8) k_mx_spmv_dot(SellView<float> A, const float* __restrict__ p,
                                                      float* __restrict__ Ap, PcgScalars* S,
                                                      ReduceScratch rs) {
   if (S->done) return;
@@ -309,60 +309,63 @@ __global__ void __launch_bounds__(256) k_mx_spmv_dot(SellView<float> A, const fl
   grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
 }
 
-// Same product as k_mx_spmv_dot from the compressed layout: identical gathers and FMA
-// order, so identical results.
-template <bool DICT>
-__global__ void __launch_bounds__(256) k_mxc_spmv_dot(SellView<float> A,
-                                                      const unsigned short* __restrict__ delta,
-                                                      const unsigned char* __restrict__ vidx,
+// Same product as k_mx_spmv_dot from the packed layout: the same gathers and the same
+// FMA order (slot by slot; padding and zeros add x*0 there and nothing here), so the same
+// results.  A warp owns a slice; in a packed slice each lane loads its row's 16-byte
+// delta word and its index word, then issues up to eight independent gathers.
+template <int NIB>
+__global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
+                                                      const uint4* __restrict__ delta,
+                                                      const void* __restrict__ idx,
                                                       const int* __restrict__ base,
                                                       const unsigned char* __restrict__ plain,
-                                                      const float* __restrict__ table, int ntable,
+                                                      const float* __restrict__ table,
                                                       const float* __restrict__ p,
                                                       float* __restrict__ Ap, PcgScalars* S,
                                                       ReduceScratch rs) {
   if (S->done) return;
-  __shared__ float tab[256];
-  if (DICT) {
-    for (int t = threadIdx.x; t < ntable; t += blockDim.x) tab[t] = table[t];
-    __syncthreads();
-  }
+  constexpr int NT = 1 << NIB;
+  __shared__ float tab[NT];
+  for (int t = threadIdx.x; t < NT; t += blockDim.x) tab[t] = table[t];
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   double acc[1] = {0.0};
   for (int s = gw; s < A.nslices; s += nw) {
+    const int i = s * 32 + lane;
     float sum;
-    if (plain[s]) {
+    if (__ldg(plain + s)) {
       sum = sell_row_f32(A, p, s, lane);
     } else {
-      const long long b0 = A.sptr[s];
-      const int len = (int)((A.sptr[s + 1] - b0) >> 5);
-      const int* bs = base + (b0 >> 5);
-      sum = 0.f;
-      constexpr int CH = 8;
-      for (int j0 = 0; j0 < len; j0 += CH) {
-        int c[CH];
-        float v[CH];
-#pragma unroll
-        for (int t = 0; t < CH; ++t) {
-          if (j0 + t < len) {
-            const long long k = b0 + 32LL * (j0 + t) + lane;
-            c[t] = __ldg(bs + j0 + t) + (int)ld_stream(delta + k);
-            v[t] = DICT ? tab[ld_stream(vidx + k)] : ld_stream(A.val + k);
-          } else {
-            c[t] = -1;
-            v[t] = 0.f;
-          }
-        }
-        float xv[CH];
-#pragma unroll
-        for (int t = 0; t < CH; ++t) xv[t] = (c[t] >= 0) ? __ldg(p + c[t]) : 0.f;
-#pragma unroll
-        for (int t = 0; t < CH; ++t) sum = fmaf(xv[t], v[t], sum);
+      const uint4 d = ld_stream(delta + i);
+      unsigned w0, w1;
+      if (NIB == 4) {
+        w0 = ld_stream(static_cast<const unsigned*>(idx) + i);
+        w1 = 0u;
+      } else {
+        const uint2 w = ld_stream(static_cast<const uint2*>(idx) + i);
+        w0 = w.x;
+        w1 = w.y;
       }
+      const int4 b0 = __ldg(reinterpret_cast<const int4*>(base) + 2 * s);
+      const int4 b1 = __ldg(reinterpret_cast<const int4*>(base) + 2 * s + 1);
+      const int c[8] = {b0.x + (int)(d.x & 0xffffu), b0.y + (int)(d.x >> 16),
+                        b0.z + (int)(d.y & 0xffffu), b0.w + (int)(d.y >> 16),
+                        b1.x + (int)(d.z & 0xffffu), b1.y + (int)(d.z >> 16),
+                        b1.z + (int)(d.w & 0xffffu), b1.w + (int)(d.w >> 16)};
+      unsigned id[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        id[j] = (NIB == 4) ? (w0 >> (4 * j)) & 15u : ((j < 4 ? w0 : w1) >> (8 * (j & 3))) & 255u;
+      float xv[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) xv[j] = id[j] ? __ldg(p + c[j]) : 0.f;
+      sum = 0.f;
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (id[j]) sum = fmaf(xv[j], tab[id[j]], sum);
     }
-    const int i = s * 32 + lane;
     if (i < A.nrows) {
       Ap[i] = sum;
       acc[0] += (double)p[i] * (double)sum;
@@ -399,6 +402,7 @@ struct BetaFinish32 {
 };
 
 // y += alpha p; r^ -= alpha A^p; r^.r^; decide on a replacement
+// y += alpha p, r -= alpha Ap, r.r; four rows per thread per pass (16-byte accesses)
 __global__ void __launch_bounds__(256) k_mx_update(int n, float* __restrict__ y,
                                                    float* __restrict__ r,
                                                    const float* __restrict__ p,
@@ -409,7 +413,29 @@ __global__ void __launch_bounds__(256) k_mx_update(int n, float* __restrict__ y,
   if (S->done) return;
   const float alpha = (float)S->alpha;
   double acc[1] = {0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const int n4 = n >> 2;
+  float4* y4 = reinterpret_cast<float4*>(y);
+  float4* r4 = reinterpret_cast<float4*>(r);
+  const float4* p4 = reinterpret_cast<const float4*>(p);
+  const float4* a4 = reinterpret_cast<const float4*>(Ap);
+  for (int q = tid; q < n4; q += stride) {
+    float4 yv = y4[q], rv = r4[q];
+    const float4 pv = p4[q], av = a4[q];
+    yv.x = fmaf(alpha, pv.x, yv.x);
+    yv.y = fmaf(alpha, pv.y, yv.y);
+    yv.z = fmaf(alpha, pv.z, yv.z);
+    yv.w = fmaf(alpha, pv.w, yv.w);
+    rv.x = fmaf(-alpha, av.x, rv.x);
+    rv.y = fmaf(-alpha, av.y, rv.y);
+    rv.z = fmaf(-alpha, av.z, rv.z);
+    rv.w = fmaf(-alpha, av.w, rv.w);
+    y4[q] = yv;
+    r4[q] = rv;
+    acc[0] += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y +
+              (double)rv.z * (double)rv.z + (double)rv.w * (double)rv.w;
+  }
+  for (int i = 4 * n4 + tid; i < n; i += stride) {
     y[i] = fmaf(alpha, p[i], y[i]);
     const float ri = fmaf(-alpha, Ap[i], r[i]);
     r[i] = ri;
@@ -438,8 +464,20 @@ __global__ void __launch_bounds__(256) k_mx_pupdate(int n, float* __restrict__ p
   if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(use_cond, loop_cond, !S->done);
   if (S->done) return;
   const float beta = (float)S->beta;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    p[i] = fmaf(beta, p[i], r[i]);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const int n4 = n >> 2;
+  float4* p4 = reinterpret_cast<float4*>(p);
+  const float4* r4 = reinterpret_cast<const float4*>(r);
+  for (int q = tid; q < n4; q += stride) {
+    float4 pv = p4[q];
+    const float4 rv = r4[q];
+    pv.x = fmaf(beta, pv.x, rv.x);
+    pv.y = fmaf(beta, pv.y, rv.y);
+    pv.z = fmaf(beta, pv.z, rv.z);
+    pv.w = fmaf(beta, pv.w, rv.w);
+    p4[q] = pv;
+  }
+  for (int i = 4 * n4 + tid; i < n; i += stride) p[i] = fmaf(beta, p[i], r[i]);
 }
 
 // scale = 1/sqrt(L_ii); lhat = S L S (columns outside the unknowns dropped to 0)
@@ -563,6 +601,7 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
       }
       k_mx_lhat<<<blocks_spmv, 256, 0, s>>>(L->view(), scale.p, n, pin_row, pin_val, lhat.p);
       GIPB_LAUNCH_CHECK();
+      GIPB_TRY(sort_fp32_rows(s));
       if (prm.mode == GIPB200_PCG_MIXED && !getenv("GIPB200_NO_COMPRESS")) GIPB_TRY(build_compressed(s));
     }
   } else {
@@ -585,7 +624,11 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
   return GIPB200_OK;
 }
 
-int Pcg::build_compressed(cudaStream_t s) {
+// Sorts each row of the FP32 operator by column (the mixed form's inner product order is
+// free; L itself keeps GIP's order) and drops the zero-valued ghost columns to padding.
+// Sorted rows give every slot of a slice one neighbour direction, which keeps the column
+// spread per slot small for the packed layout.
+int Pcg::sort_fp32_rows(cudaStream_t s) {
   const int ns = L->nslices;
   const long long nslots = L->nslots;
   if (ns == 0 || nslots == 0) return GIPB200_OK;
@@ -596,85 +639,133 @@ int Pcg::build_compressed(cudaStream_t s) {
   GIPB_CUDA(cudaMemcpyAsync(col.data(), L->col.p, col.size() * 4, cudaMemcpyDeviceToHost, s));
   GIPB_CUDA(cudaMemcpyAsync(val.data(), lhat.p, val.size() * 4, cudaMemcpyDeviceToHost, s));
   GIPB_CUDA(cudaStreamSynchronize(s));
-  std::vector<int> base((size_t)(nslots / 32), 0);
-  std::vector<unsigned char> plain((size_t)ns, 0);
-  std::vector<unsigned short> delta((size_t)nslots, 0);
-  long long comp_slots = 0;
-#pragma omp parallel for schedule(static) reduction(+ : comp_slots)
+  const int nu = n;
+#pragma omp parallel for schedule(static)
   for (int sl = 0; sl < ns; ++sl) {
     const long long b0 = sptr[sl];
     const int len = (int)((sptr[sl + 1] - b0) >> 5);
-    bool ok = true;
+    std::vector<std::pair<int, float>> row((size_t)len);
+    for (int l = 0; l < 32; ++l) {
+      int m = 0;
+      for (int j = 0; j < len; ++j) {
+        const long long k = b0 + 32LL * j + l;
+        const int c = col[k];
+        if (c >= 0 && c < nu) row[m++] = {c, val[k]};
+      }
+      std::stable_sort(row.begin(), row.begin() + m,
+                       [](const std::pair<int, float>& x, const std::pair<int, float>& y) {
+                         return x.first < y.first;
+                       });
+      for (int j = 0; j < len; ++j) {
+        const long long k = b0 + 32LL * j + l;
+        col[k] = j < m ? row[j].first : -1;
+        val[k] = j < m ? row[j].second : 0.0f;
+      }
+    }
+  }
+  GIPB_TRY(col32.upload(col.data(), col.size(), s));
+  GIPB_CUDA(cudaMemcpyAsync(lhat.p, val.data(), val.size() * 4, cudaMemcpyHostToDevice, s));
+  GIPB_CUDA(cudaStreamSynchronize(s));
+  return GIPB200_OK;
+}
+
+int Pcg::build_compressed(cudaStream_t s) {
+  const int ns = L->nslices;
+  const long long nslots = L->nslots;
+  if (ns == 0 || nslots == 0) return GIPB200_OK;
+  std::vector<long long> sptr((size_t)ns + 1);
+  std::vector<int> col((size_t)nslots);
+  std::vector<float> val((size_t)nslots);
+  GIPB_CUDA(cudaMemcpyAsync(sptr.data(), L->sptr.p, sptr.size() * 8, cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaMemcpyAsync(col.data(), col32.p, col.size() * 4, cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaMemcpyAsync(val.data(), lhat.p, val.size() * 4, cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaStreamSynchronize(s));
+  // value table over the nonzero values (index 0 = 0.0f)
+  std::vector<unsigned> keys;
+  for (long long k = 0; k < nslots; ++k) {
+    if (col[k] < 0 || val[k] == 0.0f) continue;
+    unsigned bits;
+    memcpy(&bits, &val[k], 4);
+    if (std::find(keys.begin(), keys.end(), bits) == keys.end()) {
+      if (keys.size() >= 255) return GIPB200_OK;  // no table: plain layout only
+      keys.push_back(bits);
+    }
+  }
+  std::sort(keys.begin(), keys.end());
+  const int nib = keys.size() <= 15 ? 4 : 8;
+  std::vector<float> table((size_t)1 << nib, 0.0f);
+  for (size_t t = 0; t < keys.size(); ++t) memcpy(&table[t + 1], &keys[t], 4);
+  auto index_of = [&](float v) -> unsigned {
+    if (v == 0.0f) return 0u;
+    unsigned bits;
+    memcpy(&bits, &v, 4);
+    return 1u + (unsigned)(std::lower_bound(keys.begin(), keys.end(), bits) - keys.begin());
+  };
+  const size_t nrow_pad = (size_t)ns * 32;
+  std::vector<uint4> delta(nrow_pad, make_uint4(0u, 0u, 0u, 0u));
+  std::vector<unsigned> idx4(nib == 4 ? nrow_pad : 0, 0u);
+  std::vector<uint2> idx8(nib == 8 ? nrow_pad : 0, make_uint2(0u, 0u));
+  std::vector<int> base((size_t)ns * 8, 0);
+  std::vector<unsigned char> plain((size_t)ns, 1);
+  long long packed_slots = 0, plain_slots = 0, packed_slices = 0;
+#pragma omp parallel for schedule(static) reduction(+ : packed_slots, plain_slots, packed_slices)
+  for (int sl = 0; sl < ns; ++sl) {
+    const long long b0 = sptr[sl];
+    const int len = (int)((sptr[sl + 1] - b0) >> 5);
+    bool ok = len <= 8;
+    int lo[8], hi[8];
+    for (int j = 0; j < 8; ++j) lo[j] = 0x7fffffff, hi[j] = -1;
     for (int j = 0; j < len && ok; ++j) {
-      int lo = 0x7fffffff, hi = -1;
       for (int l = 0; l < 32; ++l) {
-        const int c = col[b0 + 32LL * j + l];
-        if (c >= 0) {
-          lo = std::min(lo, c);
-          hi = std::max(hi, c);
+        const long long k = b0 + 32LL * j + l;
+        if (col[k] >= 0 && val[k] != 0.0f) {
+          lo[j] = std::min(lo[j], col[k]);
+          hi[j] = std::max(hi[j], col[k]);
         }
       }
-      if (hi < 0) lo = hi = 0;
-      if (hi - lo > 65535) ok = false;
-      base[(b0 >> 5) + j] = lo;
-      for (int l = 0; l < 32 && ok; ++l) {
-        const int c = col[b0 + 32LL * j + l];
-        delta[b0 + 32LL * j + l] = (unsigned short)(c >= 0 ? c - lo : 0);
-      }
+      if (hi[j] >= 0 && hi[j] - lo[j] > 65535) ok = false;
     }
-    plain[sl] = ok ? 0 : 1;
-    if (ok) comp_slots += 32LL * len;
+    if (!ok) {
+      plain_slots += 32LL * len;
+      continue;
+    }
+    plain[sl] = 0;
+    packed_slots += 32LL * len;
+    packed_slices += 1;
+    for (int j = 0; j < 8; ++j) base[(size_t)sl * 8 + j] = hi[j] >= 0 ? lo[j] : 0;
+    for (int l = 0; l < 32; ++l) {
+      unsigned dw[4] = {0u, 0u, 0u, 0u};
+      unsigned long long iw = 0ull;
+      for (int j = 0; j < len; ++j) {
+        const long long k = b0 + 32LL * j + l;
+        if (col[k] < 0 || val[k] == 0.0f) continue;
+        const unsigned d = (unsigned)(col[k] - lo[j]);
+        dw[j >> 1] |= d << (16 * (j & 1));
+        iw |= (unsigned long long)index_of(val[k]) << (nib * j);
+      }
+      const size_t r = (size_t)sl * 32 + l;
+      delta[r] = make_uint4(dw[0], dw[1], dw[2], dw[3]);
+      if (nib == 4) idx4[r] = (unsigned)iw;
+      else idx8[r] = make_uint2((unsigned)iw, (unsigned)(iw >> 32));
+    }
   }
-  cop.compressed_fraction = (double)comp_slots / (double)nslots;
+  cop.compressed_fraction = (double)packed_slots / (double)nslots;
   if (cop.compressed_fraction < 0.5) return GIPB200_OK;  // not worth a second layout
-  // value table (index 0 = 0.0f, shared by padding and stored zeros)
-  std::vector<float> table(1, 0.0f);
-  std::vector<unsigned char> vidx((size_t)nslots, 0);
-  bool dict = true;
-  {
-    std::vector<unsigned> keys;
-    for (long long k = 0; k < nslots && dict; ++k) {
-      const float v = (col[k] >= 0) ? val[k] : 0.0f;
-      if (v == 0.0f) continue;
-      unsigned bits;
-      memcpy(&bits, &v, 4);
-      if (std::find(keys.begin(), keys.end(), bits) == keys.end()) {
-        if (keys.size() >= 255) {
-          dict = false;
-          break;
-        }
-        keys.push_back(bits);
-        table.push_back(v);
-      }
-    }
-    if (dict) {
-#pragma omp parallel for schedule(static)
-      for (long long k = 0; k < nslots; ++k) {
-        const float v = (col[k] >= 0) ? val[k] : 0.0f;
-        unsigned char id = 0;
-        if (v != 0.0f)
-          for (size_t t = 1; t < table.size(); ++t)
-            if (table[t] == v) {
-              id = (unsigned char)t;
-              break;
-            }
-        vidx[k] = id;
-      }
-    }
-  }
-  cop.dict = dict;
-  cop.ntable = (int)table.size();
   GIPB_TRY(cop.delta.upload(delta.data(), delta.size(), s));
-  GIPB_TRY(cop.base.upload(base.data(), std::max<size_t>(base.size(), 1), s));
+  if (nib == 4) GIPB_TRY(cop.idx4.upload(idx4.data(), idx4.size(), s));
+  else GIPB_TRY(cop.idx8.upload(idx8.data(), idx8.size(), s));
+  GIPB_TRY(cop.base.upload(base.data(), base.size(), s));
   GIPB_TRY(cop.plain.upload(plain.data(), plain.size(), s));
   GIPB_TRY(cop.table.upload(table.data(), table.size(), s));
-  if (dict) GIPB_TRY(cop.vidx.upload(vidx.data(), vidx.size(), s));
   GIPB_CUDA(cudaStreamSynchronize(s));
-  const double slot_bytes = dict ? 3.0 : 6.0;
-  const double comp_nnz = (double)L->nnz * cop.compressed_fraction;
-  cop.bytes_per_launch = comp_nnz * slot_bytes + ((double)L->nnz - comp_nnz) * 8.0 +
-                         (double)base.size() * 4.0 * cop.compressed_fraction +
-                         (double)(ns + 1) * 9.0 + (double)L->nrows * 8.0;
+  cop.index_bits = nib;
+  cop.ntable = (int)keys.size() + 1;
+  // streamed bytes: packed rows (delta + index words), their slot bases; plain slices
+  // (column + value per slot, slice offsets); the plain flags; p and Ap once per row
+  const double packed_rows = 32.0 * (double)packed_slices;
+  cop.bytes_per_launch = packed_rows * (16.0 + nib) + (double)packed_slices * 32.0 +
+                         (double)plain_slots * 8.0 + (double)(ns - packed_slices) * 16.0 +
+                         (double)ns + (double)L->nrows * 8.0;
   cop.enabled = true;
   return GIPB200_OK;
 }
@@ -697,7 +788,7 @@ int Pcg::read_flag(cudaStream_t s, int which, int* v) {
   return GIPB200_OK;
 }
 
-static void launch_mx_spmv(const Pcg& P, const SellView<float>& A, cudaStream_t s);
+static void launch_mx_spmv(const Pcg& P, float* Ap, PcgScalars* sc, cudaStream_t s);
 
 // ------------------------------------------------------------------ conditional while-nodes
 static bool capturing(cudaStream_t s) {
@@ -812,14 +903,13 @@ int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaS
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 1, hl));
   cudaGraph_t loop_body;
   GIPB_TRY(add_while(s, hl, &loop_body));
-  const SellView<float> A{L->nrows, L->nslices, L->sptr.p, L->col.p, lhat.p};
   cudaStream_t os = body_stream[0], is = body_stream[1];
   GIPB_CUDA(cudaStreamBeginCaptureToGraph(os, loop_body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
   int st = [&]() -> int {
     cudaGraphConditionalHandle hu;
     GIPB_TRY(make_handle(os, 0, 0, &hu));
-    launch_mx_spmv(*this, A, os);
+    launch_mx_spmv(*this, Ap32.p, sc.p, os);
     k_mx_update<<<blocks_vec, 256, 0, os>>>(n, y32.p, r32.p, p32.p, Ap32.p, sc.p, rs,
                                              prm.inner_tol, prm.maxit, pin_row, scale.p, 1, hu);
     GIPB_LAUNCH_CHECK();
@@ -874,18 +964,17 @@ int Pcg::enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t
   return GIPB200_OK;
 }
 
-static void launch_mx_spmv(const Pcg& P, const SellView<float>& A, cudaStream_t s) {
+static void launch_mx_spmv(const Pcg& P, float* Ap, PcgScalars* sc, cudaStream_t s) {
   const CompressedOp& c = P.cop;
-  if (c.enabled && c.dict)
-    k_mxc_spmv_dot<true><<<P.blocks_spmv, 256, 0, s>>>(A, c.delta.p, c.vidx.p, c.base.p, c.plain.p,
-                                                       c.table.p, c.ntable, P.p32.p, P.Ap32.p,
-                                                       P.sc.p, P.rs);
+  const SellView<float> A = P.a32();
+  if (c.enabled && c.index_bits == 4)
+    k_mxp_spmv_dot<4><<<P.blocks_spmv, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.plain.p,
+                                                    c.table.p, P.p32.p, Ap, sc, P.rs);
   else if (c.enabled)
-    k_mxc_spmv_dot<false><<<P.blocks_spmv, 256, 0, s>>>(A, c.delta.p, c.vidx.p, c.base.p, c.plain.p,
-                                                        c.table.p, c.ntable, P.p32.p, P.Ap32.p,
-                                                        P.sc.p, P.rs);
+    k_mxp_spmv_dot<8><<<P.blocks_spmv, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.plain.p,
+                                                    c.table.p, P.p32.p, Ap, sc, P.rs);
   else
-    k_mx_spmv_dot<<<P.blocks_spmv, 256, 0, s>>>(A, P.p32.p, P.Ap32.p, P.sc.p, P.rs);
+    k_mx_spmv_dot<<<P.blocks_spmv, 256, 0, s>>>(A, P.p32.p, Ap, sc, P.rs);
 }
 
 int Pcg::launch_mixed_residual(const double* b, const double* x, int first, cudaStream_t s,
@@ -902,11 +991,10 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
                        bool host_sync) {
   if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
-  const SellView<float> A{L->nrows, L->nslices, L->sptr.p, L->col.p, lhat.p};
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 0, 0));
   const int poll = 16;
   for (int k = 0; k < prm.maxit; ++k) {
-    launch_mx_spmv(*this, A, s);
+    launch_mx_spmv(*this, Ap32.p, sc.p, s);
     k_mx_update<<<blocks_vec, 256, 0, s>>>(n, y32.p, r32.p, p32.p, Ap32.p, sc.p, rs, prm.inner_tol,
                                             prm.maxit, pin_row, scale.p, 0, 0);
     k_mx_apply<<<blocks_vec, 256, 0, s>>>(n, x, y32.p, scale.p, sc.p);
@@ -938,7 +1026,6 @@ int Pcg::time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* 
   cudaEvent_t e0, e1;
   GIPB_CUDA(cudaEventCreate(&e0));
   GIPB_CUDA(cudaEventCreate(&e1));
-  const SellView<float> A{L->nrows, L->nslices, L->sptr.p, L->col.p, lhat.p};
   if (mixed) {
     GIPB_TRY(tAp32.alloc(n));
   } else {
@@ -949,16 +1036,8 @@ int Pcg::time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* 
   // that would skip work: p.Ap > 0 for the SPD operator and a nonzero p)
   for (int k = 0; k <= reps; ++k) {
     if (k == 1) GIPB_CUDA(cudaEventRecord(e0, s));
-    if (mixed && cop.enabled && cop.dict)
-      k_mxc_spmv_dot<true><<<blocks_spmv, 256, 0, s>>>(A, cop.delta.p, cop.vidx.p, cop.base.p,
-                                                       cop.plain.p, cop.table.p, cop.ntable, p32.p,
-                                                       tAp32.p, tsc.p, rs);
-    else if (mixed && cop.enabled)
-      k_mxc_spmv_dot<false><<<blocks_spmv, 256, 0, s>>>(A, cop.delta.p, cop.vidx.p, cop.base.p,
-                                                        cop.plain.p, cop.table.p, cop.ntable, p32.p,
-                                                        tAp32.p, tsc.p, rs);
-    else if (mixed)
-      k_mx_spmv_dot<<<blocks_spmv, 256, 0, s>>>(A, p32.p, tAp32.p, tsc.p, rs);
+    if (mixed)
+      launch_mx_spmv(*this, tAp32.p, tsc.p, s);
     else
       k_pcg_spmv_dot<<<blocks_spmv, 256, 0, s>>>(L->view(), p.p, tAp.p, tsc.p, rs,
                                                   GIPB200_PCG_FIXED);
@@ -1016,6 +1095,22 @@ int gipb200_pcg_create(gipb200_matrix L, int n_all, const gipb200_pcg_params* pa
 int gipb200_pcg_destroy(gipb200_pcg S) {
   delete S;
   return GIPB200_OK;
+}
+
+int gipb200_pcg_get_info(gipb200_pcg S, gipb200_pcg_info* info) {
+  if (!S || !info) return fail(GIPB200_ERR_ARG, "null argument");
+  info->pin_row = S->P.pin_row;
+  info->compressed = S->P.cop.enabled;
+  info->value_table = S->P.cop.index_bits;
+  info->compressed_fraction = S->P.cop.compressed_fraction;
+  return GIPB200_OK;
+}
+
+int gipb200_pcg_kernel_time(gipb200_pcg S, int reps, void* stream, double* avg_ms,
+                            double* bytes) {
+  if (!S || !avg_ms || !bytes) return fail(GIPB200_ERR_ARG, "null argument");
+  return S->P.time_spmv(S->P.prm.mode == GIPB200_PCG_MIXED, reps, as_stream(stream), avg_ms,
+                        bytes);
 }
 
 int gipb200_pcg_solve(gipb200_pcg S, const double* b, double* x, const double* x0, void* stream,

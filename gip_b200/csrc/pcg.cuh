@@ -30,21 +30,25 @@ struct PcgScalars {
   int pad2;
 };
 
-// The FP32 operator of the mixed form, compressed without loss: per slot a 16-bit
-// column delta from a per-(slice, slot) base and, when the operator has at most 255
-// distinct values, an 8-bit index into a value table (index 0 = 0.0f, the padding).
-// Slices whose column spread exceeds 16 bits stay in the plain layout.
+// The FP32 operator of the mixed form, compressed without loss.  Each row's nonzeros
+// are sorted by column (the FP32 operator only: L keeps GIP's order for the FP64
+// residual).  A slice of 32 rows whose rows have at most 8 slots and whose column spread
+// per slot fits 16 bits is packed per row: eight 16-bit column deltas (one 16-byte load)
+// from a per-(slice, slot) base, and eight value-table indices (4 bits when the operator
+// has at most 15 distinct nonzero values, else 8 bits; index 0 = 0.0f, padding and
+// stored zeros).  Other slices stay in the plain sliced layout.
 struct CompressedOp {
   bool enabled = false;
-  bool dict = false;
-  DevBuf<unsigned short> delta;
-  DevBuf<unsigned char> vidx;
-  DevBuf<int> base;            // index (sptr[s] / 32 + j)
-  DevBuf<unsigned char> plain; // per slice
-  DevBuf<float> table;
+  int index_bits = 0;            // 4 or 8
+  DevBuf<uint4> delta;           // per row (nslices * 32)
+  DevBuf<unsigned> idx4;         // per row, 8 x 4 bits
+  DevBuf<uint2> idx8;            // per row, 8 x 8 bits
+  DevBuf<int> base;              // per slice, 8 slots
+  DevBuf<unsigned char> plain;   // per slice
+  DevBuf<float> table;           // 16 or 256 entries
   int ntable = 0;
-  double compressed_fraction = 0.0;
-  double bytes_per_launch = 0.0;  // stored bytes the kernel streams (+ vectors)
+  double compressed_fraction = 0.0;  // share of L's slots in packed slices
+  double bytes_per_launch = 0.0;     // stored bytes the kernel streams (+ vectors)
 };
 
 struct Pcg {
@@ -54,11 +58,14 @@ struct Pcg {
   gipb200_pcg_params prm{};
   DevBuf<double> dinv, p, Ap, r;
   // MIXED
-  DevBuf<float> lhat;        // S L S values in L's sliced layout (FP32)
+  DevBuf<float> lhat;        // S L S values in L's slice structure, rows sorted by column
+  DevBuf<int> col32;         // their columns (-1: padding and dropped ghost columns)
   DevBuf<double> scale;      // S = 1/sqrt(L_ii)
   DevBuf<float> p32, Ap32, r32, y32;
   CompressedOp cop;
+  int sort_fp32_rows(cudaStream_t s);
   int build_compressed(cudaStream_t s);
+  SellView<float> a32() const { return {L->nrows, L->nslices, L->sptr.p, col32.p, lhat.p}; }
   // Pinned-Neumann structure of L (every row sums to zero except one pinned row p with
   // sum pin > 0): the FP32 inner solve then runs on the pure-Neumann part and the
   // constant mode is restored exactly from the pin equation.

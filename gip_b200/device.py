@@ -189,6 +189,18 @@ class PcgSolver:
         return {"iterations": res.iterations, "outer": res.outer, "status": res.status,
                 "rr": res.rr, "bb": res.bb}
 
+    def kernel_time(self, reps: int = 20, stream=None) -> tuple:
+        """(mean ms, streamed bytes) of the solver's SpMV-dot kernel over `reps` launches."""
+        ms, nb = C.c_double(), C.c_double()
+        L.call("gipb200_pcg_kernel_time", self.handle, reps, _stream(stream), C.byref(ms),
+               C.byref(nb))
+        return ms.value, nb.value
+
+    def info(self) -> dict:
+        i = L.PcgInfo()
+        L.call("gipb200_pcg_get_info", self.handle, C.byref(i))
+        return {k: getattr(i, k) for k, _ in L.PcgInfo._fields_}
+
     def close(self):
         if getattr(self, "handle", None):
             L.load().gipb200_pcg_destroy(self.handle)

@@ -145,6 +145,21 @@ int gipb200_pcg_destroy(gipb200_pcg S);
 int gipb200_pcg_solve(gipb200_pcg S, const double* d_b, double* d_x, const double* d_x0,
                       void* stream, gipb200_pcg_result* h_result);
 
+/* No counterpart in the reference: how the solver stores its operator. */
+typedef struct {
+  int pin_row;                 /* MIXED: detected pinned-Neumann row (-1: none)           */
+  int compressed;              /* MIXED: FP32 operator packed (see value_table)           */
+  int value_table;             /* MIXED: bits of a packed row's value-table index (4, 8)  */
+  double compressed_fraction;  /* MIXED: share of the operator's slots in packed slices   */
+} gipb200_pcg_info;
+int gipb200_pcg_get_info(gipb200_pcg S, gipb200_pcg_info* info);
+/* No counterpart in the reference: times `reps` launches of the solver's SpMV-dot kernel
+ * (FP64 forms: the FP64 kernel; MIXED: the FP32 kernel of its operator layout) on its
+ * current search direction, with CUDA events on `stream`; returns the mean launch time and
+ * the kernel's streamed bytes per launch.  Solve once first so the direction is set. */
+int gipb200_pcg_kernel_time(gipb200_pcg S, int reps, void* stream, double* avg_ms,
+                            double* bytes);
+
 /* No counterpart in the reference.  A Jacobi-PCG solve for callers that cannot allocate
  * device memory at solve time (a framework-owned arena or caching allocator, code that
  * must not call cudaMalloc because it synchronises the device, embedders without
@@ -223,8 +238,8 @@ typedef struct {
   int reordered;               /* engine runs in its breadth-first numbering            */
   int pin_row;                 /* MIXED: detected pinned-Neumann row of L (-1: none)     */
   int compressed;              /* MIXED: FP32 operator stored compressed                 */
-  int value_table;             /* MIXED: values through an 8-bit table                   */
-  double compressed_fraction;  /* MIXED: share of slots in compressed slices             */
+  int value_table;             /* MIXED: bits of a packed row's value-table index (4, 8) */
+  double compressed_fraction;  /* MIXED: share of L's slots in packed slices             */
   long long slots_L;           /* sliced slots of L (stored nonzeros plus padding)       */
   long long nnz_L;
 } gipb200_dns_info;

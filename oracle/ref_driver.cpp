@@ -5,8 +5,11 @@
  * (src/Algorithms/GIP_LinearSolver.h).  It is compiled by oracle/Makefile from the
  * reference sources where they lie; nothing here is linked into the product.
  *
- * Compared with GIP's DrivenCavity.cpp:21-43 it adds three things a checker needs:
+ * Compared with GIP's DrivenCavity.cpp:21-43 it adds four things a checker needs:
  *   - the number of timesteps (GIP_DNS hard-codes maxIt=10 at GIP_DNS.h:132),
+ *   - the PCG iteration count (GIP_DNS sets maxIt=100 at GIP_DNS.h:183; the environment
+ *     variable GIPREF_CG_MAXIT overrides the solver's copy after setUp, so a benchmark
+ *     can time a bounded number of GIP's own iterations),
  *   - wall-clock timing of setUp() and integrate() (rank 0 prints one JSON line to
  *     stderr),
  *   - an optional dump of the final fields of every rank (u,v,w,p,p0,mf,ax0,ay0,az0)
@@ -77,6 +80,10 @@ int main(int argc, char** argv) {
   MPI_Barrier(MPI_COMM_WORLD);
   double t0 = omp_get_wtime();
   dns.setUp();
+  {
+    const char* m = getenv("GIPREF_CG_MAXIT");
+    if (m) dns.cg.maxIt = atoi(m);
+  }
   MPI_Barrier(MPI_COMM_WORLD);
   double t1 = omp_get_wtime();
   dns.integrate();
@@ -98,9 +105,9 @@ int main(int argc, char** argv) {
   if (rank == 0) {
     fprintf(stderr,
             "{\"ranks\": %d, \"steps\": %d, \"setup_s\": %.6f, \"integrate_s\": %.6f, "
-            "\"ms_per_step\": %.6f, \"dt_next\": %.17g, \"time\": %.17g}\n",
+            "\"ms_per_step\": %.6f, \"dt_next\": %.17g, \"time\": %.17g, \"cg_maxit\": %d}\n",
             nranks, dns.maxIt, t1 - t0, t2 - t1, (t2 - t1) * 1e3 / (dns.maxIt > 0 ? dns.maxIt : 1),
-            dns.dt, dns.time);
+            dns.dt, dns.time, dns.cg.maxIt);
   }
   MPI_Finalize();
   return 0;

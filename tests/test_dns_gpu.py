@@ -124,7 +124,8 @@ def test_compressed_fp32_operator_is_exact(gpu, monkeypatch):
               max_outer=200, reorder=True)
     E = DnsEngine(case, **kw)
     info = E.info()
-    assert info["compressed"] == 1 and info["value_table"] == 1 and info["pin_row"] >= 0
+    assert info["compressed"] == 1 and info["value_table"] == 4 and info["pin_row"] >= 0
+    assert info["compressed_fraction"] == 1.0
     monkeypatch.setenv("GIPB200_NO_COMPRESS", "1")
     P = DnsEngine(case, **kw)
     assert P.info()["compressed"] == 0

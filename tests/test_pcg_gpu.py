@@ -73,3 +73,59 @@ def test_pcg_mixed_reaches_fp64_tolerance(gpu, oracle_mod, n, tol):
     # against the FP64 oracle solved tighter: solution error is bounded by conditioning
     xr, _, _ = oracle_mod.pcg(L, b, np.zeros(L.nrows), maxit=20000, mode=1, tol=1e-13)
     assert np.abs(xs - xr).max() / np.abs(xr).max() < 1e4 * tol
+
+
+def _anisotropic_pinned(nx, ny, nz, w=(1.0, 2.5, 0.6), extra=30, seed=0):
+    """Pinned-Neumann graph Laplacian of an nx*ny*nz grid with direction weights w, plus
+    `extra` rows coupled to three random far cells (rows of 9-10 nonzeros), pinned as GIP
+    pins its pressure operator (L_00 += L_00 / 101)."""
+    import scipy.sparse as sp
+    from gip_b200.formats import Csr
+    N = nx * ny * nz
+    idx = np.arange(N).reshape(nz, ny, nx)
+    rows, cols, vals = [], [], []
+    for ax, ww in zip((2, 1, 0), w):
+        a = np.take(idx, range(0, idx.shape[ax] - 1), axis=ax).ravel()
+        b = np.take(idx, range(1, idx.shape[ax]), axis=ax).ravel()
+        rows += [a, b]
+        cols += [b, a]
+        vals += [np.full(a.size, -ww)] * 2
+    rng = np.random.default_rng(seed)
+    for h in rng.choice(N, extra, replace=False):
+        o = rng.choice(N, 3, replace=False)
+        o = o[o != h]
+        rows += [np.full(o.size, h), o]
+        cols += [o, np.full(o.size, h)]
+        vals += [np.full(o.size, -0.3)] * 2
+    A = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(N, N)).tocsr()
+    A.sum_duplicates()
+    A = (A + sp.diags(-np.asarray(A.sum(axis=1)).ravel())).tolil()
+    A[0, 0] += A[0, 0] / 101.0
+    A = A.tocsr()
+    A.sort_indices()
+    return Csr(N, N, A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.copy())
+
+
+def test_mixed_packed_operator_8bit_table_and_plain_slices(gpu, monkeypatch):
+    # ~100 distinct FP32 values (8-bit table) and rows longer than 8 slots (plain slices):
+    # the packed kernel, its plain fallback and the unpacked kernel give identical solves
+    from gip_b200 import device as dv
+    L = _anisotropic_pinned(20, 18, 16)
+    rng = np.random.default_rng(9)
+    b = rng.standard_normal(L.nrows)
+    kw = dict(mode="mixed", maxit=5000, tol=1e-9, inner_tol=0.1, max_outer=100)
+    S = dv.PcgSolver(dv.DeviceMatrix(L), **kw)
+    info = S.info()
+    assert info["compressed"] == 1 and info["value_table"] == 8 and info["pin_row"] == 0
+    assert 0.5 < info["compressed_fraction"] < 1.0
+    monkeypatch.setenv("GIPB200_NO_COMPRESS", "1")
+    P = dv.PcgSolver(dv.DeviceMatrix(L), **kw)
+    assert P.info()["compressed"] == 0
+    xs, xp = _t(np.zeros(L.nrows)), _t(np.zeros(L.nrows))
+    rs = S.solve(_t(b), xs, _t(np.zeros(L.nrows)))
+    rp = P.solve(_t(b), xp, _t(np.zeros(L.nrows)))
+    assert rs["status"] == 0 and (rs["iterations"], rs["outer"]) == (rp["iterations"], rp["outer"])
+    assert torch.equal(xs, xp)
+    r = b - L.to_scipy() @ xs.cpu().numpy()
+    assert np.linalg.norm(r) <= 1e-9 * np.linalg.norm(b) * 1.0001
