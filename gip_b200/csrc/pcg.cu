@@ -309,20 +309,22 @@ __global__ void __launch_bounds__(256, 8) k_mx_spmv_dot(SellView<float> A, const
   grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
 }
 
-// Same product as k_mx_spmv_dot from the packed layout: the same gathers and the same
-// FMA order (slot by slot; padding and zeros add x*0 there and nothing here), so the same
-// results.  A warp owns a slice; in a packed slice each lane loads its row's 16-byte
-// delta word and its index word, then issues up to eight independent gathers.
-template <int NIB>
+// Same product as k_mx_spmv_dot from the packed layout: the same FMA order slot by slot.
+// Every slot gathers (padding and stored zeros point at a valid column through delta 0
+// and multiply by table entry 0 = 0.0f, adding zero where the plain kernel adds x*0), so
+// the loop has no branches.  A warp owns a slice; in a packed slice each lane loads its
+// row's 16-byte delta word and its index word, then issues K independent gathers.  K = 7
+// when no packed row has an eighth slot.
+template <int NIB, int K>
 __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
-                                                      const uint4* __restrict__ delta,
-                                                      const void* __restrict__ idx,
-                                                      const int* __restrict__ base,
-                                                      const unsigned char* __restrict__ plain,
-                                                      const float* __restrict__ table,
-                                                      const float* __restrict__ p,
-                                                      float* __restrict__ Ap, PcgScalars* S,
-                                                      ReduceScratch rs) {
+                                                         const uint4* __restrict__ delta,
+                                                         const void* __restrict__ idx,
+                                                         const int* __restrict__ base,
+                                                         const unsigned char* __restrict__ plain,
+                                                         const float* __restrict__ table,
+                                                         const float* __restrict__ p,
+                                                         float* __restrict__ Ap, PcgScalars* S,
+                                                         ReduceScratch rs) {
   if (S->done) return;
   constexpr int NT = 1 << NIB;
   __shared__ float tab[NT];
@@ -354,17 +356,16 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
                         b0.z + (int)(d.y & 0xffffu), b0.w + (int)(d.y >> 16),
                         b1.x + (int)(d.z & 0xffffu), b1.y + (int)(d.z >> 16),
                         b1.z + (int)(d.w & 0xffffu), b1.w + (int)(d.w >> 16)};
-      unsigned id[8];
+      float xv[K];
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
-        id[j] = (NIB == 4) ? (w0 >> (4 * j)) & 15u : ((j < 4 ? w0 : w1) >> (8 * (j & 3))) & 255u;
-      float xv[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) xv[j] = id[j] ? __ldg(p + c[j]) : 0.f;
+      for (int j = 0; j < K; ++j) xv[j] = __ldg(p + c[j]);
       sum = 0.f;
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
-        if (id[j]) sum = fmaf(xv[j], tab[id[j]], sum);
+      for (int j = 0; j < K; ++j) {
+        const unsigned id =
+            (NIB == 4) ? (w0 >> (4 * j)) & 15u : ((j < 4 ? w0 : w1) >> (8 * (j & 3))) & 255u;
+        sum = fmaf(xv[j], tab[id], sum);
+      }
     }
     if (i < A.nrows) {
       Ap[i] = sum;
@@ -708,7 +709,9 @@ int Pcg::build_compressed(cudaStream_t s) {
   std::vector<int> base((size_t)ns * 8, 0);
   std::vector<unsigned char> plain((size_t)ns, 1);
   long long packed_slots = 0, plain_slots = 0, packed_slices = 0;
-#pragma omp parallel for schedule(static) reduction(+ : packed_slots, plain_slots, packed_slices)
+  int max_len = 0;
+#pragma omp parallel for schedule(static) reduction(+ : packed_slots, plain_slots, packed_slices) \
+    reduction(max : max_len)
   for (int sl = 0; sl < ns; ++sl) {
     const long long b0 = sptr[sl];
     const int len = (int)((sptr[sl + 1] - b0) >> 5);
@@ -732,6 +735,7 @@ int Pcg::build_compressed(cudaStream_t s) {
     plain[sl] = 0;
     packed_slots += 32LL * len;
     packed_slices += 1;
+    max_len = std::max(max_len, len);
     for (int j = 0; j < 8; ++j) base[(size_t)sl * 8 + j] = hi[j] >= 0 ? lo[j] : 0;
     for (int l = 0; l < 32; ++l) {
       unsigned dw[4] = {0u, 0u, 0u, 0u};
@@ -759,6 +763,7 @@ int Pcg::build_compressed(cudaStream_t s) {
   GIPB_TRY(cop.table.upload(table.data(), table.size(), s));
   GIPB_CUDA(cudaStreamSynchronize(s));
   cop.index_bits = nib;
+  cop.slots = max_len <= 7 ? 7 : 8;
   cop.ntable = (int)keys.size() + 1;
   // streamed bytes: packed rows (delta + index words), their slot bases; plain slices
   // (column + value per slot, slice offsets); the plain flags; p and Ap once per row
@@ -967,14 +972,21 @@ int Pcg::enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t
 static void launch_mx_spmv(const Pcg& P, float* Ap, PcgScalars* sc, cudaStream_t s) {
   const CompressedOp& c = P.cop;
   const SellView<float> A = P.a32();
-  if (c.enabled && c.index_bits == 4)
-    k_mxp_spmv_dot<4><<<P.blocks_spmv, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.plain.p,
-                                                    c.table.p, P.p32.p, Ap, sc, P.rs);
-  else if (c.enabled)
-    k_mxp_spmv_dot<8><<<P.blocks_spmv, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.plain.p,
-                                                    c.table.p, P.p32.p, Ap, sc, P.rs);
+  const int nb = P.blocks_spmv;
+  if (!c.enabled)
+    k_mx_spmv_dot<<<nb, 256, 0, s>>>(A, P.p32.p, Ap, sc, P.rs);
+  else if (c.index_bits == 4 && c.slots == 7)
+    k_mxp_spmv_dot<4, 7><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.plain.p,
+                                             c.table.p, P.p32.p, Ap, sc, P.rs);
+  else if (c.index_bits == 4)
+    k_mxp_spmv_dot<4, 8><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.plain.p,
+                                             c.table.p, P.p32.p, Ap, sc, P.rs);
+  else if (c.slots == 7)
+    k_mxp_spmv_dot<8, 7><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.plain.p,
+                                             c.table.p, P.p32.p, Ap, sc, P.rs);
   else
-    k_mx_spmv_dot<<<P.blocks_spmv, 256, 0, s>>>(A, P.p32.p, Ap, sc, P.rs);
+    k_mxp_spmv_dot<8, 8><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.plain.p,
+                                             c.table.p, P.p32.p, Ap, sc, P.rs);
 }
 
 int Pcg::launch_mixed_residual(const double* b, const double* x, int first, cudaStream_t s,

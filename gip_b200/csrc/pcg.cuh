@@ -40,6 +40,7 @@ struct PcgScalars {
 struct CompressedOp {
   bool enabled = false;
   int index_bits = 0;            // 4 or 8
+  int slots = 8;                 // 7: no packed row uses the eighth slot
   DevBuf<uint4> delta;           // per row (nslices * 32)
   DevBuf<unsigned> idx4;         // per row, 8 x 4 bits
   DevBuf<uint2> idx8;            // per row, 8 x 8 bits
