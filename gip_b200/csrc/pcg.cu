@@ -53,6 +53,10 @@ struct PcgInitFinish {
     S->status = GIPB200_OK;
     S->done = (maxit <= 0) ? 1 : 0;
     if (mode == GIPB200_PCG_TOL && !(sqrt(t[1]) > tol * sqrt(t[2]))) S->done = 1;
+    if (mode != GIPB200_PCG_FIXED && !(isfinite(t[1]) && isfinite(t[2]))) {
+      S->status = GIPB200_ERR_BREAKDOWN;  // a non-finite right-hand side or start
+      S->done = 1;
+    }
     set_loop(use_cond, cond, !S->done);
   }
 };
@@ -228,9 +232,10 @@ struct ResidualFinish {
     const double goal = 0.5 * tol * sqrt(S->bb);
     S->trig = (t[0] > 0.0) ? rz * (goal * goal) / t[0] : 0.0;
     S->upd = 0;
-    const bool conv = !(sqrt(t[0]) > tol * sqrt(S->bb));
-    if (conv || !isfinite(t[0]) || S->total_inner >= maxit || S->outer >= max_updates) {
-      if (!conv) S->status = isfinite(t[0]) ? GIPB200_ERR_NOT_CONVERGED : GIPB200_ERR_BREAKDOWN;
+    const bool finite = isfinite(t[0]) && isfinite(S->bb);
+    const bool conv = finite && !(sqrt(t[0]) > tol * sqrt(S->bb));
+    if (conv || !finite || S->total_inner >= maxit || S->outer >= max_updates) {
+      if (!conv) S->status = finite ? GIPB200_ERR_NOT_CONVERGED : GIPB200_ERR_BREAKDOWN;
       S->done = 1;
     }
     (void)delta;

@@ -129,3 +129,22 @@ def test_mixed_packed_operator_8bit_table_and_plain_slices(gpu, monkeypatch):
     assert torch.equal(xs, xp)
     r = b - L.to_scipy() @ xs.cpu().numpy()
     assert np.linalg.norm(r) <= 1e-9 * np.linalg.norm(b) * 1.0001
+
+
+@pytest.mark.parametrize("mode", ["tol", "mixed"])
+def test_pcg_reports_breakdown_and_nonconvergence(gpu, mode):
+    # failures come back as statuses (no device trap): a non-finite right-hand side is a
+    # breakdown, an iteration cap below what the tolerance needs is non-convergence
+    from gip_b200 import device as dv
+    L, b = cavity.poisson_problem(10, seed=2)
+    A = dv.DeviceMatrix(L)
+    kw = dict(inner_tol=0.3, max_outer=50) if mode == "mixed" else {}
+    S = dv.PcgSolver(A, mode=mode, maxit=3, tol=1e-12, **kw)
+    x = _t(np.zeros(L.nrows))
+    assert S.solve(_t(b), x, _t(np.zeros(L.nrows)))["status"] == 6  # NOT_CONVERGED
+    bad = b.copy()
+    bad[17] = np.nan
+    S2 = dv.PcgSolver(A, mode=mode, maxit=500, tol=1e-8, **kw)
+    assert S2.solve(_t(bad), x, _t(np.zeros(L.nrows)))["status"] == 3  # BREAKDOWN
+    res = S2.solve(_t(b), x, _t(np.zeros(L.nrows)))  # the solver is still usable
+    assert res["status"] == 0
