@@ -360,7 +360,7 @@ int Dns::grow_history(int need, cudaStream_t s) {
 }
 
 int Dns::enqueue_initial_dt(cudaStream_t s) {
-  k_dns_cfl<<<blocks_vec, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p,
+  k_dns_cfl<<<grid.cfl, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p,
                                         history(), pcg.sc.p, 0, 0, dt_seq.p, dt_seq_len, rs);
   GIPB_LAUNCH_CHECK();
   launches += 1;
@@ -373,25 +373,25 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync) {
   // PredictorVelocity: C's values from the face fluxes, then D/C products and AB2
   GIPB_TRY(launch_csr_spmv(Ec.nrows, Ec.rowptr.p, Ec.csr_col.p, Ec.csr_val.p, mf.p, cval.p, D.pos.p,
                            0.0, 0.0, 0, s));
-  k_dns_convdiff<<<blocks_cells, 256, 0, s>>>(D.view(), cval.p, u.p, v.p, w.p, ax.p, ay.p, az.p);
-  k_dns_ab2<<<blocks_vec, 256, 0, s>>>(N, u.p, v.p, w.p, ax.p, ay.p, az.p, ax0.p, ay0.p, az0.p, sc.p);
+  k_dns_convdiff<<<grid.convdiff, 256, 0, s>>>(D.view(), cval.p, u.p, v.p, w.p, ax.p, ay.p, az.p);
+  k_dns_ab2<<<grid.ab2, 256, 0, s>>>(N, u.p, v.p, w.p, ax.p, ay.p, az.p, ax0.p, ay0.p, az0.p, sc.p);
   // PoissonEquation
-  k_dns_rhs<<<blocks_cells, 256, 0, s>>>(Mx.view(), My.view(), Mz.view(), u.p, v.p, w.p, rhs.p, sc.p);
+  k_dns_rhs<<<grid.rhs, 256, 0, s>>>(Mx.view(), My.view(), Mz.view(), u.p, v.p, w.p, rhs.p, sc.p);
   GIPB_LAUNCH_CHECK();
   GIPB_TRY(pcg.enqueue(rhs.p, p.p, p0.p, s, host_sync));
   k_dns_pcopy<<<blocks_owned, 256, 0, s>>>(N, NO, p.p, p0.p);
   GIPB_LAUNCH_CHECK();
   GIPB_TRY(launch_sell_spmv(Lb, Lb.val.p, p0.p, p.p, 1.0, 1.0, 1, s));
   // VelocityCorrection
-  k_dns_gradcorr<<<blocks_owned, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p, gpx.p, gpy.p,
+  k_dns_gradcorr<<<grid.gradcorr, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p, gpx.p, gpy.p,
                                                gpz.p, u.p, v.p, w.p, N, prm.rho, sc.p);
   // MassFluxes
-  k_dns_massflux<<<blocks_faces, 256, 0, s>>>(SO.view(), SFx.view(), SFy.view(), SFz.view(), p.p,
+  k_dns_massflux<<<grid.massflux, 256, 0, s>>>(SO.view(), SFx.view(), SFy.view(), SFz.view(), p.p,
                                                gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p, prm.rho,
                                                sc.p);
   // CFLCondition
-  k_dns_massr<<<blocks_cells, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
-  k_dns_cfl<<<blocks_vec, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p, H,
+  k_dns_massr<<<grid.massr, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
+  k_dns_cfl<<<grid.cfl, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p, H,
                                         pcg.sc.p, 1, prm.pcg.mode == GIPB200_PCG_MIXED, dt_seq.p,
                                         dt_seq_len, rs);
   GIPB_LAUNCH_CHECK();
@@ -677,6 +677,13 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     GIPB_TRY(grid_blocks(256, std::max(NF, 1), 1, kMaxReduceBlocks, &E.blocks_faces));
     GIPB_TRY(grid_blocks(256, NO, 1, kMaxReduceBlocks, &E.blocks_owned));
     GIPB_TRY(grid_blocks(256, N, 4, kMaxReduceBlocks, &E.blocks_vec));
+    GIPB_TRY(one_wave(k_dns_convdiff, E.blocks_cells, &E.grid.convdiff));
+    GIPB_TRY(one_wave(k_dns_ab2, E.blocks_vec, &E.grid.ab2));
+    GIPB_TRY(one_wave(k_dns_rhs, E.blocks_cells, &E.grid.rhs));
+    GIPB_TRY(one_wave(k_dns_gradcorr, E.blocks_owned, &E.grid.gradcorr));
+    GIPB_TRY(one_wave(k_dns_massflux, E.blocks_faces, &E.grid.massflux));
+    GIPB_TRY(one_wave(k_dns_massr, E.blocks_cells, &E.grid.massr));
+    GIPB_TRY(one_wave(k_dns_cfl, E.blocks_vec, &E.grid.cfl));
     GIPB_CUDA(cudaStreamCreateWithFlags(&E.cap_stream, cudaStreamNonBlocking));
     GIPB_CUDA(cudaDeviceSynchronize());
     return GIPB200_OK;

@@ -44,6 +44,10 @@ struct Dns {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int blocks_cells = 1, blocks_faces = 1, blocks_owned = 1, blocks_vec = 1;
+  // per-kernel grids: the shared sizes above lowered to what stays resident in one wave
+  struct {
+    int convdiff = 1, ab2 = 1, rhs = 1, gradcorr = 1, massflux = 1, massr = 1, cfl = 1;
+  } grid;
   // internal renumbering (reorder): external index e lives at internal perm[e]
   bool reordered = false;
   DevBuf<int> perm_c, perm_f;

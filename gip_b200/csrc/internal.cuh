@@ -96,6 +96,18 @@ struct ReduceScratch {
   double* partials;   // [kMaxReduceWidth][kMaxReduceBlocks]
   unsigned* ticket;   // one counter, zero between launches
 };
+// `blocks` lowered to the number of 256-thread blocks of `kernel` that are resident at
+// once on the device (grid-stride kernels then run in one wave, without a tail).
+template <class K>
+int one_wave(K kernel, int blocks, int* out) {
+  DeviceInfo di;
+  GIPB_TRY(device_info(&di));
+  int per_sm = 0;
+  GIPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0));
+  *out = std::max(1, std::min(blocks, std::max(per_sm, 1) * di.nsm));
+  return GIPB200_OK;
+}
+
 int reduce_scratch_alloc(DevBuf<double>* partials, DevBuf<unsigned>* ticket, ReduceScratch* out);
 
 // ------------------------------------------------------------------ sliced ELL (SELL-32)

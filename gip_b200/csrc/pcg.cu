@@ -62,7 +62,7 @@ struct PcgInitFinish {
 };
 
 // r = b - L x;  z = dinv r;  p = z;  (rz, rr, bb)   -- GIP_LinearSolver.h:63-80
-__global__ void __launch_bounds__(256) k_pcg_init(SellView<double> L, const double* __restrict__ x,
+__global__ void __launch_bounds__(256, 8) k_pcg_init(SellView<double> L, const double* __restrict__ x,
                                                   const double* __restrict__ b,
                                                   const double* __restrict__ dinv,
                                                   double* __restrict__ r, double* __restrict__ p,
@@ -109,7 +109,7 @@ struct AlphaFinish {
 };
 
 // Ap = L p ; p.Ap  -- GIP_LinearSolver.h:89-93
-__global__ void __launch_bounds__(256) k_pcg_spmv_dot(SellView<double> L,
+__global__ void __launch_bounds__(256, 8) k_pcg_spmv_dot(SellView<double> L,
                                                       const double* __restrict__ p,
                                                       double* __restrict__ Ap, PcgScalars* S,
                                                       ReduceScratch rs, int mode) {
@@ -118,7 +118,17 @@ __global__ void __launch_bounds__(256) k_pcg_spmv_dot(SellView<double> L,
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   double acc[1] = {0.0};
+  // slot range of the slice after next, loaded one iteration ahead of its L2 prefetch
+  long long n0 = -1, n1 = -1;
+  if (gw + nw < L.nslices) n0 = __ldg(L.sptr + gw + nw), n1 = __ldg(L.sptr + gw + nw + 1);
   for (int s = gw; s < L.nslices; s += nw) {
+    if (lane == 0 && n0 >= 0 && n1 > n0) {  // this warp's next slice streams into L2
+      prefetch_l2(L.col + n0, (unsigned)(n1 - n0) * 4u);
+      prefetch_l2(L.val + n0, (unsigned)(n1 - n0) * 8u);
+    }
+    const int s2 = s + 2 * nw;
+    n0 = -1;
+    if (s2 < L.nslices) n0 = __ldg(L.sptr + s2), n1 = __ldg(L.sptr + s2 + 1);
     double sum = 0.0;
     bool any = false;
     sell_row_f64(L, p, s, lane, sum, any);
@@ -151,6 +161,10 @@ struct BetaFinish {
 };
 
 // x += alpha p; r -= alpha Ap; z = dinv r; r.z, r.r  -- GIP_LinearSolver.h:95-111
+// x += alpha p; r -= alpha Ap; z = dinv r; r.z, r.r  -- GIP_LinearSolver.h:95-111.
+// V2: two rows per access (16-byte loads and stores; x must be 16-byte aligned), the
+// same IEEE operations per element.
+template <bool V2>
 __global__ void __launch_bounds__(256) k_pcg_update(int n, double* __restrict__ x,
                                                     double* __restrict__ r,
                                                     const double* __restrict__ p,
@@ -162,7 +176,33 @@ __global__ void __launch_bounds__(256) k_pcg_update(int n, double* __restrict__ 
   const double alpha = S->alpha;
   const double malpha = dmul(-1.0, alpha);
   double acc[2] = {0.0, 0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  int i0 = 0;
+  if (V2) {
+    const int n2 = n >> 1;
+    double2* x2 = reinterpret_cast<double2*>(x);
+    double2* r2 = reinterpret_cast<double2*>(r);
+    const double2* p2 = reinterpret_cast<const double2*>(p);
+    const double2* a2 = reinterpret_cast<const double2*>(Ap);
+    const double2* d2 = reinterpret_cast<const double2*>(dinv);
+    for (int q = tid; q < n2; q += stride) {
+      double2 xv = x2[q], rv = r2[q];
+      const double2 pv = p2[q], av = a2[q], dv = d2[q];
+      xv.x = dadd(xv.x, dmul(alpha, pv.x));
+      xv.y = dadd(xv.y, dmul(alpha, pv.y));
+      rv.x = dadd(rv.x, dmul(malpha, av.x));
+      rv.y = dadd(rv.y, dmul(malpha, av.y));
+      x2[q] = xv;
+      r2[q] = rv;
+      const double zx = dadd(0.0, dmul(rv.x, dv.x)), zy = dadd(0.0, dmul(rv.y, dv.y));
+      acc[0] = dadd(acc[0], dmul(rv.x, zx));
+      acc[1] = dadd(acc[1], dmul(rv.x, rv.x));
+      acc[0] = dadd(acc[0], dmul(rv.y, zy));
+      acc[1] = dadd(acc[1], dmul(rv.y, rv.y));
+    }
+    i0 = 2 * n2;
+  }
+  for (int i = i0 + tid; i < n; i += stride) {
     x[i] = dadd(x[i], dmul(alpha, p[i]));
     const double ri = dadd(r[i], dmul(malpha, Ap[i]));
     r[i] = ri;
@@ -182,7 +222,20 @@ __global__ void __launch_bounds__(256) k_pcg_pupdate(int n, double* __restrict__
   if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(use_cond, cond, !S->done);
   if (S->done) return;
   const double beta = S->beta;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const int n2 = n >> 1;  // p, r and dinv are the solver's own (aligned) buffers
+  double2* p2 = reinterpret_cast<double2*>(p);
+  const double2* r2 = reinterpret_cast<const double2*>(r);
+  const double2* d2 = reinterpret_cast<const double2*>(dinv);
+  for (int q = tid; q < n2; q += stride) {
+    double2 pv = p2[q];
+    const double2 rv = r2[q], dv = d2[q];
+    const double zx = dadd(0.0, dmul(rv.x, dv.x)), zy = dadd(0.0, dmul(rv.y, dv.y));
+    pv.x = dadd(dmul(1.0, zx), dmul(beta, pv.x));
+    pv.y = dadd(dmul(1.0, zy), dmul(beta, pv.y));
+    p2[q] = pv;
+  }
+  for (int i = 2 * n2 + tid; i < n; i += stride) {
     const double zi = dadd(0.0, dmul(r[i], dinv[i]));
     p[i] = dadd(dmul(1.0, zi), dmul(beta, p[i]));
   }
@@ -341,9 +394,15 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
   double acc[1] = {0.0};
   for (int s = gw; s < A.nslices; s += nw) {
     const int i = s * 32 + lane;
+    // the packed words of this warp's next slice stream into L2 while this one gathers
+    if (lane == 0 && s + nw < A.nslices) {
+      const size_t nx = (size_t)(s + nw) * 32;
+      prefetch_l2(delta + nx, 32 * 16);
+      prefetch_l2(static_cast<const char*>(idx) + nx * (NIB / 2), 32 * (NIB / 2));
+    }
     float sum;
     if (__ldg(plain + s)) {
-      sum = sell_row_f32(A, p, s, lane);
+      sum = sell_row_f32<2>(A, p, s, lane);  // rare fallback: keep its registers low
     } else {
       const uint4 d = ld_stream(delta + i);
       unsigned w0, w1;
@@ -408,7 +467,11 @@ struct BetaFinish32 {
 };
 
 // y += alpha p; r^ -= alpha A^p; r^.r^; decide on a replacement
-// y += alpha p, r -= alpha Ap, r.r; four rows per thread per pass (16-byte accesses)
+// y += alpha p, r -= alpha Ap, r.r; four rows per thread per pass (16-byte accesses).
+// All grids stride through their rows in step, so a kernel's most recent accesses are the
+// end of its sweep, still in L2.  This update sweeps backwards from the last row, where
+// the SpMV (forward) ended, and p = r + beta p sweeps forwards from the first row, where
+// this update ended.
 __global__ void __launch_bounds__(256) k_mx_update(int n, float* __restrict__ y,
                                                    float* __restrict__ r,
                                                    const float* __restrict__ p,
@@ -425,7 +488,8 @@ __global__ void __launch_bounds__(256) k_mx_update(int n, float* __restrict__ y,
   float4* r4 = reinterpret_cast<float4*>(r);
   const float4* p4 = reinterpret_cast<const float4*>(p);
   const float4* a4 = reinterpret_cast<const float4*>(Ap);
-  for (int q = tid; q < n4; q += stride) {
+  for (int t = tid; t < n4; t += stride) {
+    const int q = n4 - 1 - t;
     float4 yv = y4[q], rv = r4[q];
     const float4 pv = p4[q], av = a4[q];
     yv.x = fmaf(alpha, pv.x, yv.x);
@@ -856,6 +920,15 @@ int Pcg::enqueue(const double* b, double* x, const double* x0, cudaStream_t s, b
 // TOL mode inside a graph: init, then while(!done) { A; B; C }.  C sets the loop value
 // from the stop flag; the flag is set by a convergence test or the maxit cap, so the
 // loop always ends.
+void Pcg::launch_pcg_update(double* x, cudaStream_t s) {
+  if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0)
+    k_pcg_update<true><<<blocks_vec, 256, 0, s>>>(n, x, r.p, p.p, Ap.p, dinv.p, sc.p, rs, prm.mode,
+                                                  prm.maxit, prm.tol);
+  else
+    k_pcg_update<false><<<blocks_vec, 256, 0, s>>>(n, x, r.p, p.p, Ap.p, dinv.p, sc.p, rs,
+                                                   prm.mode, prm.maxit, prm.tol);
+}
+
 int Pcg::enqueue_fp64_graph(const double* b, double* x, const double* x0, cudaStream_t s) {
   cudaGraphConditionalHandle h;
   GIPB_TRY(make_handle(s, 0, 0, &h));
@@ -871,8 +944,7 @@ int Pcg::enqueue_fp64_graph(const double* b, double* x, const double* x0, cudaSt
   GIPB_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
   k_pcg_spmv_dot<<<blocks_spmv, 256, 0, bs>>>(L->view(), p.p, Ap.p, sc.p, rs, prm.mode);
-  k_pcg_update<<<blocks_vec, 256, 0, bs>>>(n, x, r.p, p.p, Ap.p, dinv.p, sc.p, rs, prm.mode,
-                                            prm.maxit, prm.tol);
+  launch_pcg_update(x, bs);
   k_pcg_pupdate<<<blocks_vec, 256, 0, bs>>>(n, p.p, r.p, dinv.p, sc.p, 1, h);
   cudaError_t le = cudaGetLastError();
   cudaGraph_t out = nullptr;
@@ -960,8 +1032,7 @@ int Pcg::enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t
   const int poll = 16;
   for (int k = 0; k < prm.maxit; ++k) {
     k_pcg_spmv_dot<<<blocks_spmv, 256, 0, s>>>(L->view(), p.p, Ap.p, sc.p, rs, prm.mode);
-    k_pcg_update<<<blocks_vec, 256, 0, s>>>(n, x, r.p, p.p, Ap.p, dinv.p, sc.p, rs, prm.mode,
-                                             prm.maxit, prm.tol);
+    launch_pcg_update(x, s);
     k_pcg_pupdate<<<blocks_vec, 256, 0, s>>>(n, p.p, r.p, dinv.p, sc.p, 0, 0);
     GIPB_LAUNCH_CHECK();
     launches += 3;

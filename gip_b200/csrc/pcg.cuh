@@ -65,6 +65,7 @@ struct Pcg {
   DevBuf<float> p32, Ap32, r32, y32;
   CompressedOp cop;
   int sort_fp32_rows(cudaStream_t s);
+  void launch_pcg_update(double* x, cudaStream_t s);
   int build_compressed(cudaStream_t s);
   SellView<float> a32() const { return {L->nrows, L->nslices, L->sptr.p, col32.p, lhat.p}; }
   // Pinned-Neumann structure of L (every row sums to zero except one pinned row p with
