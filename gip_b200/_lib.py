@@ -101,6 +101,7 @@ _SIGNATURES = {
     "gipb200_pcg_create": (_I, [_VP, _I, C.POINTER(PcgParams), C.POINTER(_VP)]),
     "gipb200_pcg_destroy": (_I, [_VP]),
     "gipb200_pcg_get_info": (_I, [_VP, C.POINTER(PcgInfo)]),
+    "gipb200_check_bounded_wait": (_I, [_VP, C.POINTER(_I)]),
     "gipb200_pcg_kernel_time": (_I, [_VP, _I, _VP, C.POINTER(_D), C.POINTER(_D)]),
     "gipb200_pcg_solve": (_I, [_VP, _VP, _VP, _VP, _VP, C.POINTER(PcgResult)]),
     "gipb200_pcg_solve_static": (_I, [_I, _I, _VP, _VP, _VP, _VP, _VP, _VP, _I, _I, _D, _VP,
@@ -122,7 +123,7 @@ _SIGNATURES = {
                                 C.POINTER(_VP)]),
     "gipb200_dns_destroy": (_I, [_VP]),
     "gipb200_dns_advance": (_I, [_VP, _I, _VP]),
-    "gipb200_dns_history": (_I, [_VP, C.POINTER(_I), _VP, _VP, _VP, _VP, _VP, _VP]),
+    "gipb200_dns_history": (_I, [_VP, C.POINTER(_I), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "gipb200_dns_get_field": (_I, [_VP, C.c_char_p, _VP, _I]),
     "gipb200_dns_field_ptr": (_I, [_VP, C.c_char_p, C.POINTER(_VP), C.POINTER(_I)]),
     "gipb200_dns_copy_field": (_I, [_VP, C.c_char_p, _VP, _I, _VP]),

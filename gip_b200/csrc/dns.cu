@@ -294,6 +294,9 @@ struct CflStepFinish {
         H.iters[k] = pcg_mixed ? P->total_inner : P->iter;
         H.rr[k] = P->rr;
         H.outer[k] = pcg_mixed ? P->outer : 0;
+        // the step's 10 kernels and the PCG's: init + 3 per iteration in the FP64 forms,
+        // counted on the device in the mixed form
+        H.kernels[k] = 10 + (pcg_mixed ? P->kernels : 1 + 3 * P->iter);
       }
       S->step = k + 1;
     }
@@ -322,8 +325,9 @@ int Dns::grow_history(int need, cudaStream_t s) {
   if (need <= capacity) return GIPB200_OK;
   int cap = std::max(need, std::max(1024, capacity * 2));
   DevBuf<double> t, d, m, r;
-  DevBuf<int> it, ou;
+  DevBuf<int> it, ou, kn;
   GIPB_TRY(ou.alloc(cap));
+  GIPB_TRY(kn.alloc(cap));
   GIPB_TRY(t.alloc(cap));
   GIPB_TRY(d.alloc(cap));
   GIPB_TRY(m.alloc(cap));
@@ -336,6 +340,7 @@ int Dns::grow_history(int need, cudaStream_t s) {
     GIPB_CUDA(cudaMemcpyAsync(r.p, h_rr.p, capacity * 8, cudaMemcpyDeviceToDevice, s));
     GIPB_CUDA(cudaMemcpyAsync(it.p, h_iters.p, capacity * 4, cudaMemcpyDeviceToDevice, s));
     GIPB_CUDA(cudaMemcpyAsync(ou.p, h_outer.p, capacity * 4, cudaMemcpyDeviceToDevice, s));
+    GIPB_CUDA(cudaMemcpyAsync(kn.p, h_kernels.p, capacity * 4, cudaMemcpyDeviceToDevice, s));
     GIPB_CUDA(cudaStreamSynchronize(s));
   }
   std::swap(h_time.p, t.p);
@@ -344,8 +349,9 @@ int Dns::grow_history(int need, cudaStream_t s) {
   std::swap(h_rr.p, r.p);
   std::swap(h_iters.p, it.p);
   std::swap(h_outer.p, ou.p);
-  h_time.n = h_dt.n = h_massr.n = h_rr.n = h_iters.n = h_outer.n = cap;
-  t.n = d.n = m.n = r.n = it.n = ou.n = capacity;
+  std::swap(h_kernels.p, kn.p);
+  h_time.n = h_dt.n = h_massr.n = h_rr.n = h_iters.n = h_outer.n = h_kernels.n = cap;
+  t.n = d.n = m.n = r.n = it.n = ou.n = kn.n = capacity;
   capacity = cap;
   // a captured graph refers to the old history arrays
   if (exec) {
@@ -763,7 +769,7 @@ int gipb200_dns_advance(gipb200_dns Dh, int nsteps, void* stream) {
 }
 
 int gipb200_dns_history(gipb200_dns Dh, int* steps, double* t, double* dt, double* massr,
-                        int* iters, double* rr, int* outer) {
+                        int* iters, double* rr, int* outer, int* kernels) {
   if (!Dh) return fail(GIPB200_ERR_ARG, "null engine");
   Dns& E = Dh->E;
   GIPB_CUDA(cudaDeviceSynchronize());
@@ -777,6 +783,7 @@ int gipb200_dns_history(gipb200_dns Dh, int* steps, double* t, double* dt, doubl
   if (iters && n) GIPB_CUDA(cudaMemcpy(iters, E.h_iters.p, n * 4, cudaMemcpyDeviceToHost));
   if (rr && n) GIPB_CUDA(cudaMemcpy(rr, E.h_rr.p, n * 8, cudaMemcpyDeviceToHost));
   if (outer && n) GIPB_CUDA(cudaMemcpy(outer, E.h_outer.p, n * 4, cudaMemcpyDeviceToHost));
+  if (kernels && n) GIPB_CUDA(cudaMemcpy(kernels, E.h_kernels.p, n * 4, cudaMemcpyDeviceToHost));
   return GIPB200_OK;
 }
 

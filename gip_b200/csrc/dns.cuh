@@ -21,6 +21,7 @@ struct DnsHistory {
   int* iters;
   double* rr;
   int* outer;
+  int* kernels;  // kernels the step launched (early exits included)
   int capacity;
 };
 
@@ -33,7 +34,7 @@ struct Dns {
   Pcg pcg;
   DevBuf<DnsScalars> sc;
   DevBuf<double> h_time, h_dt, h_massr, h_rr;
-  DevBuf<int> h_iters, h_outer;
+  DevBuf<int> h_iters, h_outer, h_kernels;
   int capacity = 0;
   DevBuf<double> partials;
   DevBuf<unsigned> ticket;
@@ -69,7 +70,7 @@ struct Dns {
     if (cap_stream) cudaStreamDestroy(cap_stream);
   }
   DnsHistory history() const {
-    return {h_time.p, h_dt.p, h_massr.p, h_iters.p, h_rr.p, h_outer.p, capacity};
+    return {h_time.p, h_dt.p, h_massr.p, h_iters.p, h_rr.p, h_outer.p, h_kernels.p, capacity};
   }
   int grow_history(int need, cudaStream_t s);
   int enqueue_step(cudaStream_t s, bool host_sync);

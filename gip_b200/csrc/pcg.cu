@@ -39,6 +39,17 @@ __device__ __forceinline__ void set_loop(int use, cudaGraphConditionalHandle h, 
   if (use) cudaGraphSetConditional(h, keep ? 1u : 0u);
 }
 
+// Start of every FP32 loop kernel: count the launch; the SpMV, first kernel of an
+// iteration, also sets the loop's graph condition from the stop flag.
+__device__ __forceinline__ void mx_enter(PcgScalars* S, int use_cond,
+                                         cudaGraphConditionalHandle loop_cond) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    atomicAdd(&S->kernels, 1);
+    set_loop(use_cond, loop_cond, !S->done);
+  }
+}
+
+
 struct PcgInitFinish {
   PcgScalars* S;
   int mode, maxit;
@@ -307,6 +318,7 @@ __global__ void __launch_bounds__(256) k_mx_residual(SellView<double> L, const d
                                                      double delta, int maxit, int max_updates,
                                                      int pin_row, double pin_val, int use_cond,
                                                      cudaGraphConditionalHandle loop_cond) {
+  mx_enter(S, 0, 0);
   if (!first && (!S->upd || S->done)) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -348,20 +360,74 @@ struct AlphaFinish32 {
   }
 };
 
-__global__ void __launch_bounds__(256, 8) k_mx_spmv_dot(SellView<float> A, const float* __restrict__ p,
+// One row of the plain FP32 layout, the gathered vector being the new search direction
+// p = r + beta p_in formed on the fly (the same FMA as a separate update would do, so
+// the same values), summed slot by slot.
+template <int CH>
+__device__ __forceinline__ float sell_row_dir(const SellView<float>& A, const float* __restrict__ r,
+                                              const float* __restrict__ pin, float beta, int s,
+                                              int lane) {
+  const long long base = A.sptr[s];
+  const int len = (int)((A.sptr[s + 1] - base) >> 5);
+  const int* cp = A.col + base + lane;
+  const float* vp = A.val + base + lane;
+  float sum = 0.f;
+  for (int j0 = 0; j0 < len; j0 += CH) {
+    int c[CH];
+    float v[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+      if (j0 + t < len) {
+        c[t] = ld_stream(cp + (size_t)(j0 + t) * 32);
+        v[t] = ld_stream(vp + (size_t)(j0 + t) * 32);
+      } else {
+        c[t] = -1;
+        v[t] = 0.f;
+      }
+    }
+    float xv[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t)
+      xv[t] = (c[t] >= 0) ? fmaf(beta, __ldg(pin + c[t]), __ldg(r + c[t])) : 0.f;
+#pragma unroll
+    for (int t = 0; t < CH; ++t) sum = fmaf(xv[t], v[t], sum);
+  }
+  return sum;
+}
+
+// Ap = Â p and p.Ap with p = r + beta p_in (the direction update of GIP_LinearSolver.h:
+// 113-115 folded into the product): rows write p_out, gathers form p from r and p_in.
+__global__ void __launch_bounds__(256, 8) k_mx_spmv_dot(SellView<float> A, const float* __restrict__ r,
+                                                     const float* __restrict__ pin,
+                                                     float* __restrict__ pout,
                                                      float* __restrict__ Ap, PcgScalars* S,
-                                                     ReduceScratch rs) {
+                                                     ReduceScratch rs, int use_cond,
+                                                     cudaGraphConditionalHandle loop_cond) {
+  mx_enter(S, use_cond, loop_cond);
   if (S->done) return;
+  const float beta = (float)S->beta;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   double acc[1] = {0.0};
+  // slot range of the slice after next, loaded one iteration ahead of its L2 prefetch
+  long long n0 = -1, n1 = -1;
+  if (gw + nw < A.nslices) n0 = __ldg(A.sptr + gw + nw), n1 = __ldg(A.sptr + gw + nw + 1);
   for (int s = gw; s < A.nslices; s += nw) {
-    const float sum = sell_row_f32(A, p, s, lane);
+    if (lane == 0 && n0 >= 0 && n1 > n0) {  // this warp's next slice streams into L2
+      prefetch_l2(A.col + n0, (unsigned)(n1 - n0) * 4u);
+      prefetch_l2(A.val + n0, (unsigned)(n1 - n0) * 4u);
+    }
+    const int s2 = s + 2 * nw;
+    n0 = -1;
+    if (s2 < A.nslices) n0 = __ldg(A.sptr + s2), n1 = __ldg(A.sptr + s2 + 1);
+    const float sum = sell_row_dir<4>(A, r, pin, beta, s, lane);
     const int i = s * 32 + lane;
     if (i < A.nrows) {
+      const float pi = fmaf(beta, pin[i], r[i]);
+      pout[i] = pi;
       Ap[i] = sum;
-      acc[0] += (double)p[i] * (double)sum;
+      acc[0] += (double)pi * (double)sum;
     }
   }
   grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
@@ -371,8 +437,8 @@ __global__ void __launch_bounds__(256, 8) k_mx_spmv_dot(SellView<float> A, const
 // Every slot gathers (padding and stored zeros point at a valid column through delta 0
 // and multiply by table entry 0 = 0.0f, adding zero where the plain kernel adds x*0), so
 // the loop has no branches.  A warp owns a slice; in a packed slice each lane loads its
-// row's 16-byte delta word and its index word, then issues K independent gathers.  K = 7
-// when no packed row has an eighth slot.
+// row's 16-byte delta word and its index word, then issues K independent pairs of
+// gathers (r and p_in).  K = 7 when no packed row has an eighth slot.
 template <int NIB, int K>
 __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
                                                          const uint4* __restrict__ delta,
@@ -380,29 +446,28 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
                                                          const int* __restrict__ base,
                                                          const unsigned char* __restrict__ plain,
                                                          const float* __restrict__ table,
-                                                         const float* __restrict__ p,
+                                                         const float* __restrict__ r,
+                                                         const float* __restrict__ pin,
+                                                         float* __restrict__ pout,
                                                          float* __restrict__ Ap, PcgScalars* S,
-                                                         ReduceScratch rs) {
+                                                         ReduceScratch rs, int use_cond,
+                                                         cudaGraphConditionalHandle loop_cond) {
+  mx_enter(S, use_cond, loop_cond);
   if (S->done) return;
   constexpr int NT = 1 << NIB;
   __shared__ float tab[NT];
   for (int t = threadIdx.x; t < NT; t += blockDim.x) tab[t] = table[t];
   __syncthreads();
+  const float beta = (float)S->beta;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   double acc[1] = {0.0};
   for (int s = gw; s < A.nslices; s += nw) {
     const int i = s * 32 + lane;
-    // the packed words of this warp's next slice stream into L2 while this one gathers
-    if (lane == 0 && s + nw < A.nslices) {
-      const size_t nx = (size_t)(s + nw) * 32;
-      prefetch_l2(delta + nx, 32 * 16);
-      prefetch_l2(static_cast<const char*>(idx) + nx * (NIB / 2), 32 * (NIB / 2));
-    }
     float sum;
     if (__ldg(plain + s)) {
-      sum = sell_row_f32<2>(A, p, s, lane);  // rare fallback: keep its registers low
+      sum = sell_row_dir<2>(A, r, pin, beta, s, lane);  // rare fallback: few registers
     } else {
       const uint4 d = ld_stream(delta + i);
       unsigned w0, w1;
@@ -422,7 +487,7 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
                         b1.z + (int)(d.w & 0xffffu), b1.w + (int)(d.w >> 16)};
       float xv[K];
 #pragma unroll
-      for (int j = 0; j < K; ++j) xv[j] = __ldg(p + c[j]);
+      for (int j = 0; j < K; ++j) xv[j] = fmaf(beta, __ldg(pin + c[j]), __ldg(r + c[j]));
       sum = 0.f;
 #pragma unroll
       for (int j = 0; j < K; ++j) {
@@ -432,8 +497,181 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
       }
     }
     if (i < A.nrows) {
+      const float pi = fmaf(beta, pin[i], r[i]);
+      pout[i] = pi;
       Ap[i] = sum;
-      acc[0] += (double)p[i] * (double)sum;
+      acc[0] += (double)pi * (double)sum;
+    }
+  }
+  grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
+}
+
+// ------------------------------------------------------------------ TMA-staged packed SpMV
+// Bulk copies (cp.async.bulk, no tensor map, no multicast) and mbarriers, hand-written.
+namespace tma {
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void bar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void bar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void bar_expect(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// global -> this CTA's shared memory; completion counted on `bar` in bytes
+__device__ __forceinline__ void copy_g2s(void* dst, const void* src, unsigned bytes,
+                                         unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool bar_try(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for the phase with the given parity; gives up after ~1 s of SM clock.
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parity) {
+  const long long t0 = clock64();
+  while (!bar_try(bar, parity))
+    if (clock64() - t0 > 2000000000LL) return false;
+  return true;
+}
+}  // namespace tma
+
+// A wait that can never complete (no copy, no arrival): the bounded wait must give up.
+__global__ void k_bounded_wait_check(int* status) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x == 0) {
+    tma::bar_init(&bar, 1);
+    tma::bar_init_fence();
+    *status = tma::bar_wait(&bar, 0) ? GIPB200_OK : GIPB200_ERR_TIMEOUT;
+  }
+}
+
+// k_mxp_spmv_dot with the packed stream staged through shared memory: each block walks
+// chunks of 8 slices (one per warp); thread 0 keeps kStages chunks of delta words, index
+// words and slot bases in flight with bulk copies, so the warps only wait for their
+// gathers.  Plain slices (slot base -1) read the plain layout from global memory.  The
+// same FMA order as k_mxp_spmv_dot and k_mx_spmv_dot, so the same results.
+constexpr int kStages = 3;
+template <int NIB, int K>
+__global__ void __launch_bounds__(256, 8) k_mxt_spmv_dot(SellView<float> A,
+                                                         const uint4* __restrict__ delta,
+                                                         const void* __restrict__ idx,
+                                                         const int* __restrict__ base,
+                                                         const float* __restrict__ table,
+                                                         const float* __restrict__ r,
+                                                         const float* __restrict__ pin,
+                                                         float* __restrict__ pout,
+                                                         float* __restrict__ Ap, PcgScalars* S,
+                                                         ReduceScratch rs, int use_cond,
+                                                         cudaGraphConditionalHandle loop_cond) {
+  mx_enter(S, use_cond, loop_cond);
+  if (S->done) return;
+  constexpr int NT = 1 << NIB;
+  constexpr int IW = NIB / 4;  // 32-bit index words per row
+  __shared__ __align__(128) uint4 s_delta[kStages][256];
+  __shared__ __align__(128) unsigned s_idx[kStages][256 * IW];
+  __shared__ __align__(128) int s_base[kStages][64];
+  __shared__ __align__(8) unsigned long long s_bar[kStages];
+  __shared__ float tab[NT];
+  for (int t = threadIdx.x; t < NT; t += blockDim.x) tab[t] = table[t];
+  const int nchunks = (A.nslices + 7) >> 3;
+  // issues chunk c into stage st (thread 0)
+  auto fill = [&](int c, int st) {
+    const int nsl = min(8, A.nslices - 8 * c);
+    const unsigned bd = (unsigned)nsl * 512u, bi = (unsigned)nsl * 128u * IW,
+                   bb = (unsigned)nsl * 32u;
+    tma::bar_expect(&s_bar[st], bd + bi + bb);
+    tma::copy_g2s(&s_delta[st][0], delta + (size_t)c * 256, bd, &s_bar[st]);
+    tma::copy_g2s(&s_idx[st][0], static_cast<const unsigned*>(idx) + (size_t)c * 256 * IW, bi,
+                  &s_bar[st]);
+    tma::copy_g2s(&s_base[st][0], base + (size_t)c * 64, bb, &s_bar[st]);
+  };
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < kStages; ++st) tma::bar_init(&s_bar[st], 1);
+    tma::bar_init_fence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int st = 0; st < kStages; ++st) {
+      const int c = blockIdx.x + st * gridDim.x;
+      if (c < nchunks) fill(c, st);
+    }
+  const float beta = (float)S->beta;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double acc[1] = {0.0};
+  bool failed = false;
+  int it = 0;
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x, ++it) {
+    const int st = it % kStages;
+    const unsigned par = (unsigned)(it / kStages) & 1u;
+    const bool ok = tma::bar_wait(&s_bar[st], par);
+    if (__syncthreads_or(!ok)) {  // a copy never landed: stop, report, drain
+      failed = true;
+      break;
+    }
+    const int s = 8 * c + warp;
+    if (s < A.nslices) {
+      const int i = s * 32 + lane;
+      const int* sb = &s_base[st][warp * 8];
+      float sum;
+      if (sb[0] < 0) {
+        sum = sell_row_dir<2>(A, r, pin, beta, s, lane);
+      } else {
+        const uint4 d = s_delta[st][warp * 32 + lane];
+        const unsigned w0 = s_idx[st][(warp * 32 + lane) * IW];
+        const unsigned w1 = (IW == 2) ? s_idx[st][(warp * 32 + lane) * IW + 1] : 0u;
+        const int c8[8] = {sb[0] + (int)(d.x & 0xffffu), sb[1] + (int)(d.x >> 16),
+                           sb[2] + (int)(d.y & 0xffffu), sb[3] + (int)(d.y >> 16),
+                           sb[4] + (int)(d.z & 0xffffu), sb[5] + (int)(d.z >> 16),
+                           sb[6] + (int)(d.w & 0xffffu), sb[7] + (int)(d.w >> 16)};
+        float xv[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) xv[j] = fmaf(beta, __ldg(pin + c8[j]), __ldg(r + c8[j]));
+        sum = 0.f;
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+          const unsigned id =
+              (NIB == 4) ? (w0 >> (4 * j)) & 15u : ((j < 4 ? w0 : w1) >> (8 * (j & 3))) & 255u;
+          sum = fmaf(xv[j], tab[id], sum);
+        }
+      }
+      if (i < A.nrows) {
+        const float pi = fmaf(beta, pin[i], r[i]);
+        pout[i] = pi;
+        Ap[i] = sum;
+        acc[0] += (double)pi * (double)sum;
+      }
+    }
+    __syncthreads();  // every warp is done with stage st
+    if (threadIdx.x == 0) {
+      const int nc = c + kStages * gridDim.x;
+      if (nc < nchunks) fill(nc, st);
+    }
+  }
+  if (failed && threadIdx.x == 0) {
+    S->status = GIPB200_ERR_TIMEOUT;
+    S->done = 1;
+    // wait (bounded) for the copies still in flight into this block's shared memory
+    for (int k = 0; k < kStages; ++k) {
+      const int j = it + k;
+      if (blockIdx.x + j * gridDim.x < nchunks)
+        tma::bar_wait(&s_bar[j % kStages], (unsigned)(j / kStages) & 1u);
     }
   }
   grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
@@ -479,6 +717,7 @@ __global__ void __launch_bounds__(256) k_mx_update(int n, float* __restrict__ y,
                                                    ReduceScratch rs, double delta, int maxit,
                                                    int pin_row, const double* __restrict__ scale,
                                                    int use_cond, cudaGraphConditionalHandle upd_cond) {
+  mx_enter(S, 0, 0);
   if (S->done) return;
   const float alpha = (float)S->alpha;
   double acc[1] = {0.0};
@@ -517,7 +756,8 @@ __global__ void __launch_bounds__(256) k_mx_update(int n, float* __restrict__ y,
 // x += S y + kappa (FP64); y = 0   -- only when a replacement is due
 __global__ void __launch_bounds__(256) k_mx_apply(int n, double* __restrict__ x, float* __restrict__ y,
                                                   const double* __restrict__ scale,
-                                                  const PcgScalars* S) {
+                                                  PcgScalars* S) {
+  mx_enter(S, 0, 0);
   if (!S->upd || S->done) return;
   const double kappa = S->kappa;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -527,28 +767,6 @@ __global__ void __launch_bounds__(256) k_mx_apply(int n, double* __restrict__ x,
 }
 
 // p = r^ + beta p; sets the while-loop value
-__global__ void __launch_bounds__(256) k_mx_pupdate(int n, float* __restrict__ p,
-                                                    const float* __restrict__ r,
-                                                    const PcgScalars* S, int use_cond,
-                                                    cudaGraphConditionalHandle loop_cond) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) set_loop(use_cond, loop_cond, !S->done);
-  if (S->done) return;
-  const float beta = (float)S->beta;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  const int n4 = n >> 2;
-  float4* p4 = reinterpret_cast<float4*>(p);
-  const float4* r4 = reinterpret_cast<const float4*>(r);
-  for (int q = tid; q < n4; q += stride) {
-    float4 pv = p4[q];
-    const float4 rv = r4[q];
-    pv.x = fmaf(beta, pv.x, rv.x);
-    pv.y = fmaf(beta, pv.y, rv.y);
-    pv.z = fmaf(beta, pv.z, rv.z);
-    pv.w = fmaf(beta, pv.w, rv.w);
-    p4[q] = pv;
-  }
-  for (int i = 4 * n4 + tid; i < n; i += stride) p[i] = fmaf(beta, p[i], r[i]);
-}
 
 // scale = 1/sqrt(L_ii); lhat = S L S (columns outside the unknowns dropped to 0)
 __global__ void k_mx_scale(int n, const int* __restrict__ rp, const int* __restrict__ col,
@@ -636,6 +854,8 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
     GIPB_TRY(lhat.alloc((size_t)std::max<long long>(L->nslots, 1)));
     GIPB_TRY(p32.alloc(n_all));
     GIPB_TRY(p32.zero(s));
+    GIPB_TRY(p32b.alloc(n_all));
+    GIPB_TRY(p32b.zero(s));
     GIPB_TRY(Ap32.alloc(n));
     GIPB_TRY(r32.alloc(n));
     GIPB_TRY(y32.alloc(n));
@@ -799,6 +1019,7 @@ int Pcg::build_compressed(cudaStream_t s) {
     }
     if (!ok) {
       plain_slots += 32LL * len;
+      for (int j = 0; j < 8; ++j) base[(size_t)sl * 8 + j] = -1;  // marks a plain slice
       continue;
     }
     plain[sl] = 0;
@@ -833,13 +1054,32 @@ int Pcg::build_compressed(cudaStream_t s) {
   GIPB_CUDA(cudaStreamSynchronize(s));
   cop.index_bits = nib;
   cop.slots = max_len <= 7 ? 7 : 8;
+  cop.tma = getenv("GIPB200_NO_TMA") == nullptr;
+  if (cop.tma) {
+    // enough shared memory per SM for 8 resident blocks (the rest stays L1), and the
+    // grid cap that keeps the kernel in one wave
+    const void* kfn = nib == 4 ? (cop.slots == 7 ? (const void*)k_mxt_spmv_dot<4, 7>
+                                                 : (const void*)k_mxt_spmv_dot<4, 8>)
+                               : (cop.slots == 7 ? (const void*)k_mxt_spmv_dot<8, 7>
+                                                 : (const void*)k_mxt_spmv_dot<8, 8>);
+    cudaFuncAttributes fa;
+    GIPB_CUDA(cudaFuncGetAttributes(&fa, kfn));
+    int dev = 0, smem_sm = 0;
+    GIPB_CUDA(cudaGetDevice(&dev));
+    GIPB_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    const int pct = (int)std::min<long long>(
+        100, (800LL * ((long long)fa.sharedSizeBytes + 1024) + smem_sm - 1) / smem_sm);
+    GIPB_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+    GIPB_TRY(one_wave(kfn, kMaxReduceBlocks, &cop.max_blocks));
+  }
   cop.ntable = (int)keys.size() + 1;
   // streamed bytes: packed rows (delta + index words), their slot bases; plain slices
-  // (column + value per slot, slice offsets); the plain flags; p and Ap once per row
+  // (column + value per slot, slice offsets); the plain flags; per row r and the old
+  // direction read once, the new direction and the product written once
   const double packed_rows = 32.0 * (double)packed_slices;
   cop.bytes_per_launch = packed_rows * (16.0 + nib) + (double)packed_slices * 32.0 +
                          (double)plain_slots * 8.0 + (double)(ns - packed_slices) * 16.0 +
-                         (double)ns + (double)L->nrows * 8.0;
+                         (double)ns + (double)L->nrows * 16.0;
   cop.enabled = true;
   return GIPB200_OK;
 }
@@ -862,7 +1102,9 @@ int Pcg::read_flag(cudaStream_t s, int which, int* v) {
   return GIPB200_OK;
 }
 
-static void launch_mx_spmv(const Pcg& P, float* Ap, PcgScalars* sc, cudaStream_t s);
+static void launch_mx_spmv(const Pcg& P, const float* pin, float* pout, float* Ap,
+                           PcgScalars* sc, int use_cond, cudaGraphConditionalHandle h,
+                           cudaStream_t s);
 
 // ------------------------------------------------------------------ conditional while-nodes
 static bool capturing(cudaStream_t s) {
@@ -988,34 +1230,39 @@ int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaS
   cudaStream_t os = body_stream[0], is = body_stream[1];
   GIPB_CUDA(cudaStreamBeginCaptureToGraph(os, loop_body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
+  // two iterations per body: the first reads direction buffer p32 and writes p32b, the
+  // second the reverse.  Each kernel returns at once when the solve has finished, and
+  // the SpMV sets the loop condition, so the loop ends within one body of the stop flag.
   int st = [&]() -> int {
-    cudaGraphConditionalHandle hu;
-    GIPB_TRY(make_handle(os, 0, 0, &hu));
-    launch_mx_spmv(*this, Ap32.p, sc.p, os);
-    k_mx_update<<<blocks_vec, 256, 0, os>>>(n, y32.p, r32.p, p32.p, Ap32.p, sc.p, rs,
-                                             prm.inner_tol, prm.maxit, pin_row, scale.p, 1, hu);
-    GIPB_LAUNCH_CHECK();
-    cudaGraph_t if_body;
-    GIPB_TRY(add_if(os, hu, &if_body));
-    GIPB_CUDA(cudaStreamBeginCaptureToGraph(is, if_body, nullptr, nullptr, 0,
-                                            cudaStreamCaptureModeRelaxed));
-    k_mx_apply<<<blocks_vec, 256, 0, is>>>(n, x, y32.p, scale.p, sc.p);
-    int rst = launch_mixed_residual(b, x, 0, is, 0, 0);
-    cudaError_t le = cudaGetLastError();
-    cudaGraph_t out = nullptr;
-    GIPB_CUDA(cudaStreamEndCapture(is, &out));
-    if (rst != GIPB200_OK) return rst;
-    if (le != cudaSuccess)
-      return fail(GIPB200_ERR_CUDA, "launch in replacement body: %s", cudaGetErrorString(le));
-    k_mx_pupdate<<<blocks_vec, 256, 0, os>>>(n, p32.p, r32.p, sc.p, 1, hl);
-    GIPB_LAUNCH_CHECK();
+    for (int half = 0; half < 2; ++half) {
+      float* pin = half ? p32b.p : p32.p;
+      float* pout = half ? p32.p : p32b.p;
+      cudaGraphConditionalHandle hu;
+      GIPB_TRY(make_handle(os, 0, 0, &hu));
+      launch_mx_spmv(*this, pin, pout, Ap32.p, sc.p, 1, hl, os);
+      k_mx_update<<<blocks_vec, 256, 0, os>>>(n, y32.p, r32.p, pout, Ap32.p, sc.p, rs,
+                                               prm.inner_tol, prm.maxit, pin_row, scale.p, 1, hu);
+      GIPB_LAUNCH_CHECK();
+      cudaGraph_t if_body;
+      GIPB_TRY(add_if(os, hu, &if_body));
+      GIPB_CUDA(cudaStreamBeginCaptureToGraph(is, if_body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeRelaxed));
+      k_mx_apply<<<blocks_vec, 256, 0, is>>>(n, x, y32.p, scale.p, sc.p);
+      int rst = launch_mixed_residual(b, x, 0, is, 0, 0);
+      cudaError_t le = cudaGetLastError();
+      cudaGraph_t out = nullptr;
+      GIPB_CUDA(cudaStreamEndCapture(is, &out));
+      if (rst != GIPB200_OK) return rst;
+      if (le != cudaSuccess)
+        return fail(GIPB200_ERR_CUDA, "launch in replacement body: %s", cudaGetErrorString(le));
+    }
     return GIPB200_OK;
   }();
   cudaGraph_t out = nullptr;
   cudaError_t ce = cudaStreamEndCapture(os, &out);
   if (st != GIPB200_OK) return st;
   if (ce != cudaSuccess) return fail(GIPB200_ERR_CUDA, "loop body capture: %s", cudaGetErrorString(ce));
-  launches += 4;
+  launches += 8;
   return GIPB200_OK;
 }
 
@@ -1045,24 +1292,39 @@ int Pcg::enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t
   return GIPB200_OK;
 }
 
-static void launch_mx_spmv(const Pcg& P, float* Ap, PcgScalars* sc, cudaStream_t s) {
+static void launch_mx_spmv(const Pcg& P, const float* pin, float* pout, float* Ap,
+                           PcgScalars* sc, int use_cond, cudaGraphConditionalHandle h,
+                           cudaStream_t s) {
   const CompressedOp& c = P.cop;
   const SellView<float> A = P.a32();
-  const int nb = P.blocks_spmv;
+  const int nb = c.tma ? std::min(P.blocks_spmv, c.max_blocks) : P.blocks_spmv;
+  const float* r = P.r32.p;
   if (!c.enabled)
-    k_mx_spmv_dot<<<nb, 256, 0, s>>>(A, P.p32.p, Ap, sc, P.rs);
+    k_mx_spmv_dot<<<nb, 256, 0, s>>>(A, r, pin, pout, Ap, sc, P.rs, use_cond, h);
+  else if (c.tma && c.index_bits == 4 && c.slots == 7)
+    k_mxt_spmv_dot<4, 7><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.table.p, r, pin,
+                                             pout, Ap, sc, P.rs, use_cond, h);
+  else if (c.tma && c.index_bits == 4)
+    k_mxt_spmv_dot<4, 8><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.table.p, r, pin,
+                                             pout, Ap, sc, P.rs, use_cond, h);
+  else if (c.tma && c.slots == 7)
+    k_mxt_spmv_dot<8, 7><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.table.p, r, pin,
+                                             pout, Ap, sc, P.rs, use_cond, h);
+  else if (c.tma)
+    k_mxt_spmv_dot<8, 8><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.table.p, r, pin,
+                                             pout, Ap, sc, P.rs, use_cond, h);
   else if (c.index_bits == 4 && c.slots == 7)
     k_mxp_spmv_dot<4, 7><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.plain.p,
-                                             c.table.p, P.p32.p, Ap, sc, P.rs);
+                                             c.table.p, r, pin, pout, Ap, sc, P.rs, use_cond, h);
   else if (c.index_bits == 4)
     k_mxp_spmv_dot<4, 8><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.plain.p,
-                                             c.table.p, P.p32.p, Ap, sc, P.rs);
+                                             c.table.p, r, pin, pout, Ap, sc, P.rs, use_cond, h);
   else if (c.slots == 7)
     k_mxp_spmv_dot<8, 7><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.plain.p,
-                                             c.table.p, P.p32.p, Ap, sc, P.rs);
+                                             c.table.p, r, pin, pout, Ap, sc, P.rs, use_cond, h);
   else
     k_mxp_spmv_dot<8, 8><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.plain.p,
-                                             c.table.p, P.p32.p, Ap, sc, P.rs);
+                                             c.table.p, r, pin, pout, Ap, sc, P.rs, use_cond, h);
 }
 
 int Pcg::launch_mixed_residual(const double* b, const double* x, int first, cudaStream_t s,
@@ -1082,14 +1344,14 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 0, 0));
   const int poll = 16;
   for (int k = 0; k < prm.maxit; ++k) {
-    launch_mx_spmv(*this, Ap32.p, sc.p, s);
-    k_mx_update<<<blocks_vec, 256, 0, s>>>(n, y32.p, r32.p, p32.p, Ap32.p, sc.p, rs, prm.inner_tol,
+    float* pin = (k & 1) ? p32b.p : p32.p;
+    float* pout = (k & 1) ? p32.p : p32b.p;
+    launch_mx_spmv(*this, pin, pout, Ap32.p, sc.p, 0, 0, s);
+    k_mx_update<<<blocks_vec, 256, 0, s>>>(n, y32.p, r32.p, pout, Ap32.p, sc.p, rs, prm.inner_tol,
                                             prm.maxit, pin_row, scale.p, 0, 0);
     k_mx_apply<<<blocks_vec, 256, 0, s>>>(n, x, y32.p, scale.p, sc.p);
     GIPB_LAUNCH_CHECK();
     GIPB_TRY(launch_mixed_residual(b, x, 0, s, 0, 0));
-    k_mx_pupdate<<<blocks_vec, 256, 0, s>>>(n, p32.p, r32.p, sc.p, 0, 0);
-    GIPB_LAUNCH_CHECK();
     launches += 4;
     if (host_sync && (k + 1) % poll == 0) {
       int d;
@@ -1125,7 +1387,7 @@ int Pcg::time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* 
   for (int k = 0; k <= reps; ++k) {
     if (k == 1) GIPB_CUDA(cudaEventRecord(e0, s));
     if (mixed)
-      launch_mx_spmv(*this, tAp32.p, tsc.p, s);
+      launch_mx_spmv(*this, p32.p, p32b.p, tAp32.p, tsc.p, 0, 0, s);
     else
       k_pcg_spmv_dot<<<blocks_spmv, 256, 0, s>>>(L->view(), p.p, tAp.p, tsc.p, rs,
                                                   GIPB200_PCG_FIXED);
@@ -1139,9 +1401,10 @@ int Pcg::time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* 
   cudaEventDestroy(e1);
   *avg_ms = (double)ms / reps;
   // compulsory bytes: stored values + indices once, slice offsets, p once, Ap once
+  // (mixed: r and the old direction read, the new direction and the product written)
   const double vbytes = mixed ? 4.0 : 8.0;
   *bytes = (double)L->nnz * (vbytes + 4.0) + (double)(L->nslices + 1) * 8.0 +
-           (double)L->nrows * 2.0 * vbytes;
+           (double)L->nrows * (mixed ? 4.0 : 2.0) * vbytes;
   if (mixed && cop.enabled) *bytes = cop.bytes_per_launch;
   return GIPB200_OK;
 }
@@ -1182,6 +1445,18 @@ int gipb200_pcg_create(gipb200_matrix L, int n_all, const gipb200_pcg_params* pa
 
 int gipb200_pcg_destroy(gipb200_pcg S) {
   delete S;
+  return GIPB200_OK;
+}
+
+int gipb200_check_bounded_wait(void* stream, int* h_status) {
+  if (!h_status) return fail(GIPB200_ERR_ARG, "null argument");
+  cudaStream_t s = as_stream(stream);
+  DevBuf<int> st;
+  GIPB_TRY(st.alloc(1));
+  k_bounded_wait_check<<<1, 32, 0, s>>>(st.p);
+  GIPB_LAUNCH_CHECK();
+  GIPB_CUDA(cudaMemcpyAsync(h_status, st.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaStreamSynchronize(s));
   return GIPB200_OK;
 }
 

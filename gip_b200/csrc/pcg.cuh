@@ -20,7 +20,8 @@ struct PcgScalars {
   int status;       // GIPB200_OK or GIPB200_ERR_BREAKDOWN / NOT_CONVERGED
   int outer;        // MIXED: refinement cycles done
   int total_inner;  // MIXED: inner iterations summed over cycles
-  int pad[2];
+  int kernels;      // MIXED: PCG kernel launches of this solve, early exits included
+  int pad1;
   double rsum;      // MIXED: sum of the FP64 residual (pinned-Neumann deflation)
   double kappa_c;   // MIXED: sum(r)/pin of the current segment
   double kappa;     // MIXED: constant added to x at the next replacement
@@ -41,6 +42,8 @@ struct CompressedOp {
   bool enabled = false;
   int index_bits = 0;            // 4 or 8
   int slots = 8;                 // 7: no packed row uses the eighth slot
+  bool tma = true;               // stage the packed stream through shared memory
+  int max_blocks = 0;            // resident blocks of the staged kernel (one wave)
   DevBuf<uint4> delta;           // per row (nslices * 32)
   DevBuf<unsigned> idx4;         // per row, 8 x 4 bits
   DevBuf<uint2> idx8;            // per row, 8 x 8 bits
@@ -63,6 +66,7 @@ struct Pcg {
   DevBuf<int> col32;         // their columns (-1: padding and dropped ghost columns)
   DevBuf<double> scale;      // S = 1/sqrt(L_ii)
   DevBuf<float> p32, Ap32, r32, y32;
+  DevBuf<float> p32b;        // second direction buffer: each SpMV reads one, writes the other
   CompressedOp cop;
   int sort_fp32_rows(cudaStream_t s);
   void launch_pcg_update(double* x, cudaStream_t s);

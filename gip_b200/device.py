@@ -247,13 +247,14 @@ class DnsEngine:
     def history(self) -> Dict[str, np.ndarray]:
         steps = C.c_int()
         L.call("gipb200_dns_history", self.handle, C.byref(steps), None, None, None, None, None,
-               None)
+               None, None)
         n = steps.value
         out = {"time": np.zeros(n), "dt": np.zeros(n), "massr": np.zeros(n),
-               "iters": np.zeros(n, np.int32), "rr": np.zeros(n), "outer": np.zeros(n, np.int32)}
+               "iters": np.zeros(n, np.int32), "rr": np.zeros(n), "outer": np.zeros(n, np.int32),
+               "kernels": np.zeros(n, np.int32)}
         L.call("gipb200_dns_history", self.handle, C.byref(steps), _hptr(out["time"]),
                _hptr(out["dt"]), _hptr(out["massr"]), _hptr(out["iters"]), _hptr(out["rr"]),
-               _hptr(out["outer"]))
+               _hptr(out["outer"]), _hptr(out["kernels"]))
         return out
 
     def field(self, name: str) -> np.ndarray:

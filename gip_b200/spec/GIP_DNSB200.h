@@ -74,7 +74,7 @@ inline void GIP_DNS<GIP_MatrixB200, GIP_VectorB200, GIP_ArchB200, GIP_NonLinearB
   std::vector<double> t(maxIt > 0 ? maxIt : 1), dtv(t.size()), mr(t.size()), rr(t.size());
   std::vector<int> its(t.size());
   gipb200_require(gipb200_dns_history(E, &steps, t.data(), dtv.data(), mr.data(), its.data(),
-                                      rr.data(), 0),
+                                      rr.data(), 0, 0),
                   "gipb200_dns_history");
   int rank;
   MPI_Comm_rank(MPI_COMM_WORLD, &rank);

@@ -145,6 +145,12 @@ int gipb200_pcg_destroy(gipb200_pcg S);
 int gipb200_pcg_solve(gipb200_pcg S, const double* d_b, double* d_x, const double* d_x0,
                       void* stream, gipb200_pcg_result* h_result);
 
+/* No counterpart in the reference: launches a kernel whose shared-memory barrier wait can
+ * never complete and writes the status it reported (GIPB200_ERR_TIMEOUT after about one
+ * second of SM clock).  Checks on the device that the bounded wait of the staged SpMV
+ * gives up instead of hanging; the context stays usable. */
+int gipb200_check_bounded_wait(void* stream, int* h_status);
+
 /* No counterpart in the reference: how the solver stores its operator. */
 typedef struct {
   int pin_row;                 /* MIXED: detected pinned-Neumann row (-1: none)           */
@@ -216,9 +222,12 @@ int gipb200_dns_destroy(gipb200_dns E);
 int gipb200_dns_advance(gipb200_dns E, int nsteps, void* stream);
 /* Per-step history of all steps so far (host arrays of length >= steps taken, any may
  * be NULL): time, dt used, massr (GIP_DNS.h:399-404), PCG iterations (MIXED: FP32
- * iterations), final r.r, MIXED residual replacements (FP64 true-residual updates). */
+ * iterations), final r.r, MIXED residual replacements (FP64 true-residual updates), and
+ * the library kernels the step launched (kernels that found their solve finished and
+ * returned at once included). */
 int gipb200_dns_history(gipb200_dns E, int* steps_taken, double* h_time, double* h_dt,
-                        double* h_massr, int* h_iters, double* h_rr, int* h_outer);
+                        double* h_massr, int* h_iters, double* h_rr, int* h_outer,
+                        int* h_kernels);
 /* Copies a field to the host: "u","v","w","p","p0","mf","ax0","ay0","az0","gpx",... */
 int gipb200_dns_get_field(gipb200_dns E, const char* name, double* h_out, int n);
 /* Copies h_in[0:n) into a field at `offset` on `stream` (no host synchronisation; the

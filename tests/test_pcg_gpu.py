@@ -119,14 +119,18 @@ def test_mixed_packed_operator_8bit_table_and_plain_slices(gpu, monkeypatch):
     info = S.info()
     assert info["compressed"] == 1 and info["value_table"] == 8 and info["pin_row"] == 0
     assert 0.5 < info["compressed_fraction"] < 1.0
+    monkeypatch.setenv("GIPB200_NO_TMA", "1")  # packed words read straight from global memory
+    T = dv.PcgSolver(dv.DeviceMatrix(L), **kw)
     monkeypatch.setenv("GIPB200_NO_COMPRESS", "1")
     P = dv.PcgSolver(dv.DeviceMatrix(L), **kw)
     assert P.info()["compressed"] == 0
-    xs, xp = _t(np.zeros(L.nrows)), _t(np.zeros(L.nrows))
+    xs, xt, xp = _t(np.zeros(L.nrows)), _t(np.zeros(L.nrows)), _t(np.zeros(L.nrows))
     rs = S.solve(_t(b), xs, _t(np.zeros(L.nrows)))
+    rt = T.solve(_t(b), xt, _t(np.zeros(L.nrows)))
     rp = P.solve(_t(b), xp, _t(np.zeros(L.nrows)))
     assert rs["status"] == 0 and (rs["iterations"], rs["outer"]) == (rp["iterations"], rp["outer"])
-    assert torch.equal(xs, xp)
+    assert (rt["iterations"], rt["outer"]) == (rp["iterations"], rp["outer"])
+    assert torch.equal(xs, xp) and torch.equal(xt, xp)
     r = b - L.to_scipy() @ xs.cpu().numpy()
     assert np.linalg.norm(r) <= 1e-9 * np.linalg.norm(b) * 1.0001
 
@@ -148,3 +152,16 @@ def test_pcg_reports_breakdown_and_nonconvergence(gpu, mode):
     assert S2.solve(_t(bad), x, _t(np.zeros(L.nrows)))["status"] == 3  # BREAKDOWN
     res = S2.solve(_t(b), x, _t(np.zeros(L.nrows)))  # the solver is still usable
     assert res["status"] == 0
+
+
+def test_bounded_wait_gives_up_with_status(gpu):
+    # a barrier wait that nothing completes times out and reports; the context stays usable
+    import ctypes as C
+    from gip_b200 import _lib
+    from gip_b200 import device as dv
+    st = C.c_int(-1)
+    _lib.call("gipb200_check_bounded_wait", None, C.byref(st))
+    assert st.value == 4  # GIPB200_ERR_TIMEOUT
+    L, b = cavity.poisson_problem(6, seed=1)
+    S = dv.PcgSolver(dv.DeviceMatrix(L), mode="tol", maxit=500, tol=1e-8)
+    assert S.solve(_t(b), _t(np.zeros(L.nrows)), _t(np.zeros(L.nrows)))["status"] == 0
