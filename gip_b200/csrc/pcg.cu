@@ -562,12 +562,13 @@ __global__ void k_bounded_wait_check(int* status) {
   }
 }
 
-// k_mxp_spmv_dot with the packed stream staged through shared memory: each block walks
-// chunks of 8 slices (one per warp); thread 0 keeps kStages chunks of delta words, index
-// words and slot bases in flight with bulk copies, so the warps only wait for their
-// gathers.  Plain slices (slot base -1) read the plain layout from global memory.  The
-// same FMA order as k_mxp_spmv_dot and k_mx_spmv_dot, so the same results.
-constexpr int kStages = 3;
+// k_mxp_spmv_dot with the packed stream staged through shared memory by bulk copies.
+// Each warp runs its own pipeline over its own slices (gw, gw + nw, ...): lane 0 keeps
+// kStages slices of delta words, index words and slot bases in flight, each stage with
+// its own mbarrier, so a warp waits only for its own data and never for other warps.
+// Plain slices (slot base -1) read the plain layout from global memory.  The same FMA
+// order as k_mxp_spmv_dot and k_mx_spmv_dot, so the same results.
+constexpr int kStages = 4;
 template <int NIB, int K>
 __global__ void __launch_bounds__(256, 8) k_mxt_spmv_dot(SellView<float> A,
                                                          const uint4* __restrict__ delta,
@@ -584,94 +585,92 @@ __global__ void __launch_bounds__(256, 8) k_mxt_spmv_dot(SellView<float> A,
   if (S->done) return;
   constexpr int NT = 1 << NIB;
   constexpr int IW = NIB / 4;  // 32-bit index words per row
-  __shared__ __align__(128) uint4 s_delta[kStages][256];
-  __shared__ __align__(128) unsigned s_idx[kStages][256 * IW];
-  __shared__ __align__(128) int s_base[kStages][64];
-  __shared__ __align__(8) unsigned long long s_bar[kStages];
+  __shared__ __align__(128) uint4 s_delta[8][kStages][32];
+  __shared__ __align__(128) unsigned s_idx[8][kStages][32 * IW];
+  __shared__ __align__(128) int s_base[8][kStages][8];
+  __shared__ __align__(8) unsigned long long s_bar[8][kStages];
   __shared__ float tab[NT];
   for (int t = threadIdx.x; t < NT; t += blockDim.x) tab[t] = table[t];
-  const int nchunks = (A.nslices + 7) >> 3;
-  // issues chunk c into stage st (thread 0)
-  auto fill = [&](int c, int st) {
-    const int nsl = min(8, A.nslices - 8 * c);
-    const unsigned bd = (unsigned)nsl * 512u, bi = (unsigned)nsl * 128u * IW,
-                   bb = (unsigned)nsl * 32u;
-    tma::bar_expect(&s_bar[st], bd + bi + bb);
-    tma::copy_g2s(&s_delta[st][0], delta + (size_t)c * 256, bd, &s_bar[st]);
-    tma::copy_g2s(&s_idx[st][0], static_cast<const unsigned*>(idx) + (size_t)c * 256 * IW, bi,
-                  &s_bar[st]);
-    tma::copy_g2s(&s_base[st][0], base + (size_t)c * 64, bb, &s_bar[st]);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  uint4(*sd)[32] = s_delta[warp];
+  unsigned(*si)[32 * IW] = s_idx[warp];
+  int(*sb)[8] = s_base[warp];
+  unsigned long long* bar = s_bar[warp];
+  // slice sl into stage st (lane 0)
+  auto fill = [&](int sl, int st) {
+    tma::bar_expect(&bar[st], 512u + 128u * IW + 32u);
+    tma::copy_g2s(&sd[st][0], delta + (size_t)sl * 32, 512u, &bar[st]);
+    tma::copy_g2s(&si[st][0], static_cast<const unsigned*>(idx) + (size_t)sl * 32 * IW,
+                  128u * IW, &bar[st]);
+    tma::copy_g2s(&sb[st][0], base + (size_t)sl * 8, 32u, &bar[st]);
   };
-  if (threadIdx.x == 0) {
-    for (int st = 0; st < kStages; ++st) tma::bar_init(&s_bar[st], 1);
+  if (lane == 0) {
+    for (int st = 0; st < kStages; ++st) tma::bar_init(&bar[st], 1);
     tma::bar_init_fence();
   }
-  __syncthreads();
-  if (threadIdx.x == 0)
+  __syncthreads();  // table and barriers ready
+  if (lane == 0)
     for (int st = 0; st < kStages; ++st) {
-      const int c = blockIdx.x + st * gridDim.x;
-      if (c < nchunks) fill(c, st);
+      const int sl = gw + st * nw;
+      if (sl < A.nslices) fill(sl, st);
     }
   const float beta = (float)S->beta;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double acc[1] = {0.0};
   bool failed = false;
   int it = 0;
-  for (int c = blockIdx.x; c < nchunks; c += gridDim.x, ++it) {
+  for (int s = gw; s < A.nslices; s += nw, ++it) {
     const int st = it % kStages;
     const unsigned par = (unsigned)(it / kStages) & 1u;
-    const bool ok = tma::bar_wait(&s_bar[st], par);
-    if (__syncthreads_or(!ok)) {  // a copy never landed: stop, report, drain
+    const bool ok = tma::bar_wait(&bar[st], par);
+    if (!__all_sync(0xffffffffu, ok)) {  // a copy never landed: stop, report, drain
       failed = true;
       break;
     }
-    const int s = 8 * c + warp;
-    if (s < A.nslices) {
-      const int i = s * 32 + lane;
-      const int* sb = &s_base[st][warp * 8];
-      float sum;
-      if (sb[0] < 0) {
-        sum = sell_row_dir<2>(A, r, pin, beta, s, lane);
-      } else {
-        const uint4 d = s_delta[st][warp * 32 + lane];
-        const unsigned w0 = s_idx[st][(warp * 32 + lane) * IW];
-        const unsigned w1 = (IW == 2) ? s_idx[st][(warp * 32 + lane) * IW + 1] : 0u;
-        const int c8[8] = {sb[0] + (int)(d.x & 0xffffu), sb[1] + (int)(d.x >> 16),
-                           sb[2] + (int)(d.y & 0xffffu), sb[3] + (int)(d.y >> 16),
-                           sb[4] + (int)(d.z & 0xffffu), sb[5] + (int)(d.z >> 16),
-                           sb[6] + (int)(d.w & 0xffffu), sb[7] + (int)(d.w >> 16)};
-        float xv[K];
+    const int i = s * 32 + lane;
+    float sum;
+    if (sb[st][0] < 0) {
+      sum = sell_row_dir<2>(A, r, pin, beta, s, lane);
+    } else {
+      const uint4 d = sd[st][lane];
+      const unsigned w0 = si[st][lane * IW];
+      const unsigned w1 = (IW == 2) ? si[st][lane * IW + 1] : 0u;
+      const int* b8 = sb[st];
+      const int c8[8] = {b8[0] + (int)(d.x & 0xffffu), b8[1] + (int)(d.x >> 16),
+                         b8[2] + (int)(d.y & 0xffffu), b8[3] + (int)(d.y >> 16),
+                         b8[4] + (int)(d.z & 0xffffu), b8[5] + (int)(d.z >> 16),
+                         b8[6] + (int)(d.w & 0xffffu), b8[7] + (int)(d.w >> 16)};
+      float xv[K];
 #pragma unroll
-        for (int j = 0; j < K; ++j) xv[j] = fmaf(beta, __ldg(pin + c8[j]), __ldg(r + c8[j]));
-        sum = 0.f;
+      for (int j = 0; j < K; ++j) xv[j] = fmaf(beta, __ldg(pin + c8[j]), __ldg(r + c8[j]));
+      sum = 0.f;
 #pragma unroll
-        for (int j = 0; j < K; ++j) {
-          const unsigned id =
-              (NIB == 4) ? (w0 >> (4 * j)) & 15u : ((j < 4 ? w0 : w1) >> (8 * (j & 3))) & 255u;
-          sum = fmaf(xv[j], tab[id], sum);
-        }
-      }
-      if (i < A.nrows) {
-        const float pi = fmaf(beta, pin[i], r[i]);
-        pout[i] = pi;
-        Ap[i] = sum;
-        acc[0] += (double)pi * (double)sum;
+      for (int j = 0; j < K; ++j) {
+        const unsigned id =
+            (NIB == 4) ? (w0 >> (4 * j)) & 15u : ((j < 4 ? w0 : w1) >> (8 * (j & 3))) & 255u;
+        sum = fmaf(xv[j], tab[id], sum);
       }
     }
-    __syncthreads();  // every warp is done with stage st
-    if (threadIdx.x == 0) {
-      const int nc = c + kStages * gridDim.x;
-      if (nc < nchunks) fill(nc, st);
+    __syncwarp();  // every lane is done with stage st
+    if (lane == 0) {
+      const int ns2 = s + kStages * nw;
+      if (ns2 < A.nslices) fill(ns2, st);
+    }
+    if (i < A.nrows) {
+      const float pi = fmaf(beta, pin[i], r[i]);
+      pout[i] = pi;
+      Ap[i] = sum;
+      acc[0] += (double)pi * (double)sum;
     }
   }
-  if (failed && threadIdx.x == 0) {
+  if (failed && lane == 0) {
     S->status = GIPB200_ERR_TIMEOUT;
     S->done = 1;
-    // wait (bounded) for the copies still in flight into this block's shared memory
+    // wait (bounded) for the copies still in flight into this warp's stages
     for (int k = 0; k < kStages; ++k) {
       const int j = it + k;
-      if (blockIdx.x + j * gridDim.x < nchunks)
-        tma::bar_wait(&s_bar[j % kStages], (unsigned)(j / kStages) & 1u);
+      if (gw + j * nw < A.nslices) tma::bar_wait(&bar[j % kStages], (unsigned)(j / kStages) & 1u);
     }
   }
   grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
@@ -1054,7 +1053,10 @@ int Pcg::build_compressed(cudaStream_t s) {
   GIPB_CUDA(cudaStreamSynchronize(s));
   cop.index_bits = nib;
   cop.slots = max_len <= 7 ? 7 : 8;
-  cop.tma = getenv("GIPB200_NO_TMA") == nullptr;
+  {
+    const char* e = getenv("GIPB200_TMA");  // "1": stage the stream, "0": read it directly
+    if (e) cop.tma = e[0] == '1';
+  }
   if (cop.tma) {
     // enough shared memory per SM for 8 resident blocks (the rest stays L1), and the
     // grid cap that keeps the kernel in one wave
@@ -1297,7 +1299,7 @@ static void launch_mx_spmv(const Pcg& P, const float* pin, float* pout, float* A
                            cudaStream_t s) {
   const CompressedOp& c = P.cop;
   const SellView<float> A = P.a32();
-  const int nb = c.tma ? std::min(P.blocks_spmv, c.max_blocks) : P.blocks_spmv;
+  const int nb = (c.enabled && c.tma) ? std::min(P.blocks_spmv, c.max_blocks) : P.blocks_spmv;
   const float* r = P.r32.p;
   if (!c.enabled)
     k_mx_spmv_dot<<<nb, 256, 0, s>>>(A, r, pin, pout, Ap, sc, P.rs, use_cond, h);

@@ -42,7 +42,7 @@ struct CompressedOp {
   bool enabled = false;
   int index_bits = 0;            // 4 or 8
   int slots = 8;                 // 7: no packed row uses the eighth slot
-  bool tma = true;               // stage the packed stream through shared memory
+  bool tma = false;              // stage the packed stream through shared memory
   int max_blocks = 0;            // resident blocks of the staged kernel (one wave)
   DevBuf<uint4> delta;           // per row (nslices * 32)
   DevBuf<unsigned> idx4;         // per row, 8 x 4 bits

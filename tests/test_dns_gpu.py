@@ -132,12 +132,14 @@ def test_compressed_fp32_operator_is_exact(gpu, monkeypatch):
     case, _ = cavity.generate(20, re=400.0, permute_seed=4)
     kw = dict(gamma=1.0 / 400, pcg_mode="mixed", maxit=5000, tol=1e-8, inner_tol=0.1,
               max_outer=200, reorder=True)
+    monkeypatch.setenv("GIPB200_TMA", "0")  # packed words read straight from global memory
     E = DnsEngine(case, **kw)
     info = E.info()
     assert info["compressed"] == 1 and info["value_table"] == 4 and info["pin_row"] >= 0
     assert info["compressed_fraction"] == 1.0
-    monkeypatch.setenv("GIPB200_NO_TMA", "1")
+    monkeypatch.setenv("GIPB200_TMA", "1")  # staged through shared memory by bulk copies
     T = DnsEngine(case, **kw)
+    monkeypatch.delenv("GIPB200_TMA")
     monkeypatch.setenv("GIPB200_NO_COMPRESS", "1")
     P = DnsEngine(case, **kw)
     assert P.info()["compressed"] == 0
