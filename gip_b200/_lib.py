@@ -34,7 +34,8 @@ class DnsOps(C.Structure):
 
 class PcgParams(C.Structure):
     _fields_ = [("mode", C.c_int), ("maxit", C.c_int), ("tol", C.c_double),
-                ("inner_tol", C.c_double), ("inner_maxit", C.c_int), ("max_outer", C.c_int)]
+                ("inner_tol", C.c_double), ("inner_maxit", C.c_int), ("max_outer", C.c_int),
+                ("precond", C.c_int)]
 
 
 class PcgResult(C.Structure):
@@ -49,13 +50,15 @@ class DnsParams(C.Structure):
 
 class PcgInfo(C.Structure):
     _fields_ = [("pin_row", C.c_int), ("compressed", C.c_int), ("value_table", C.c_int),
-                ("compressed_fraction", C.c_double)]
+                ("compressed_fraction", C.c_double), ("amg_levels", C.c_int),
+                ("amg_complexity", C.c_double), ("amg_setup_s", C.c_double)]
 
 
 class DnsInfo(C.Structure):
     _fields_ = [("reordered", C.c_int), ("pin_row", C.c_int), ("compressed", C.c_int),
                 ("value_table", C.c_int), ("compressed_fraction", C.c_double),
-                ("slots_L", C.c_longlong), ("nnz_L", C.c_longlong)]
+                ("slots_L", C.c_longlong), ("nnz_L", C.c_longlong), ("amg_levels", C.c_int),
+                ("amg_complexity", C.c_double), ("amg_setup_s", C.c_double)]
 
 
 class AdjointParams(C.Structure):

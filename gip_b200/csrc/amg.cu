@@ -1,0 +1,509 @@
+// Smoothed-aggregation AMG (setup on the host, FP32 V-cycle on the device).
+//
+// Setup per level (operator A, near-null vector z):
+//   strength   |a_ij| > theta sqrt(|a_ii a_jj|)
+//   aggregates greedy: (1) a node whose strong neighbours are all free starts an aggregate
+//              with them; (2) a free node joins the aggregate of its strongest aggregated
+//              neighbour; (3) what is left forms aggregates with its free neighbours
+//   P0         tentative prolongator: P0[i, agg(i)] = z_i / |z restricted to agg(i)|
+//   P          smoothed: (I - w D^-1 A) P0, w = 4 / (3 rho), rho = the Gershgorin bound of
+//              D^-1 A; coarse near-null vector = the aggregate norms (so P z_c = z)
+//   A_c        Galerkin: R A P with R = P^T
+// The coarsest level (<= kCoarse unknowns) is inverted densely; for the pinned-Neumann
+// inner system (A z = 0) the inverse is taken of A + sigma z z^T / |z|^2, which solves
+// consistent right-hand sides exactly.
+// V-cycle on level l (b -> x): x = D^-1 b (weighted Jacobi from zero), t = b - A x,
+// b_{l+1} = R t, recurse, x += P x_{l+1}, result x + D^-1 (b - A x): the same smoother
+// before and after, so the cycle is a symmetric operator.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+
+#include "amg.cuh"
+#include "device.cuh"
+#include "pcg.cuh"
+
+namespace gipb200 {
+
+namespace {
+
+constexpr int kCoarse = 1024;    // largest level inverted densely
+constexpr int kMaxLevels = 16;
+constexpr double kTheta = 0.08;  // strength threshold
+
+struct HCsr {
+  int nr = 0, nc = 0;
+  std::vector<int> rp, ci;
+  std::vector<double> v;
+  long long nnz() const { return (long long)ci.size(); }
+};
+
+std::vector<double> diagonal(const HCsr& A) {
+  std::vector<double> d((size_t)A.nr, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < A.nr; ++i)
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] == i) d[i] += A.v[k];
+  return d;
+}
+
+// Gershgorin bound of the spectral radius of D^-1 A.
+double rho_bound(const HCsr& A, const std::vector<double>& d) {
+  double rho = 0.0;
+#pragma omp parallel for schedule(static) reduction(max : rho)
+  for (int i = 0; i < A.nr; ++i) {
+    double s = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) s += std::fabs(A.v[k]);
+    if (d[i] > 0.0) rho = std::max(rho, s / d[i]);
+  }
+  return rho > 0.0 ? rho : 1.0;
+}
+
+int aggregate(const HCsr& A, const std::vector<double>& d, std::vector<int>& agg) {
+  const int n = A.nr;
+  auto strong = [&](int i, int k) {
+    const int j = A.ci[k];
+    return j != i && A.v[k] != 0.0 && std::fabs(A.v[k]) > kTheta * std::sqrt(std::fabs(d[i] * d[j]));
+  };
+  agg.assign((size_t)n, -1);
+  int na = 0;
+  for (int i = 0; i < n; ++i) {  // phase 1
+    if (agg[i] != -1) continue;
+    bool free = true, any = false;
+    for (int k = A.rp[i]; k < A.rp[i + 1] && free; ++k)
+      if (strong(i, k)) {
+        any = true;
+        if (agg[A.ci[k]] != -1) free = false;
+      }
+    if (!free || !any) continue;
+    agg[i] = na;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (strong(i, k)) agg[A.ci[k]] = na;
+    ++na;
+  }
+  const std::vector<int> first = agg;
+  for (int i = 0; i < n; ++i) {  // phase 2
+    if (first[i] != -1) continue;
+    int best = -1;
+    double bw = 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (strong(i, k) && first[A.ci[k]] >= 0 && std::fabs(A.v[k]) > bw) {
+        bw = std::fabs(A.v[k]);
+        best = first[A.ci[k]];
+      }
+    if (best >= 0) agg[i] = best;
+  }
+  for (int i = 0; i < n; ++i) {  // phase 3
+    if (agg[i] != -1) continue;
+    agg[i] = na;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (strong(i, k) && agg[A.ci[k]] == -1) agg[A.ci[k]] = na;
+    ++na;
+  }
+  return na;
+}
+
+// Row-wise product C = A B (Gustavson), rows in the order their columns first appear.
+HCsr spgemm(const HCsr& A, const HCsr& B) {
+  HCsr C;
+  C.nr = A.nr;
+  C.nc = B.nc;
+  C.rp.assign((size_t)A.nr + 1, 0);
+#pragma omp parallel
+  {
+    std::vector<int> mark((size_t)B.nc, -1);
+#pragma omp for schedule(dynamic, 1024)
+    for (int i = 0; i < A.nr; ++i) {
+      int c = 0;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        const int j = A.ci[k];
+        for (int q = B.rp[j]; q < B.rp[j + 1]; ++q)
+          if (mark[B.ci[q]] != i) {
+            mark[B.ci[q]] = i;
+            ++c;
+          }
+      }
+      C.rp[i + 1] = c;
+    }
+  }
+  for (int i = 0; i < A.nr; ++i) C.rp[i + 1] += C.rp[i];
+  C.ci.resize((size_t)C.rp[A.nr]);
+  C.v.resize((size_t)C.rp[A.nr]);
+#pragma omp parallel
+  {
+    std::vector<int> where((size_t)B.nc, -1);
+#pragma omp for schedule(dynamic, 1024)
+    for (int i = 0; i < A.nr; ++i) {
+      int o = C.rp[i];
+      const int o0 = o;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        const int j = A.ci[k];
+        const double a = A.v[k];
+        for (int q = B.rp[j]; q < B.rp[j + 1]; ++q) {
+          const int c = B.ci[q];
+          if (where[c] < o0) {
+            where[c] = o;
+            C.ci[o] = c;
+            C.v[o] = a * B.v[q];
+            ++o;
+          } else {
+            C.v[where[c]] += a * B.v[q];
+          }
+        }
+      }
+    }
+  }
+  return C;
+}
+
+HCsr transpose(const HCsr& A) {
+  HCsr T;
+  T.nr = A.nc;
+  T.nc = A.nr;
+  T.rp.assign((size_t)A.nc + 1, 0);
+  for (int c : A.ci) T.rp[c + 1]++;
+  for (int i = 0; i < A.nc; ++i) T.rp[i + 1] += T.rp[i];
+  T.ci.resize(A.ci.size());
+  T.v.resize(A.v.size());
+  std::vector<int> next(T.rp.begin(), T.rp.end() - 1);
+  for (int i = 0; i < A.nr; ++i)
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      const int o = next[A.ci[k]]++;
+      T.ci[o] = i;
+      T.v[o] = A.v[k];
+    }
+  return T;
+}
+
+// Smoothed prolongator (I - w D^-1 A) P0 with P0[i, agg(i)] = p0[i].
+HCsr smoothed_prolongator(const HCsr& A, const std::vector<double>& d, const std::vector<int>& agg,
+                          const std::vector<double>& p0, int na, double w) {
+  HCsr P;
+  P.nr = A.nr;
+  P.nc = na;
+  P.rp.assign((size_t)A.nr + 1, 0);
+  auto row = [&](int i, std::vector<std::pair<int, double>>& e) {
+    e.clear();
+    e.emplace_back(agg[i], p0[i]);
+    const double s = d[i] > 0.0 ? w / d[i] : 0.0;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      const int j = A.ci[k];
+      const double val = -s * A.v[k] * p0[j];
+      bool found = false;
+      for (auto& q : e)
+        if (q.first == agg[j]) {
+          q.second += val;
+          found = true;
+          break;
+        }
+      if (!found) e.emplace_back(agg[j], val);
+    }
+  };
+#pragma omp parallel
+  {
+    std::vector<std::pair<int, double>> e;
+#pragma omp for schedule(static)
+    for (int i = 0; i < A.nr; ++i) {
+      row(i, e);
+      P.rp[i + 1] = (int)e.size();
+    }
+  }
+  for (int i = 0; i < A.nr; ++i) P.rp[i + 1] += P.rp[i];
+  P.ci.resize((size_t)P.rp[A.nr]);
+  P.v.resize((size_t)P.rp[A.nr]);
+#pragma omp parallel
+  {
+    std::vector<std::pair<int, double>> e;
+#pragma omp for schedule(static)
+    for (int i = 0; i < A.nr; ++i) {
+      row(i, e);
+      int o = P.rp[i];
+      for (auto& q : e) {
+        P.ci[o] = q.first;
+        P.v[o] = q.second;
+        ++o;
+      }
+    }
+  }
+  return P;
+}
+
+// Dense inverse of the SPD matrix M (m x m, row-major) by Cholesky; false if not SPD.
+bool dense_inverse(int m, std::vector<double>& M, std::vector<double>& inv) {
+  std::vector<double> Lc((size_t)m * m, 0.0);
+  for (int j = 0; j < m; ++j) {
+    double s = M[(size_t)j * m + j];
+    for (int k = 0; k < j; ++k) s -= Lc[(size_t)j * m + k] * Lc[(size_t)j * m + k];
+    if (!(s > 0.0)) return false;
+    const double ljj = std::sqrt(s);
+    Lc[(size_t)j * m + j] = ljj;
+    for (int i = j + 1; i < m; ++i) {
+      double t = M[(size_t)i * m + j];
+      for (int k = 0; k < j; ++k) t -= Lc[(size_t)i * m + k] * Lc[(size_t)j * m + k];
+      Lc[(size_t)i * m + j] = t / ljj;
+    }
+  }
+  inv.assign((size_t)m * m, 0.0);
+  std::vector<double> y((size_t)m);
+  for (int c = 0; c < m; ++c) {  // column c of the inverse: L L^T x = e_c
+    for (int i = 0; i < m; ++i) {
+      double t = (i == c) ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) t -= Lc[(size_t)i * m + k] * y[k];
+      y[i] = t / Lc[(size_t)i * m + i];
+    }
+    for (int i = m - 1; i >= 0; --i) {
+      double t = y[i];
+      for (int k = i + 1; k < m; ++k) t -= Lc[(size_t)k * m + i] * inv[(size_t)k * m + c];
+      inv[(size_t)i * m + c] = t / Lc[(size_t)i * m + i];
+    }
+  }
+  return true;
+}
+
+int upload(const HCsr& A, Sell32* S, cudaStream_t s) {
+  GIPB_TRY(validate_csr(A.nr, A.nc, (int)A.nnz(), A.rp.data(), A.ci.data(), A.nc, "AMG operator"));
+  S->nrows = A.nr;
+  S->ncols = A.nc;
+  S->nnz = A.nnz();
+  S->nslices = (A.nr + 31) / 32;
+  std::vector<long long> sptr((size_t)S->nslices + 1, 0);
+  for (int sl = 0; sl < S->nslices; ++sl) {
+    int len = 0;
+    for (int r = sl * 32; r < std::min(A.nr, sl * 32 + 32); ++r) len = std::max(len, A.rp[r + 1] - A.rp[r]);
+    sptr[sl + 1] = sptr[sl] + 32LL * len;
+  }
+  S->nslots = sptr[S->nslices];
+  if (S->nslots > 0x7fffffffLL) return fail(GIPB200_ERR_ARG, "AMG operator too large");
+  std::vector<int> col((size_t)std::max<long long>(S->nslots, 1), -1);
+  std::vector<float> val((size_t)std::max<long long>(S->nslots, 1), 0.0f);
+#pragma omp parallel for schedule(static)
+  for (int r = 0; r < A.nr; ++r) {
+    const int sl = r >> 5, lane = r & 31;
+    for (int k = A.rp[r]; k < A.rp[r + 1]; ++k) {
+      const long long slot = sptr[sl] + 32LL * (k - A.rp[r]) + lane;
+      col[slot] = A.ci[k];
+      val[slot] = (float)A.v[k];
+    }
+  }
+  GIPB_TRY(S->sptr.upload(sptr.data(), sptr.size(), s));
+  GIPB_TRY(S->col.upload(col.data(), col.size(), s));
+  GIPB_TRY(S->val.upload(val.data(), val.size(), s));
+  GIPB_CUDA(cudaStreamSynchronize(s));  // host staging goes out of scope
+  return GIPB200_OK;
+}
+
+// ------------------------------------------------------------------ V-cycle kernels
+// All of them count their launch and return at once when the solve has finished.
+__device__ __forceinline__ bool amg_enter(PcgScalars* S) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&S->kernels, 1);
+  return S->done != 0;
+}
+
+// x = dinv b
+__global__ void __launch_bounds__(256) k_amg_jacobi0(int n, const float* __restrict__ dinv,
+                                                     const float* __restrict__ b,
+                                                     float* __restrict__ x, PcgScalars* S) {
+  if (amg_enter(S)) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = dinv[i] * b[i];
+}
+
+enum { kResid = 0, kPlain = 1, kAdd = 2, kSmooth = 3 };
+// kResid: y = b - A x;  kPlain: y = A x;  kAdd: y += A x;  kSmooth: y = x + dinv (b - A x)
+template <int MODE>
+__global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<float> A, const float* __restrict__ x,
+                                                     const float* __restrict__ b,
+                                                     const float* __restrict__ dinv,
+                                                     float* __restrict__ y, PcgScalars* S) {
+  if (amg_enter(S)) return;
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int s = gw; s < A.nslices; s += nw) {
+    const float sum = sell_row_f32<4>(A, x, s, lane);
+    const int i = s * 32 + lane;
+    if (i < A.nrows) {
+      if (MODE == kResid) y[i] = b[i] - sum;
+      else if (MODE == kPlain) y[i] = sum;
+      else if (MODE == kAdd) y[i] += sum;
+      else y[i] = fmaf(dinv[i], b[i] - sum, x[i]);
+    }
+  }
+}
+
+struct CycleFinish {
+  PcgScalars* S;
+  __device__ void operator()(const double* t) const {
+    const double rz = t[0];
+    if (!(rz > 0.0) || !isfinite(rz)) {  // preconditioner lost definiteness: restart CG
+      S->beta = 0.0;
+      S->rz = 0.0;
+      return;
+    }
+    S->beta = (S->rz > 0.0) ? rz / S->rz : 0.0;
+    S->rz = rz;
+  }
+};
+
+// Level 0 post-smoothing with the dot: z = x + dinv (r - A x), r.z, beta.
+__global__ void __launch_bounds__(256, 8) k_amg_smooth_dot(SellView<float> A, const float* __restrict__ x,
+                                                           const float* __restrict__ r,
+                                                           const float* __restrict__ dinv,
+                                                           float* __restrict__ z, PcgScalars* S,
+                                                           ReduceScratch rs) {
+  if (amg_enter(S)) return;
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  double acc[1] = {0.0};
+  for (int s = gw; s < A.nslices; s += nw) {
+    const float sum = sell_row_f32<4>(A, x, s, lane);
+    const int i = s * 32 + lane;
+    if (i < A.nrows) {
+      const float ri = r[i];
+      const float zi = fmaf(dinv[i], ri - sum, x[i]);
+      z[i] = zi;
+      acc[0] += (double)ri * (double)zi;
+    }
+  }
+  grid_reduce<SumOp, 1>(acc, rs, CycleFinish{S});
+}
+
+// Coarsest level: x = C b, one warp per row of the dense inverse.
+__global__ void __launch_bounds__(256) k_amg_dense(int m, const float* __restrict__ C,
+                                                   const float* __restrict__ b,
+                                                   float* __restrict__ x, PcgScalars* S) {
+  if (amg_enter(S)) return;
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = gw; i < m; i += nw) {
+    float acc = 0.f;
+    for (int j = lane; j < m; j += 32) acc = fmaf(C[(size_t)i * m + j], b[j], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) x[i] = acc;
+  }
+}
+
+int vec_blocks(int n) {
+  int b = 1;
+  grid_blocks(256, std::max(n, 1), 1, kMaxReduceBlocks, &b);
+  return b;
+}
+
+}  // namespace
+
+int Amg::build(int n, const int* rp, const int* ci, const double* v, const double* z0,
+               bool singular, cudaStream_t s) {
+  const auto t0 = std::chrono::steady_clock::now();
+  HCsr A;
+  A.nr = A.nc = n;
+  A.rp.assign(rp, rp + n + 1);
+  A.ci.assign(ci, ci + rp[n]);
+  A.v.assign(v, v + rp[n]);
+  std::vector<double> z(z0, z0 + n);
+  lv.clear();
+  const double nnz0 = (double)A.nnz();
+  double nnz_all = 0.0;
+  for (int l = 0; l < kMaxLevels; ++l) {
+    std::unique_ptr<AmgLevel> Lp(new AmgLevel());
+    AmgLevel& L = *Lp;
+    L.n = A.nr;
+    const std::vector<double> d = diagonal(A);
+    for (int i = 0; i < A.nr; ++i)
+      if (!(d[i] > 0.0)) return fail(GIPB200_ERR_ARG, "AMG: level %d row %d has no positive diagonal", l, i);
+    const double rho = rho_bound(A, d);
+    const double w = 4.0 / (3.0 * rho);
+    std::vector<float> dinv((size_t)A.nr);
+    for (int i = 0; i < A.nr; ++i) dinv[i] = (float)(w / d[i]);
+    GIPB_TRY(L.dinv.upload(dinv.data(), dinv.size(), s));
+    GIPB_TRY(L.x.alloc((size_t)A.nr));
+    GIPB_TRY(L.t.alloc((size_t)A.nr));
+    if (l > 0) {
+      GIPB_TRY(L.b.alloc((size_t)A.nr));
+      GIPB_TRY(upload(A, &L.A, s));
+    }
+    nnz_all += (double)A.nnz();
+    if (A.nr <= kCoarse && l > 0) {  // coarsest: dense inverse
+      const int m = A.nr;
+      std::vector<double> M((size_t)m * m, 0.0);
+      for (int i = 0; i < m; ++i)
+        for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) M[(size_t)i * m + A.ci[k]] += A.v[k];
+      if (singular) {
+        double zz = 0.0, dm = 0.0;
+        for (int i = 0; i < m; ++i) zz += z[i] * z[i], dm += d[i];
+        const double sigma = dm / m;
+        for (int i = 0; i < m; ++i)
+          for (int j = 0; j < m; ++j) M[(size_t)i * m + j] += sigma * z[i] * z[j] / zz;
+      }
+      std::vector<double> inv;
+      if (!dense_inverse(m, M, inv))
+        return fail(GIPB200_ERR_ARG, "AMG: coarsest operator (%d) is not positive definite", m);
+      std::vector<float> cf(inv.begin(), inv.end());
+      GIPB_TRY(cinv.upload(cf.data(), cf.size(), s));
+      nc = m;
+      lv.push_back(std::move(Lp));
+      break;
+    }
+    std::vector<int> agg;
+    const int na = aggregate(A, d, agg);
+    if (na >= A.nr || na == 0) return fail(GIPB200_ERR_ARG, "AMG: level %d does not coarsen", l);
+    std::vector<double> nrm((size_t)na, 0.0);
+    for (int i = 0; i < A.nr; ++i) nrm[agg[i]] += z[i] * z[i];
+    for (auto& q : nrm) q = std::sqrt(q);
+    std::vector<double> p0((size_t)A.nr);
+    for (int i = 0; i < A.nr; ++i) p0[i] = nrm[agg[i]] > 0.0 ? z[i] / nrm[agg[i]] : 0.0;
+    HCsr P = smoothed_prolongator(A, d, agg, p0, na, w);
+    HCsr R = transpose(P);
+    HCsr Ac = spgemm(R, spgemm(A, P));
+    GIPB_TRY(upload(P, &L.P, s));
+    GIPB_TRY(upload(R, &L.R, s));
+    lv.push_back(std::move(Lp));
+    A = std::move(Ac);
+    z = nrm;
+  }
+  if (nc == 0) return fail(GIPB200_ERR_ARG, "AMG: more than %d levels", kMaxLevels);
+  op_complexity = nnz_all / std::max(nnz0, 1.0);
+  kernels_per_cycle = 5LL * ((long long)lv.size() - 1) + 1;
+  GIPB_TRY(grid_blocks(256, n, 1, kMaxReduceBlocks, &blocks));
+  GIPB_CUDA(cudaStreamSynchronize(s));
+  setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return GIPB200_OK;
+}
+
+int Amg::enqueue(SellView<float> A0, const float* r, float* z0, PcgScalars* S, ReduceScratch rs,
+                 cudaStream_t s) const {
+  const int L = (int)lv.size();
+  // downward: pre-smooth from zero, residual, restriction
+  for (int l = 0; l < L - 1; ++l) {
+    const AmgLevel& V = *lv[l];
+    const SellView<float> A = l == 0 ? A0 : V.A.view();
+    const float* b = l == 0 ? r : V.b.p;
+    const int bn = vec_blocks(V.n), bs = vec_blocks(A.nslices * 32);
+    k_amg_jacobi0<<<bn, 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
+    k_amg_spmv<kResid><<<bs, 256, 0, s>>>(A, V.x.p, b, nullptr, V.t.p, S);
+    const SellView<float> R = V.R.view();
+    k_amg_spmv<kPlain><<<vec_blocks(R.nslices * 32), 256, 0, s>>>(R, V.t.p, nullptr, nullptr,
+                                                                  lv[l + 1]->b.p, S);
+  }
+  const AmgLevel& C = *lv[L - 1];
+  k_amg_dense<<<std::min(kMaxReduceBlocks, (nc + 7) / 8), 256, 0, s>>>(nc, cinv.p, C.b.p, C.x.p, S);
+  // upward: prolongation, post-smoothing (level 0 also reduces r.z)
+  for (int l = L - 2; l >= 0; --l) {
+    const AmgLevel& V = *lv[l];
+    const float* xc = (l + 1 == L - 1) ? lv[l + 1]->x.p : lv[l + 1]->t.p;
+    const SellView<float> P = V.P.view();
+    k_amg_spmv<kAdd><<<vec_blocks(P.nslices * 32), 256, 0, s>>>(P, xc, nullptr, nullptr, V.x.p, S);
+    const SellView<float> A = l == 0 ? A0 : V.A.view();
+    const int bs = vec_blocks(A.nslices * 32);
+    if (l == 0)
+      k_amg_smooth_dot<<<bs, 256, 0, s>>>(A, V.x.p, r, V.dinv.p, z0, S, rs);
+    else
+      k_amg_spmv<kSmooth><<<bs, 256, 0, s>>>(A, V.x.p, V.b.p, V.dinv.p, V.t.p, S);
+  }
+  GIPB_LAUNCH_CHECK();
+  return GIPB200_OK;
+}
+
+}  // namespace gipb200

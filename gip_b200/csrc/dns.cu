@@ -888,6 +888,10 @@ int gipb200_dns_get_info(gipb200_dns Dh, gipb200_dns_info* info) {
   info->compressed_fraction = E.pcg.cop.compressed_fraction;
   info->slots_L = E.L.nslots;
   info->nnz_L = E.L.nnz;
+  const Amg* amg = E.pcg.amg.get();
+  info->amg_levels = amg ? (int)amg->lv.size() : 0;
+  info->amg_complexity = amg ? amg->op_complexity : 0.0;
+  info->amg_setup_s = amg ? amg->setup_s : 0.0;
   return GIPB200_OK;
 }
 

@@ -271,6 +271,7 @@ struct ResidualFinish {
   float* p32;
   int use_cond;
   cudaGraphConditionalHandle loop_cond;
+  int amg;  // beta and r.z come from the preconditioner's last kernel instead
   __device__ void operator()(const double* t) const {
     // t[0] = r.r (FP64 true residual), t[1] = r^.r^ before the pin projection,
     // t[2] = b.b, t[3] = sum(r)
@@ -287,10 +288,10 @@ struct ResidualFinish {
       S->kappa_c = t[3] / pin_val;
     }
     if (!first) {
-      S->beta = rz / S->rz;  // continue the direction with the replaced residual
+      if (!amg) S->beta = rz / S->rz;  // continue the direction with the replaced residual
       S->outer += 1;
     }
-    S->rz = rz;
+    if (!amg) S->rz = rz;
     S->maxr2 = rz;
     // FP32 level at which the predicted true residual reaches tol*||b|| / 2
     const double goal = 0.5 * tol * sqrt(S->bb);
@@ -317,7 +318,7 @@ __global__ void __launch_bounds__(256) k_mx_residual(SellView<double> L, const d
                                                      ReduceScratch rs, int first, double tol,
                                                      double delta, int maxit, int max_updates,
                                                      int pin_row, double pin_val, int use_cond,
-                                                     cudaGraphConditionalHandle loop_cond) {
+                                                     cudaGraphConditionalHandle loop_cond, int amg) {
   mx_enter(S, 0, 0);
   if (!first && (!S->upd || S->done)) return;
   const int lane = threadIdx.x & 31;
@@ -346,7 +347,7 @@ __global__ void __launch_bounds__(256) k_mx_residual(SellView<double> L, const d
   }
   grid_reduce<SumOp, 4>(acc, rs,
                         ResidualFinish{S, first, tol, delta, maxit, max_updates, pin_row, pin_val,
-                                       scale, r32, p32, use_cond, loop_cond});
+                                       scale, r32, p32, use_cond, loop_cond, amg});
 }
 
 struct AlphaFinish32 {
@@ -685,6 +686,7 @@ struct BetaFinish32 {
   const float* y32;
   int use_cond;
   cudaGraphConditionalHandle upd_cond;
+  int amg;  // beta and r.z come from the preconditioner's last kernel instead
   __device__ void operator()(const double* t) const {
     S->iter += 1;
     S->total_inner += 1;
@@ -695,7 +697,7 @@ struct BetaFinish32 {
     if (upd) {
       S->upd = 1;
       S->kappa = (pin_row >= 0) ? S->kappa_c - scale[pin_row] * (double)__ldcg(y32 + pin_row) : 0.0;
-    } else {
+    } else if (!amg) {
       S->beta = rz_new / S->rz;
       S->rz = rz_new;
     }
@@ -715,7 +717,8 @@ __global__ void __launch_bounds__(256) k_mx_update(int n, float* __restrict__ y,
                                                    const float* __restrict__ Ap, PcgScalars* S,
                                                    ReduceScratch rs, double delta, int maxit,
                                                    int pin_row, const double* __restrict__ scale,
-                                                   int use_cond, cudaGraphConditionalHandle upd_cond) {
+                                                   int use_cond, cudaGraphConditionalHandle upd_cond,
+                                                   int amg) {
   mx_enter(S, 0, 0);
   if (S->done) return;
   const float alpha = (float)S->alpha;
@@ -749,7 +752,8 @@ __global__ void __launch_bounds__(256) k_mx_update(int n, float* __restrict__ y,
     r[i] = ri;
     acc[0] += (double)ri * (double)ri;
   }
-  grid_reduce<SumOp, 1>(acc, rs, BetaFinish32{S, delta, maxit, pin_row, scale, y, use_cond, upd_cond});
+  grid_reduce<SumOp, 1>(acc, rs,
+                        BetaFinish32{S, delta, maxit, pin_row, scale, y, use_cond, upd_cond, amg});
 }
 
 // x += S y + kappa (FP64); y = 0   -- only when a replacement is due
@@ -836,6 +840,10 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
   n_all = nall;
   prm = params;
   if (prm.mode != GIPB200_PCG_FIXED && !(prm.tol > 0)) return fail(GIPB200_ERR_ARG, "tol must be > 0");
+  if (prm.precond != GIPB200_PRECOND_JACOBI && prm.precond != GIPB200_PRECOND_AMG)
+    return fail(GIPB200_ERR_ARG, "unknown preconditioner %d", prm.precond);
+  if (prm.precond == GIPB200_PRECOND_AMG && prm.mode != GIPB200_PCG_MIXED)
+    return fail(GIPB200_ERR_ARG, "the AMG preconditioner is available in the mixed form only");
   if (prm.mode == GIPB200_PCG_MIXED) {
     if (!(prm.inner_tol > 0 && prm.inner_tol < 1))
       return fail(GIPB200_ERR_ARG, "inner_tol (replacement factor) must be in (0,1)");
@@ -892,6 +900,7 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
       GIPB_LAUNCH_CHECK();
       GIPB_TRY(sort_fp32_rows(s));
       if (prm.mode == GIPB200_PCG_MIXED && !getenv("GIPB200_NO_COMPRESS")) GIPB_TRY(build_compressed(s));
+      if (prm.precond == GIPB200_PRECOND_AMG) GIPB_TRY(build_amg(s));
     }
   } else {
     GIPB_TRY(dinv.alloc(n));
@@ -917,6 +926,38 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
 // free; L itself keeps GIP's order) and drops the zero-valued ghost columns to padding.
 // Sorted rows give every slot of a slice one neighbour direction, which keeps the column
 // spread per slot small for the packed layout.
+// AMG hierarchy of the inner system: the Jacobi-scaled operator S L S with the pin
+// removed (the pure-Neumann part when L has the pinned structure), columns < n.  Its
+// near-null vector is S^-1 1 (L_N 1 = 0).
+int Pcg::build_amg(cudaStream_t s) {
+  std::vector<double> hval((size_t)std::max(L->nnz, 1)), hs((size_t)std::max(n, 1));
+  GIPB_CUDA(cudaMemcpyAsync(hval.data(), L->csr_val.p, (size_t)L->nnz * 8, cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaMemcpyAsync(hs.data(), scale.p, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> rp((size_t)n + 1, 0), ci;
+  std::vector<double> v;
+  ci.reserve((size_t)L->nnz);
+  v.reserve((size_t)L->nnz);
+  for (int i = 0; i < n; ++i) {
+    for (int k = L->h_rowptr[i]; k < L->h_rowptr[i + 1]; ++k) {
+      const int j = L->h_col[k];
+      if (j >= n) continue;
+      double a = hval[k];
+      if (i == pin_row && j == pin_row) a -= pin_val;
+      ci.push_back(j);
+      v.push_back(hs[i] * a * hs[j]);
+    }
+    rp[i + 1] = (int)ci.size();
+  }
+  std::vector<double> z((size_t)n);
+  for (int i = 0; i < n; ++i) z[i] = hs[i] > 0.0 ? 1.0 / hs[i] : 0.0;
+  amg.reset(new Amg());
+  GIPB_TRY(amg->build(n, rp.data(), ci.data(), v.data(), z.data(), pin_row >= 0, s));
+  GIPB_TRY(z32.alloc((size_t)n_all));
+  GIPB_TRY(z32.zero(s));
+  return GIPB200_OK;
+}
+
 int Pcg::sort_fp32_rows(cudaStream_t s) {
   const int ns = L->nslices;
   const long long nslots = L->nslots;
@@ -1227,6 +1268,7 @@ int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaS
   if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 1, hl));
+  if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, s));
   cudaGraph_t loop_body;
   GIPB_TRY(add_while(s, hl, &loop_body));
   cudaStream_t os = body_stream[0], is = body_stream[1];
@@ -1243,7 +1285,8 @@ int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaS
       GIPB_TRY(make_handle(os, 0, 0, &hu));
       launch_mx_spmv(*this, pin, pout, Ap32.p, sc.p, 1, hl, os);
       k_mx_update<<<blocks_vec, 256, 0, os>>>(n, y32.p, r32.p, pout, Ap32.p, sc.p, rs,
-                                               prm.inner_tol, prm.maxit, pin_row, scale.p, 1, hu);
+                                               prm.inner_tol, prm.maxit, pin_row, scale.p, 1, hu,
+                                               amg ? 1 : 0);
       GIPB_LAUNCH_CHECK();
       cudaGraph_t if_body;
       GIPB_TRY(add_if(os, hu, &if_body));
@@ -1257,6 +1300,7 @@ int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaS
       if (rst != GIPB200_OK) return rst;
       if (le != cudaSuccess)
         return fail(GIPB200_ERR_CUDA, "launch in replacement body: %s", cudaGetErrorString(le));
+      if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, os));
     }
     return GIPB200_OK;
   }();
@@ -1300,7 +1344,7 @@ static void launch_mx_spmv(const Pcg& P, const float* pin, float* pout, float* A
   const CompressedOp& c = P.cop;
   const SellView<float> A = P.a32();
   const int nb = (c.enabled && c.tma) ? std::min(P.blocks_spmv, c.max_blocks) : P.blocks_spmv;
-  const float* r = P.r32.p;
+  const float* r = P.amg ? P.z32.p : P.r32.p;  // direction from the preconditioned residual
   if (!c.enabled)
     k_mx_spmv_dot<<<nb, 256, 0, s>>>(A, r, pin, pout, Ap, sc, P.rs, use_cond, h);
   else if (c.tma && c.index_bits == 4 && c.slots == 7)
@@ -1333,7 +1377,8 @@ int Pcg::launch_mixed_residual(const double* b, const double* x, int first, cuda
                                int use_cond, cudaGraphConditionalHandle h) {
   k_mx_residual<<<blocks_spmv, 256, 0, s>>>(L->view(), x, b, scale.p, r32.p, p32.p, y32.p, sc.p,
                                              rs, first, prm.tol, prm.inner_tol, prm.maxit,
-                                             prm.max_outer, pin_row, pin_val, use_cond, h);
+                                             prm.max_outer, pin_row, pin_val, use_cond, h,
+                                             amg ? 1 : 0);
   GIPB_LAUNCH_CHECK();
   launches += 1;
   return GIPB200_OK;
@@ -1344,16 +1389,18 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
   if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 0, 0));
+  if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, s));
   const int poll = 16;
   for (int k = 0; k < prm.maxit; ++k) {
     float* pin = (k & 1) ? p32b.p : p32.p;
     float* pout = (k & 1) ? p32.p : p32b.p;
     launch_mx_spmv(*this, pin, pout, Ap32.p, sc.p, 0, 0, s);
     k_mx_update<<<blocks_vec, 256, 0, s>>>(n, y32.p, r32.p, pout, Ap32.p, sc.p, rs, prm.inner_tol,
-                                            prm.maxit, pin_row, scale.p, 0, 0);
+                                            prm.maxit, pin_row, scale.p, 0, 0, amg ? 1 : 0);
     k_mx_apply<<<blocks_vec, 256, 0, s>>>(n, x, y32.p, scale.p, sc.p);
     GIPB_LAUNCH_CHECK();
     GIPB_TRY(launch_mixed_residual(b, x, 0, s, 0, 0));
+    if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, s));
     launches += 4;
     if (host_sync && (k + 1) % poll == 0) {
       int d;
@@ -1468,6 +1515,10 @@ int gipb200_pcg_get_info(gipb200_pcg S, gipb200_pcg_info* info) {
   info->compressed = S->P.cop.enabled;
   info->value_table = S->P.cop.index_bits;
   info->compressed_fraction = S->P.cop.compressed_fraction;
+  const Amg* amg = S->P.amg.get();
+  info->amg_levels = amg ? (int)amg->lv.size() : 0;
+  info->amg_complexity = amg ? amg->op_complexity : 0.0;
+  info->amg_setup_s = amg ? amg->setup_s : 0.0;
   return GIPB200_OK;
 }
 

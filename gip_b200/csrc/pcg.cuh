@@ -1,6 +1,9 @@
 // Device-resident Jacobi-PCG shared by the PCG handle and the timestep engine.
 #pragma once
 
+#include <memory>
+
+#include "amg.cuh"
 #include "internal.cuh"
 
 namespace gipb200 {
@@ -68,6 +71,10 @@ struct Pcg {
   DevBuf<float> p32, Ap32, r32, y32;
   DevBuf<float> p32b;        // second direction buffer: each SpMV reads one, writes the other
   CompressedOp cop;
+  // AMG preconditioner of the FP32 inner CG (MIXED with GIPB200_PRECOND_AMG)
+  std::unique_ptr<Amg> amg;
+  DevBuf<float> z32;         // preconditioned residual
+  int build_amg(cudaStream_t s);
   int sort_fp32_rows(cudaStream_t s);
   void launch_pcg_update(double* x, cudaStream_t s);
   int build_compressed(cudaStream_t s);

@@ -156,11 +156,16 @@ class DeviceMatrix:
 
 
 MODES = {"fixed": L.PCG_FIXED, "tol": L.PCG_TOL, "mixed": L.PCG_MIXED}
+PRECONDS = {"jacobi": 0, "amg": 1}
 
 
 def pcg_params(mode: str = "fixed", maxit: int = 100, tol: float = 1e-6,
-               inner_tol: float = 1e-3, inner_maxit: int = 2000, max_outer: int = 30) -> L.PcgParams:
-    return L.PcgParams(MODES[mode], maxit, tol, inner_tol, inner_maxit, max_outer)
+               inner_tol: float = 1e-3, inner_maxit: int = 2000, max_outer: int = 30,
+               precond: str = "jacobi") -> L.PcgParams:
+    """precond: "jacobi" (GIP's) or "amg" (mixed mode only: an FP32 smoothed-aggregation
+    V-cycle, hierarchy built on the host at create time)."""
+    return L.PcgParams(MODES[mode], maxit, tol, inner_tol, inner_maxit, max_outer,
+                       PRECONDS[precond])
 
 
 class PcgSolver:
@@ -220,7 +225,8 @@ class DnsEngine:
     def __init__(self, case: Optional[GipCase], rho: float = 1.0, gamma: float = 1e-3,
                  pcg_mode: str = "fixed", maxit: int = 100, tol: float = 1e-6,
                  inner_tol: float = 1e-3, inner_maxit: int = 2000, max_outer: int = 30,
-                 use_graph: bool = True, reorder: bool = False, _handle=None, _sizes=None):
+                 use_graph: bool = True, reorder: bool = False, precond: str = "jacobi",
+                 _handle=None, _sizes=None):
         self._owned = _handle is None
         if _handle is not None:  # a view of an engine owned elsewhere (a batch instance)
             self.handle = _handle
@@ -232,8 +238,8 @@ class DnsEngine:
                        n_inner=case.n_inner, n_owned=case.n_owned, n_faces=case.n_faces)
         f = {k: np.ascontiguousarray(case.fields[k], np.float64) for k in ("u", "v", "w", "dxs")}
         self.params = L.DnsParams(rho, gamma, pcg_params(pcg_mode, maxit, tol, inner_tol,
-                                                         inner_maxit, max_outer), int(use_graph),
-                                  int(reorder))
+                                                         inner_maxit, max_outer, precond),
+                                  int(use_graph), int(reorder))
         handle = C.c_void_p()
         L.check(lib.gipb200_dns_create(C.byref(ops), _hptr(f["u"]), _hptr(f["v"]), _hptr(f["w"]),
                                        _hptr(f["dxs"]), C.byref(self.params), C.byref(handle)),
@@ -321,9 +327,10 @@ class DnsEngine:
 
 def dns_params(rho: float = 1.0, gamma: float = 1e-3, pcg_mode: str = "fixed", maxit: int = 100,
                tol: float = 1e-6, inner_tol: float = 1e-3, inner_maxit: int = 2000,
-               max_outer: int = 30, use_graph: bool = True, reorder: bool = False) -> L.DnsParams:
+               max_outer: int = 30, use_graph: bool = True, reorder: bool = False,
+               precond: str = "jacobi") -> L.DnsParams:
     return L.DnsParams(rho, gamma, pcg_params(pcg_mode, maxit, tol, inner_tol, inner_maxit,
-                                              max_outer), int(use_graph), int(reorder))
+                                              max_outer, precond), int(use_graph), int(reorder))
 
 
 class DnsBatch:

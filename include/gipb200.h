@@ -127,7 +127,13 @@ typedef struct {
                         FP32 residual has fallen by this factor (reliable update)   */
   int inner_maxit;   /* MIXED: unused (kept for layout)                              */
   int max_outer;     /* MIXED: cap on residual replacements                          */
+  int precond;       /* GIPB200_PRECOND_*: GIP's Jacobi (0); MIXED may take AMG (1)  */
 } gipb200_pcg_params;
+
+/* Preconditioners.  JACOBI is GIP's (GIP_LinearSolver.h:70-80).  AMG (no counterpart in
+ * the reference; MIXED only): a smoothed-aggregation multigrid V-cycle in FP32, its
+ * hierarchy built on the host once at create time from the Jacobi-scaled operator. */
+enum { GIPB200_PRECOND_JACOBI = 0, GIPB200_PRECOND_AMG = 1 };
 
 typedef struct {
   int iterations;        /* FIXED/TOL: PCG iterations; MIXED: inner iterations summed */
@@ -157,6 +163,9 @@ typedef struct {
   int compressed;              /* MIXED: FP32 operator packed (see value_table)           */
   int value_table;             /* MIXED: bits of a packed row's value-table index (4, 8)  */
   double compressed_fraction;  /* MIXED: share of the operator's slots in packed slices   */
+  int amg_levels;              /* AMG: levels of the hierarchy (0: no AMG)                */
+  double amg_complexity;       /* AMG: operator nonzeros of all levels / of the finest     */
+  double amg_setup_s;          /* AMG: host setup time                                    */
 } gipb200_pcg_info;
 int gipb200_pcg_get_info(gipb200_pcg S, gipb200_pcg_info* info);
 /* No counterpart in the reference: times `reps` launches of the solver's SpMV-dot kernel
@@ -251,6 +260,9 @@ typedef struct {
   double compressed_fraction;  /* MIXED: share of L's slots in packed slices             */
   long long slots_L;           /* sliced slots of L (stored nonzeros plus padding)       */
   long long nnz_L;
+  int amg_levels;              /* AMG: levels of the hierarchy (0: no AMG)               */
+  double amg_complexity;       /* AMG: operator nonzeros of all levels / of the finest    */
+  double amg_setup_s;          /* AMG: host setup time                                   */
 } gipb200_dns_info;
 int gipb200_dns_get_info(gipb200_dns E, gipb200_dns_info* info);
 

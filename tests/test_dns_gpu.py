@@ -169,3 +169,20 @@ def test_snapshot_restore_replays_exactly(gpu, mode):
     assert len(h2["time"]) == 5 and np.array_equal(h1["massr"], h2["massr"])
     for k, v in first.items():
         assert np.array_equal(E.field(k), v), k
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_engine_mixed_amg_close_to_fp64(gpu, oracle_mod, graph):
+    from gip_b200.device import DnsEngine
+    case, _ = cavity.generate(16, re=400.0, permute_seed=7)
+    E = DnsEngine(case, gamma=1.0 / 400, pcg_mode="mixed", maxit=3000, tol=1e-8,
+                  inner_tol=1e-3, max_outer=100, use_graph=graph, reorder=True, precond="amg")
+    assert E.info()["amg_levels"] >= 2
+    E.advance(5)
+    d = oracle_mod.OracleDNS(case, gamma=1.0 / 400, cg_maxit=3000, cg_mode=1, cg_tol=1e-10)
+    hr = d.run(5)
+    h = E.history()
+    assert np.all(h["massr"] < 1e-6)
+    assert np.all(h["iters"] * 4 < hr["iters"]), (h["iters"], hr["iters"])
+    for k in ("u", "v", "w"):
+        assert rel_err(E.field(k), d.vec[k]) < 1e-6, k

@@ -167,3 +167,35 @@ def test_bounded_wait_gives_up_with_status(gpu):
     L, b = cavity.poisson_problem(6, seed=1)
     S = dv.PcgSolver(dv.DeviceMatrix(L), mode="tol", maxit=500, tol=1e-8)
     assert S.solve(_t(b), _t(np.zeros(L.nrows)), _t(np.zeros(L.nrows)))["status"] == 0
+
+
+@pytest.mark.parametrize("n,tol", [(20, 1e-8), (33, 1e-6)])
+def test_mixed_amg_preconditioner(gpu, oracle_mod, n, tol):
+    # the AMG V-cycle (FP32) inside the mixed form: the FP64 true residual meets the
+    # tolerance in a few dozen iterations where Jacobi-scaled CG needs hundreds, and the
+    # solution agrees with the FP64 oracle solved tighter
+    from gip_b200 import device as dv
+    L, b = cavity.poisson_problem(n, seed=4)
+    A = dv.DeviceMatrix(L)
+    S = dv.PcgSolver(A, mode="mixed", maxit=2000, tol=tol, inner_tol=1e-3, max_outer=100,
+                     precond="amg")
+    info = S.info()
+    assert info["amg_levels"] >= 2 and info["pin_row"] >= 0
+    x = _t(np.zeros(L.nrows))
+    res = S.solve(_t(b), x, _t(np.zeros(L.nrows)))
+    J = dv.PcgSolver(A, mode="mixed", maxit=20000, tol=tol, inner_tol=0.3, max_outer=400)
+    rj = J.solve(_t(b), _t(np.zeros(L.nrows)), _t(np.zeros(L.nrows)))
+    assert res["status"] == 0, res
+    assert res["iterations"] < 60 and res["iterations"] * 5 < rj["iterations"], (res, rj)
+    xs = x.cpu().numpy()
+    assert np.linalg.norm(b - L.to_scipy() @ xs) <= tol * np.linalg.norm(b) * 1.0001
+    xr, _, _ = oracle_mod.pcg(L, b, np.zeros(L.nrows), maxit=20000, mode=1, tol=1e-13)
+    assert np.abs(xs - xr).max() / np.abs(xr).max() < 1e4 * tol
+
+
+def test_amg_only_in_mixed_form(gpu):
+    from gip_b200 import _lib
+    from gip_b200 import device as dv
+    L, _ = cavity.poisson_problem(6, seed=1)
+    with pytest.raises(_lib.GipB200Error):
+        dv.PcgSolver(dv.DeviceMatrix(L), mode="tol", maxit=10, tol=1e-6, precond="amg")
