@@ -63,6 +63,7 @@ inline void GIP_DNS<GIP_MatrixB200, GIP_VectorB200, GIP_ArchB200, GIP_NonLinearB
   prm.pcg.inner_tol = 0.0;
   prm.pcg.inner_maxit = 0;
   prm.pcg.max_outer = 0;
+  prm.pcg.precond = GIPB200_PRECOND_JACOBI;
   prm.use_graph = 1;
   prm.reorder = 1;
   gipb200_dns E = 0;

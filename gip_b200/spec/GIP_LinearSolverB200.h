@@ -25,6 +25,7 @@ inline void GIP_LinearSolver<GIP_MatrixB200, GIP_VectorB200>::solve(GIP_VectorB2
     p.inner_tol = 0.0;
     p.inner_maxit = 0;
     p.max_outer = 0;
+    p.precond = GIPB200_PRECOND_JACOBI;  // GIP_LinearSolver.h:70-80
     gipb200_require(gipb200_pcg_create(dA->handle(), myTopo->getAllSize(), &p, &S),
                     "gipb200_pcg_create");
   }
