@@ -1,7 +1,9 @@
 // Smoothed-aggregation AMG (setup on the host, FP32 V-cycle on the device).
 //
 // Setup per level (operator A, near-null vector z):
-//   strength   |a_ij| > theta sqrt(|a_ii a_jj|)
+//   strength   |a_ij| > theta sqrt(|a_ii a_jj|), theta = 0 (with a positive threshold the
+//              smoothed coarse operators lose their weak couplings to singleton aggregates
+//              and fill in level after level)
 //   aggregates greedy: (1) a node whose strong neighbours are all free starts an aggregate
 //              with them; (2) a free node joins the aggregate of its strongest aggregated
 //              neighbour; (3) what is left forms aggregates with its free neighbours
@@ -29,7 +31,7 @@ namespace {
 
 constexpr int kCoarse = 1024;    // largest level inverted densely
 constexpr int kMaxLevels = 16;
-constexpr double kTheta = 0.08;  // strength threshold
+constexpr double kTheta = 0.0;   // strength threshold: every nonzero coupling is strong
 
 struct HCsr {
   int nr = 0, nc = 0;
@@ -104,8 +106,7 @@ int aggregate(const HCsr& A, const std::vector<double>& d, std::vector<int>& agg
 }
 
 // Row-wise product C = A B (Gustavson), rows in the order their columns first appear.
-HCsr spgemm(const HCsr& A, const HCsr& B) {
-  HCsr C;
+int spgemm(const HCsr& A, const HCsr& B, HCsr& C) {
   C.nr = A.nr;
   C.nc = B.nc;
   C.rp.assign((size_t)A.nr + 1, 0);
@@ -126,6 +127,10 @@ HCsr spgemm(const HCsr& A, const HCsr& B) {
       C.rp[i + 1] = c;
     }
   }
+  long long total = 0;
+  for (int i = 0; i < A.nr; ++i) total += C.rp[i + 1];
+  if (total > 0x7fffffffLL)
+    return fail(GIPB200_ERR_ARG, "AMG: a Galerkin product has %lld nonzeros (more than 2^31)", total);
   for (int i = 0; i < A.nr; ++i) C.rp[i + 1] += C.rp[i];
   C.ci.resize((size_t)C.rp[A.nr]);
   C.v.resize((size_t)C.rp[A.nr]);
@@ -153,7 +158,7 @@ HCsr spgemm(const HCsr& A, const HCsr& B) {
       }
     }
   }
-  return C;
+  return GIPB200_OK;
 }
 
 HCsr transpose(const HCsr& A) {
@@ -448,7 +453,8 @@ int Amg::build(int n, const int* rp, const int* ci, const double* v, const doubl
     }
     std::vector<int> agg;
     const int na = aggregate(A, d, agg);
-    if (na >= A.nr || na == 0) return fail(GIPB200_ERR_ARG, "AMG: level %d does not coarsen", l);
+    if (na == 0 || na > 0.8 * A.nr)
+      return fail(GIPB200_ERR_ARG, "AMG: level %d (%d unknowns) coarsens only to %d", l, A.nr, na);
     std::vector<double> nrm((size_t)na, 0.0);
     for (int i = 0; i < A.nr; ++i) nrm[agg[i]] += z[i] * z[i];
     for (auto& q : nrm) q = std::sqrt(q);
@@ -456,7 +462,9 @@ int Amg::build(int n, const int* rp, const int* ci, const double* v, const doubl
     for (int i = 0; i < A.nr; ++i) p0[i] = nrm[agg[i]] > 0.0 ? z[i] / nrm[agg[i]] : 0.0;
     HCsr P = smoothed_prolongator(A, d, agg, p0, na, w);
     HCsr R = transpose(P);
-    HCsr Ac = spgemm(R, spgemm(A, P));
+    HCsr AP, Ac;
+    GIPB_TRY(spgemm(A, P, AP));
+    GIPB_TRY(spgemm(R, AP, Ac));
     GIPB_TRY(upload(P, &L.P, s));
     GIPB_TRY(upload(R, &L.R, s));
     lv.push_back(std::move(Lp));
