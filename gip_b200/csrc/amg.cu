@@ -265,7 +265,8 @@ bool dense_inverse(int m, std::vector<double>& M, std::vector<double>& inv) {
   return true;
 }
 
-int upload(const HCsr& A, Sell32* S, cudaStream_t s) {
+template <typename T>
+int upload(const HCsr& A, SellT<T>* S, cudaStream_t s) {
   GIPB_TRY(validate_csr(A.nr, A.nc, (int)A.nnz(), A.rp.data(), A.ci.data(), A.nc, "AMG operator"));
   S->nrows = A.nr;
   S->ncols = A.nc;
@@ -280,14 +281,14 @@ int upload(const HCsr& A, Sell32* S, cudaStream_t s) {
   S->nslots = sptr[S->nslices];
   if (S->nslots > 0x7fffffffLL) return fail(GIPB200_ERR_ARG, "AMG operator too large");
   std::vector<int> col((size_t)std::max<long long>(S->nslots, 1), -1);
-  std::vector<float> val((size_t)std::max<long long>(S->nslots, 1), 0.0f);
+  std::vector<T> val((size_t)std::max<long long>(S->nslots, 1), T(0));
 #pragma omp parallel for schedule(static)
   for (int r = 0; r < A.nr; ++r) {
     const int sl = r >> 5, lane = r & 31;
     for (int k = A.rp[r]; k < A.rp[r + 1]; ++k) {
       const long long slot = sptr[sl] + 32LL * (k - A.rp[r]) + lane;
       col[slot] = A.ci[k];
-      val[slot] = (float)A.v[k];
+      val[slot] = (T)A.v[k];
     }
   }
   GIPB_TRY(S->sptr.upload(sptr.data(), sptr.size(), s));
@@ -304,10 +305,39 @@ __device__ __forceinline__ bool amg_enter(PcgScalars* S) {
   return S->done != 0;
 }
 
+__device__ __forceinline__ float fmat(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmat(double a, double b, double c) { return fma(a, b, c); }
+
+// One row of a sliced operator, summed slot by slot (padding: column -1, skipped).
+template <typename T, int CH>
+__device__ __forceinline__ T amg_row(const SellView<T>& A, const T* __restrict__ x, int s, int lane) {
+  const long long base = A.sptr[s];
+  const int len = (int)((A.sptr[s + 1] - base) >> 5);
+  const int* cp = A.col + base + lane;
+  const T* vp = A.val + base + lane;
+  T sum = T(0);
+  for (int j0 = 0; j0 < len; j0 += CH) {
+    int c[CH];
+    T v[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+      c[t] = (j0 + t < len) ? ld_stream(cp + (size_t)(j0 + t) * 32) : -1;
+      v[t] = (j0 + t < len) ? ld_stream(vp + (size_t)(j0 + t) * 32) : T(0);
+    }
+    T xv[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) xv[t] = (c[t] >= 0) ? __ldg(x + c[t]) : T(0);
+#pragma unroll
+    for (int t = 0; t < CH; ++t) sum = fmat(xv[t], v[t], sum);
+  }
+  return sum;
+}
+
 // x = dinv b
-__global__ void __launch_bounds__(256) k_amg_jacobi0(int n, const float* __restrict__ dinv,
-                                                     const float* __restrict__ b,
-                                                     float* __restrict__ x, PcgScalars* S) {
+template <typename T>
+__global__ void __launch_bounds__(256) k_amg_jacobi0(int n, const T* __restrict__ dinv,
+                                                     const T* __restrict__ b, T* __restrict__ x,
+                                                     PcgScalars* S) {
   if (amg_enter(S)) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     x[i] = dinv[i] * b[i];
@@ -315,29 +345,30 @@ __global__ void __launch_bounds__(256) k_amg_jacobi0(int n, const float* __restr
 
 enum { kResid = 0, kPlain = 1, kAdd = 2, kSmooth = 3 };
 // kResid: y = b - A x;  kPlain: y = A x;  kAdd: y += A x;  kSmooth: y = x + dinv (b - A x)
-template <int MODE>
-__global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<float> A, const float* __restrict__ x,
-                                                     const float* __restrict__ b,
-                                                     const float* __restrict__ dinv,
-                                                     float* __restrict__ y, PcgScalars* S) {
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<T> A, const T* __restrict__ x,
+                                                     const T* __restrict__ b,
+                                                     const T* __restrict__ dinv,
+                                                     T* __restrict__ y, PcgScalars* S) {
   if (amg_enter(S)) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int s = gw; s < A.nslices; s += nw) {
-    const float sum = sell_row_f32<4>(A, x, s, lane);
+    const T sum = amg_row<T, 4>(A, x, s, lane);
     const int i = s * 32 + lane;
     if (i < A.nrows) {
       if (MODE == kResid) y[i] = b[i] - sum;
       else if (MODE == kPlain) y[i] = sum;
       else if (MODE == kAdd) y[i] += sum;
-      else y[i] = fmaf(dinv[i], b[i] - sum, x[i]);
+      else y[i] = fmat(dinv[i], b[i] - sum, x[i]);
     }
   }
 }
 
 struct CycleFinish {
   PcgScalars* S;
+  int first;
   __device__ void operator()(const double* t) const {
     const double rz = t[0];
     if (!(rz > 0.0) || !isfinite(rz)) {  // preconditioner lost definiteness: restart CG
@@ -345,46 +376,48 @@ struct CycleFinish {
       S->rz = 0.0;
       return;
     }
-    S->beta = (S->rz > 0.0) ? rz / S->rz : 0.0;
+    S->beta = (!first && S->rz > 0.0) ? rz / S->rz : 0.0;
     S->rz = rz;
   }
 };
 
 // Level 0 post-smoothing with the dot: z = x + dinv (r - A x), r.z, beta.
-__global__ void __launch_bounds__(256, 8) k_amg_smooth_dot(SellView<float> A, const float* __restrict__ x,
-                                                           const float* __restrict__ r,
-                                                           const float* __restrict__ dinv,
-                                                           float* __restrict__ z, PcgScalars* S,
-                                                           ReduceScratch rs) {
+template <typename T>
+__global__ void __launch_bounds__(256, 8) k_amg_smooth_dot(SellView<T> A, const T* __restrict__ x,
+                                                           const T* __restrict__ r,
+                                                           const T* __restrict__ dinv,
+                                                           T* __restrict__ z, PcgScalars* S,
+                                                           ReduceScratch rs, int first) {
   if (amg_enter(S)) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   double acc[1] = {0.0};
   for (int s = gw; s < A.nslices; s += nw) {
-    const float sum = sell_row_f32<4>(A, x, s, lane);
+    const T sum = amg_row<T, 4>(A, x, s, lane);
     const int i = s * 32 + lane;
     if (i < A.nrows) {
-      const float ri = r[i];
-      const float zi = fmaf(dinv[i], ri - sum, x[i]);
+      const T ri = r[i];
+      const T zi = fmat(dinv[i], ri - sum, x[i]);
       z[i] = zi;
       acc[0] += (double)ri * (double)zi;
     }
   }
-  grid_reduce<SumOp, 1>(acc, rs, CycleFinish{S});
+  grid_reduce<SumOp, 1>(acc, rs, CycleFinish{S, first});
 }
 
 // Coarsest level: x = C b, one warp per row of the dense inverse.
-__global__ void __launch_bounds__(256) k_amg_dense(int m, const float* __restrict__ C,
-                                                   const float* __restrict__ b,
-                                                   float* __restrict__ x, PcgScalars* S) {
+template <typename T>
+__global__ void __launch_bounds__(256) k_amg_dense(int m, const T* __restrict__ C,
+                                                   const T* __restrict__ b, T* __restrict__ x,
+                                                   PcgScalars* S) {
   if (amg_enter(S)) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int i = gw; i < m; i += nw) {
-    float acc = 0.f;
-    for (int j = lane; j < m; j += 32) acc = fmaf(C[(size_t)i * m + j], b[j], acc);
+    T acc = T(0);
+    for (int j = lane; j < m; j += 32) acc = fmat(C[(size_t)i * m + j], b[j], acc);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if (lane == 0) x[i] = acc;
@@ -399,8 +432,9 @@ int vec_blocks(int n) {
 
 }  // namespace
 
-int Amg::build(int n, const int* rp, const int* ci, const double* v, const double* z0,
-               bool singular, cudaStream_t s) {
+template <typename T>
+int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const double* z0,
+                   bool singular, int x0_len, cudaStream_t s) {
   const auto t0 = std::chrono::steady_clock::now();
   HCsr A;
   A.nr = A.nc = n;
@@ -412,18 +446,19 @@ int Amg::build(int n, const int* rp, const int* ci, const double* v, const doubl
   const double nnz0 = (double)A.nnz();
   double nnz_all = 0.0;
   for (int l = 0; l < kMaxLevels; ++l) {
-    std::unique_ptr<AmgLevel> Lp(new AmgLevel());
-    AmgLevel& L = *Lp;
+    std::unique_ptr<AmgLevel<T>> Lp(new AmgLevel<T>());
+    AmgLevel<T>& L = *Lp;
     L.n = A.nr;
     const std::vector<double> d = diagonal(A);
     for (int i = 0; i < A.nr; ++i)
       if (!(d[i] > 0.0)) return fail(GIPB200_ERR_ARG, "AMG: level %d row %d has no positive diagonal", l, i);
     const double rho = rho_bound(A, d);
     const double w = 4.0 / (3.0 * rho);
-    std::vector<float> dinv((size_t)A.nr);
-    for (int i = 0; i < A.nr; ++i) dinv[i] = (float)(w / d[i]);
+    std::vector<T> dinv((size_t)A.nr);
+    for (int i = 0; i < A.nr; ++i) dinv[i] = (T)(w / d[i]);
     GIPB_TRY(L.dinv.upload(dinv.data(), dinv.size(), s));
-    GIPB_TRY(L.x.alloc((size_t)A.nr));
+    GIPB_TRY(L.x.alloc((size_t)(l == 0 ? std::max(A.nr, x0_len) : A.nr)));
+    GIPB_TRY(L.x.zero(s));  // level 0: entries past n are gathered (as zero) by A0
     GIPB_TRY(L.t.alloc((size_t)A.nr));
     if (l > 0) {
       GIPB_TRY(L.b.alloc((size_t)A.nr));
@@ -445,7 +480,7 @@ int Amg::build(int n, const int* rp, const int* ci, const double* v, const doubl
       std::vector<double> inv;
       if (!dense_inverse(m, M, inv))
         return fail(GIPB200_ERR_ARG, "AMG: coarsest operator (%d) is not positive definite", m);
-      std::vector<float> cf(inv.begin(), inv.end());
+      std::vector<T> cf(inv.begin(), inv.end());
       GIPB_TRY(cinv.upload(cf.data(), cf.size(), s));
       nc = m;
       lv.push_back(std::move(Lp));
@@ -473,45 +508,49 @@ int Amg::build(int n, const int* rp, const int* ci, const double* v, const doubl
   }
   if (nc == 0) return fail(GIPB200_ERR_ARG, "AMG: more than %d levels", kMaxLevels);
   op_complexity = nnz_all / std::max(nnz0, 1.0);
-  kernels_per_cycle = 5LL * ((long long)lv.size() - 1) + 1;
-  GIPB_TRY(grid_blocks(256, n, 1, kMaxReduceBlocks, &blocks));
   GIPB_CUDA(cudaStreamSynchronize(s));
   setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return GIPB200_OK;
 }
 
-int Amg::enqueue(SellView<float> A0, const float* r, float* z0, PcgScalars* S, ReduceScratch rs,
-                 cudaStream_t s) const {
+template <typename T>
+int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScratch rs, int first,
+                     cudaStream_t s) const {
   const int L = (int)lv.size();
   // downward: pre-smooth from zero, residual, restriction
   for (int l = 0; l < L - 1; ++l) {
-    const AmgLevel& V = *lv[l];
-    const SellView<float> A = l == 0 ? A0 : V.A.view();
-    const float* b = l == 0 ? r : V.b.p;
+    const AmgLevel<T>& V = *lv[l];
+    const SellView<T> A = l == 0 ? A0 : V.A.view();
+    const T* b = l == 0 ? r : V.b.p;
     const int bn = vec_blocks(V.n), bs = vec_blocks(A.nslices * 32);
-    k_amg_jacobi0<<<bn, 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
-    k_amg_spmv<kResid><<<bs, 256, 0, s>>>(A, V.x.p, b, nullptr, V.t.p, S);
-    const SellView<float> R = V.R.view();
-    k_amg_spmv<kPlain><<<vec_blocks(R.nslices * 32), 256, 0, s>>>(R, V.t.p, nullptr, nullptr,
-                                                                  lv[l + 1]->b.p, S);
+    k_amg_jacobi0<T><<<bn, 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
+    k_amg_spmv<T, kResid><<<bs, 256, 0, s>>>(A, V.x.p, b, nullptr, V.t.p, S);
+    const SellView<T> R = V.R.view();
+    k_amg_spmv<T, kPlain><<<vec_blocks(R.nslices * 32), 256, 0, s>>>(R, V.t.p, nullptr, nullptr,
+                                                                     lv[l + 1]->b.p, S);
   }
-  const AmgLevel& C = *lv[L - 1];
-  k_amg_dense<<<std::min(kMaxReduceBlocks, (nc + 7) / 8), 256, 0, s>>>(nc, cinv.p, C.b.p, C.x.p, S);
+  const AmgLevel<T>& C = *lv[L - 1];
+  k_amg_dense<T><<<std::min(kMaxReduceBlocks, (nc + 7) / 8), 256, 0, s>>>(nc, cinv.p, C.b.p,
+                                                                            C.x.p, S);
   // upward: prolongation, post-smoothing (level 0 also reduces r.z)
   for (int l = L - 2; l >= 0; --l) {
-    const AmgLevel& V = *lv[l];
-    const float* xc = (l + 1 == L - 1) ? lv[l + 1]->x.p : lv[l + 1]->t.p;
-    const SellView<float> P = V.P.view();
-    k_amg_spmv<kAdd><<<vec_blocks(P.nslices * 32), 256, 0, s>>>(P, xc, nullptr, nullptr, V.x.p, S);
-    const SellView<float> A = l == 0 ? A0 : V.A.view();
+    const AmgLevel<T>& V = *lv[l];
+    const T* xc = (l + 1 == L - 1) ? lv[l + 1]->x.p : lv[l + 1]->t.p;
+    const SellView<T> P = V.P.view();
+    k_amg_spmv<T, kAdd><<<vec_blocks(P.nslices * 32), 256, 0, s>>>(P, xc, nullptr, nullptr, V.x.p,
+                                                                   S);
+    const SellView<T> A = l == 0 ? A0 : V.A.view();
     const int bs = vec_blocks(A.nslices * 32);
     if (l == 0)
-      k_amg_smooth_dot<<<bs, 256, 0, s>>>(A, V.x.p, r, V.dinv.p, z0, S, rs);
+      k_amg_smooth_dot<T><<<bs, 256, 0, s>>>(A, V.x.p, r, V.dinv.p, z0, S, rs, first);
     else
-      k_amg_spmv<kSmooth><<<bs, 256, 0, s>>>(A, V.x.p, V.b.p, V.dinv.p, V.t.p, S);
+      k_amg_spmv<T, kSmooth><<<bs, 256, 0, s>>>(A, V.x.p, V.b.p, V.dinv.p, V.t.p, S);
   }
   GIPB_LAUNCH_CHECK();
   return GIPB200_OK;
 }
+
+template struct AmgT<float>;
+template struct AmgT<double>;
 
 }  // namespace gipb200

@@ -11,41 +11,49 @@ namespace gipb200 {
 
 struct PcgScalars;
 
-// FP32 sliced operator without the extra copies a Sell keeps (no FP64 values, no CSR).
-struct Sell32 {
+// Sliced operator without the extra copies a Sell keeps (values of one precision, no CSR).
+template <typename T>
+struct SellT {
   int nrows = 0, ncols = 0, nslices = 0;
   long long nslots = 0, nnz = 0;
   DevBuf<long long> sptr;
   DevBuf<int> col;
-  DevBuf<float> val;
-  SellView<float> view() const { return {nrows, nslices, sptr.p, col.p, val.p}; }
+  DevBuf<T> val;
+  SellView<T> view() const { return {nrows, nslices, sptr.p, col.p, val.p}; }
 };
 
+template <typename T>
 struct AmgLevel {
   int n = 0;
-  Sell32 A;               // the level's operator (level 0: the solver's own FP32 operator)
-  Sell32 P, R;            // prolongation (n x n_next) and restriction (n_next x n)
-  DevBuf<float> dinv;     // omega / a_ii of the Jacobi smoother
-  DevBuf<float> b, x, t;  // right-hand side (levels >= 1), iterate, work / smoothed iterate
+  SellT<T> A;             // the level's operator (level 0: the solver's own operator)
+  SellT<T> P, R;          // prolongation (n x n_next) and restriction (n_next x n)
+  DevBuf<T> dinv;         // omega / a_ii of the Jacobi smoother
+  DevBuf<T> b, x, t;      // right-hand side (levels >= 1), iterate, work / smoothed iterate
 };
 
-struct Amg {
-  std::vector<std::unique_ptr<AmgLevel>> lv;
+// T = float: preconditioner of the mixed form's FP32 CG; T = double: of the FP64 CG.
+template <typename T>
+struct AmgT {
+  std::vector<std::unique_ptr<AmgLevel<T>>> lv;
   int nc = 0;             // coarsest size: solved with a dense (pseudo-)inverse
-  DevBuf<float> cinv;     // nc x nc, row-major
+  DevBuf<T> cinv;         // nc x nc, row-major
   double op_complexity = 0.0, setup_s = 0.0;
-  int blocks = 1;
-  long long kernels_per_cycle = 0;
 
   // Hierarchy of the n x n operator (host CSR, FP64 values; columns < n), near-null
   // vector z.  singular: the operator annihilates z (pinned-Neumann inner system), so the
-  // coarsest level is inverted on the complement of z.
+  // coarsest level is inverted on the complement of z.  x0_len: length of level 0's
+  // iterate, at least the number of columns the level-0 operator given to enqueue gathers
+  // from (its entries past n stay zero).
   int build(int n, const int* rp, const int* ci, const double* v, const double* z, bool singular,
-            cudaStream_t s);
+            int x0_len, cudaStream_t s);
   // z0 = M r with the level-0 operator A0; the last kernel reduces r.z and sets the CG's
-  // beta = (r.z) / (previous r.z) (0 on the first cycle of a solve) and r.z in S.
-  int enqueue(SellView<float> A0, const float* r, float* z0, PcgScalars* S, ReduceScratch rs,
+  // beta = (r.z) / (previous r.z) (0 when `first` or when no previous r.z is stored) and
+  // stores r.z in S.
+  int enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScratch rs, int first,
               cudaStream_t s) const;
 };
+
+using Amg = AmgT<float>;
+using Amg64 = AmgT<double>;
 
 }  // namespace gipb200

@@ -294,9 +294,11 @@ struct CflStepFinish {
         H.iters[k] = pcg_mixed ? P->total_inner : P->iter;
         H.rr[k] = P->rr;
         H.outer[k] = pcg_mixed ? P->outer : 0;
-        // the step's 10 kernels and the PCG's: init + 3 per iteration in the FP64 forms,
-        // counted on the device in the mixed form
-        H.kernels[k] = 10 + (pcg_mixed ? P->kernels : 1 + 3 * P->iter);
+        // the step's 10 kernels and the PCG's: init + 3 per iteration in the FP64 forms
+        // (2 with AMG, whose V-cycle and direction kernels count themselves on the device),
+        // all counted on the device in the mixed form
+        H.kernels[k] = 10 + (pcg_mixed ? P->kernels
+                                       : 1 + (P->kernels ? 2 : 3) * P->iter + P->kernels);
       }
       S->step = k + 1;
     }
@@ -889,9 +891,10 @@ int gipb200_dns_get_info(gipb200_dns Dh, gipb200_dns_info* info) {
   info->slots_L = E.L.nslots;
   info->nnz_L = E.L.nnz;
   const Amg* amg = E.pcg.amg.get();
-  info->amg_levels = amg ? (int)amg->lv.size() : 0;
-  info->amg_complexity = amg ? amg->op_complexity : 0.0;
-  info->amg_setup_s = amg ? amg->setup_s : 0.0;
+  const Amg64* amg64 = E.pcg.amg64.get();
+  info->amg_levels = amg ? (int)amg->lv.size() : amg64 ? (int)amg64->lv.size() : 0;
+  info->amg_complexity = amg ? amg->op_complexity : amg64 ? amg64->op_complexity : 0.0;
+  info->amg_setup_s = amg ? amg->setup_s : amg64 ? amg64->setup_s : 0.0;
   return GIPB200_OK;
 }
 

@@ -225,6 +225,62 @@ __global__ void __launch_bounds__(256) k_pcg_update(int n, double* __restrict__ 
 }
 
 // p = 1.0 z + beta p  -- GIP_LinearSolver.h:113
+// ---- FP64 tolerance mode with the AMG preconditioner: the update keeps GIP's x and r
+// steps and tests r.r; z = M r, r.z and beta come from the V-cycle; then p = z + beta p.
+struct BetaFinishAmg {
+  PcgScalars* S;
+  int maxit;
+  double tol;
+  __device__ void operator()(const double* t) const {
+    S->rr = t[0];
+    S->iter += 1;
+    if (!isfinite(t[0])) {
+      S->status = GIPB200_ERR_BREAKDOWN;
+      S->done = 1;
+    } else if (!(sqrt(t[0]) > tol * sqrt(S->bb))) {
+      S->done = 1;
+    }
+    if (S->iter >= maxit) {
+      if (!S->done) S->status = GIPB200_ERR_NOT_CONVERGED;
+      S->done = 1;
+    }
+  }
+};
+
+__global__ void __launch_bounds__(256) k_pcg_update_amg(int n, double* __restrict__ x,
+                                                        double* __restrict__ r,
+                                                        const double* __restrict__ p,
+                                                        const double* __restrict__ Ap,
+                                                        PcgScalars* S, ReduceScratch rs, int maxit,
+                                                        double tol) {
+  if (S->done) return;
+  const double alpha = S->alpha;
+  const double malpha = dmul(-1.0, alpha);
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] = dadd(x[i], dmul(alpha, p[i]));
+    const double ri = dadd(r[i], dmul(malpha, Ap[i]));
+    r[i] = ri;
+    acc[0] = dadd(acc[0], dmul(ri, ri));
+  }
+  grid_reduce<SumOp, 1>(acc, rs, BetaFinishAmg{S, maxit, tol});
+}
+
+// p = z + beta p; counted on the device with the V-cycle's kernels
+__global__ void __launch_bounds__(256) k_pcg_pupdate_z(int n, double* __restrict__ p,
+                                                       const double* __restrict__ z,
+                                                       PcgScalars* S, int use_cond,
+                                                       cudaGraphConditionalHandle cond) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    atomicAdd(&S->kernels, 1);
+    set_loop(use_cond, cond, !S->done);
+  }
+  if (S->done) return;
+  const double beta = S->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = dadd(z[i], dmul(beta, p[i]));
+}
+
 __global__ void __launch_bounds__(256) k_pcg_pupdate(int n, double* __restrict__ p,
                                                      const double* __restrict__ r,
                                                      const double* __restrict__ dinv,
@@ -842,8 +898,8 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
   if (prm.mode != GIPB200_PCG_FIXED && !(prm.tol > 0)) return fail(GIPB200_ERR_ARG, "tol must be > 0");
   if (prm.precond != GIPB200_PRECOND_JACOBI && prm.precond != GIPB200_PRECOND_AMG)
     return fail(GIPB200_ERR_ARG, "unknown preconditioner %d", prm.precond);
-  if (prm.precond == GIPB200_PRECOND_AMG && prm.mode != GIPB200_PCG_MIXED)
-    return fail(GIPB200_ERR_ARG, "the AMG preconditioner is available in the mixed form only");
+  if (prm.precond == GIPB200_PRECOND_AMG && prm.mode == GIPB200_PCG_FIXED)
+    return fail(GIPB200_ERR_ARG, "the AMG preconditioner needs a tolerance mode (TOL or MIXED)");
   if (prm.mode == GIPB200_PCG_MIXED) {
     if (!(prm.inner_tol > 0 && prm.inner_tol < 1))
       return fail(GIPB200_ERR_ARG, "inner_tol (replacement factor) must be in (0,1)");
@@ -917,15 +973,12 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
       GIPB_LAUNCH_CHECK();
       GIPB_CUDA(cudaStreamSynchronize(s));
     }
+    if (prm.precond == GIPB200_PRECOND_AMG) GIPB_TRY(build_amg64(s));
   }
   GIPB_CUDA(cudaStreamSynchronize(s));
   return GIPB200_OK;
 }
 
-// Sorts each row of the FP32 operator by column (the mixed form's inner product order is
-// free; L itself keeps GIP's order) and drops the zero-valued ghost columns to padding.
-// Sorted rows give every slot of a slice one neighbour direction, which keeps the column
-// spread per slot small for the packed layout.
 // AMG hierarchy of the inner system: the Jacobi-scaled operator S L S with the pin
 // removed (the pure-Neumann part when L has the pinned structure), columns < n.  Its
 // near-null vector is S^-1 1 (L_N 1 = 0).
@@ -952,12 +1005,40 @@ int Pcg::build_amg(cudaStream_t s) {
   std::vector<double> z((size_t)n);
   for (int i = 0; i < n; ++i) z[i] = hs[i] > 0.0 ? 1.0 / hs[i] : 0.0;
   amg.reset(new Amg());
-  GIPB_TRY(amg->build(n, rp.data(), ci.data(), v.data(), z.data(), pin_row >= 0, s));
+  GIPB_TRY(amg->build(n, rp.data(), ci.data(), v.data(), z.data(), pin_row >= 0, n, s));
   GIPB_TRY(z32.alloc((size_t)n_all));
   GIPB_TRY(z32.zero(s));
   return GIPB200_OK;
 }
 
+// FP64 AMG hierarchy of L itself (columns < n; GIP's pin keeps L definite), near-null
+// vector the constants.
+int Pcg::build_amg64(cudaStream_t s) {
+  std::vector<double> hval((size_t)std::max(L->nnz, 1));
+  GIPB_CUDA(cudaMemcpyAsync(hval.data(), L->csr_val.p, (size_t)L->nnz * 8, cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> rp((size_t)n + 1, 0), ci;
+  std::vector<double> v;
+  for (int i = 0; i < n; ++i) {
+    for (int k = L->h_rowptr[i]; k < L->h_rowptr[i + 1]; ++k)
+      if (L->h_col[k] < n) {
+        ci.push_back(L->h_col[k]);
+        v.push_back(hval[k]);
+      }
+    rp[i + 1] = (int)ci.size();
+  }
+  std::vector<double> z((size_t)n, 1.0);
+  amg64.reset(new Amg64());
+  GIPB_TRY(amg64->build(n, rp.data(), ci.data(), v.data(), z.data(), false, n_all, s));
+  GIPB_TRY(z64.alloc((size_t)n));
+  GIPB_TRY(z64.zero(s));
+  return GIPB200_OK;
+}
+
+// Sorts each row of the FP32 operator by column (the mixed form's inner product order is
+// free; L itself keeps GIP's order) and drops the zero-valued ghost columns to padding.
+// Sorted rows give every slot of a slice one neighbour direction, which keeps the column
+// spread per slot small for the packed layout.
 int Pcg::sort_fp32_rows(cudaStream_t s) {
   const int ns = L->nslices;
   const long long nslots = L->nslots;
@@ -1223,17 +1304,29 @@ int Pcg::enqueue_fp64_graph(const double* b, double* x, const double* x0, cudaSt
   k_pcg_init<<<blocks_spmv, 256, 0, s>>>(L->view(), x, b, dinv.p, r.p, p.p, Ap.p, sc.p, rs,
                                           prm.mode, prm.maxit, prm.tol, 1, h);
   GIPB_LAUNCH_CHECK();
+  if (amg64) {  // z = M r, p = z
+    GIPB_TRY(amg64->enqueue(L->view(), r.p, z64.p, sc.p, rs, 1, s));
+    k_pcg_pupdate_z<<<blocks_vec, 256, 0, s>>>(n, p.p, z64.p, sc.p, 1, h);
+  }
   cudaGraph_t body;
   GIPB_TRY(add_while(s, h, &body));
   cudaStream_t bs = body_stream[0];
   GIPB_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeRelaxed));
   k_pcg_spmv_dot<<<blocks_spmv, 256, 0, bs>>>(L->view(), p.p, Ap.p, sc.p, rs, prm.mode);
-  launch_pcg_update(x, bs);
-  k_pcg_pupdate<<<blocks_vec, 256, 0, bs>>>(n, p.p, r.p, dinv.p, sc.p, 1, h);
+  int ast = GIPB200_OK;
+  if (amg64) {
+    k_pcg_update_amg<<<blocks_vec, 256, 0, bs>>>(n, x, r.p, p.p, Ap.p, sc.p, rs, prm.maxit, prm.tol);
+    ast = amg64->enqueue(L->view(), r.p, z64.p, sc.p, rs, 0, bs);
+    k_pcg_pupdate_z<<<blocks_vec, 256, 0, bs>>>(n, p.p, z64.p, sc.p, 1, h);
+  } else {
+    launch_pcg_update(x, bs);
+    k_pcg_pupdate<<<blocks_vec, 256, 0, bs>>>(n, p.p, r.p, dinv.p, sc.p, 1, h);
+  }
   cudaError_t le = cudaGetLastError();
   cudaGraph_t out = nullptr;
   GIPB_CUDA(cudaStreamEndCapture(bs, &out));
+  if (ast != GIPB200_OK) return ast;
   if (le != cudaSuccess) return fail(GIPB200_ERR_CUDA, "launch in loop body: %s", cudaGetErrorString(le));
   launches += 4;
   return GIPB200_OK;
@@ -1268,7 +1361,7 @@ int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaS
   if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 1, hl));
-  if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, s));
+  if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s));
   cudaGraph_t loop_body;
   GIPB_TRY(add_while(s, hl, &loop_body));
   cudaStream_t os = body_stream[0], is = body_stream[1];
@@ -1300,7 +1393,7 @@ int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaS
       if (rst != GIPB200_OK) return rst;
       if (le != cudaSuccess)
         return fail(GIPB200_ERR_CUDA, "launch in replacement body: %s", cudaGetErrorString(le));
-      if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, os));
+      if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, os));
     }
     return GIPB200_OK;
   }();
@@ -1322,11 +1415,22 @@ int Pcg::enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t
                                           prm.mode, prm.maxit, prm.tol, 0, 0);
   GIPB_LAUNCH_CHECK();
   launches += 1;
+  if (amg64) {  // z = M r, p = z
+    GIPB_TRY(amg64->enqueue(L->view(), r.p, z64.p, sc.p, rs, 1, s));
+    k_pcg_pupdate_z<<<blocks_vec, 256, 0, s>>>(n, p.p, z64.p, sc.p, 0, 0);
+  }
   const int poll = 16;
   for (int k = 0; k < prm.maxit; ++k) {
     k_pcg_spmv_dot<<<blocks_spmv, 256, 0, s>>>(L->view(), p.p, Ap.p, sc.p, rs, prm.mode);
-    launch_pcg_update(x, s);
-    k_pcg_pupdate<<<blocks_vec, 256, 0, s>>>(n, p.p, r.p, dinv.p, sc.p, 0, 0);
+    if (amg64) {
+      k_pcg_update_amg<<<blocks_vec, 256, 0, s>>>(n, x, r.p, p.p, Ap.p, sc.p, rs, prm.maxit,
+                                                   prm.tol);
+      GIPB_TRY(amg64->enqueue(L->view(), r.p, z64.p, sc.p, rs, 0, s));
+      k_pcg_pupdate_z<<<blocks_vec, 256, 0, s>>>(n, p.p, z64.p, sc.p, 0, 0);
+    } else {
+      launch_pcg_update(x, s);
+      k_pcg_pupdate<<<blocks_vec, 256, 0, s>>>(n, p.p, r.p, dinv.p, sc.p, 0, 0);
+    }
     GIPB_LAUNCH_CHECK();
     launches += 3;
     if (host_sync && prm.mode != GIPB200_PCG_FIXED && (k + 1) % poll == 0) {
@@ -1389,7 +1493,7 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
   if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 0, 0));
-  if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, s));
+  if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s));
   const int poll = 16;
   for (int k = 0; k < prm.maxit; ++k) {
     float* pin = (k & 1) ? p32b.p : p32.p;
@@ -1400,7 +1504,7 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
     k_mx_apply<<<blocks_vec, 256, 0, s>>>(n, x, y32.p, scale.p, sc.p);
     GIPB_LAUNCH_CHECK();
     GIPB_TRY(launch_mixed_residual(b, x, 0, s, 0, 0));
-    if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, s));
+    if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s));
     launches += 4;
     if (host_sync && (k + 1) % poll == 0) {
       int d;
@@ -1516,9 +1620,10 @@ int gipb200_pcg_get_info(gipb200_pcg S, gipb200_pcg_info* info) {
   info->value_table = S->P.cop.index_bits;
   info->compressed_fraction = S->P.cop.compressed_fraction;
   const Amg* amg = S->P.amg.get();
-  info->amg_levels = amg ? (int)amg->lv.size() : 0;
-  info->amg_complexity = amg ? amg->op_complexity : 0.0;
-  info->amg_setup_s = amg ? amg->setup_s : 0.0;
+  const Amg64* amg64 = S->P.amg64.get();
+  info->amg_levels = amg ? (int)amg->lv.size() : amg64 ? (int)amg64->lv.size() : 0;
+  info->amg_complexity = amg ? amg->op_complexity : amg64 ? amg64->op_complexity : 0.0;
+  info->amg_setup_s = amg ? amg->setup_s : amg64 ? amg64->setup_s : 0.0;
   return GIPB200_OK;
 }
 

@@ -75,6 +75,10 @@ struct Pcg {
   std::unique_ptr<Amg> amg;
   DevBuf<float> z32;         // preconditioned residual
   int build_amg(cudaStream_t s);
+  // AMG preconditioner of the FP64 CG (TOL with GIPB200_PRECOND_AMG)
+  std::unique_ptr<Amg64> amg64;
+  DevBuf<double> z64;
+  int build_amg64(cudaStream_t s);
   int sort_fp32_rows(cudaStream_t s);
   void launch_pcg_update(double* x, cudaStream_t s);
   int build_compressed(cudaStream_t s);

@@ -127,12 +127,13 @@ typedef struct {
                         FP32 residual has fallen by this factor (reliable update)   */
   int inner_maxit;   /* MIXED: unused (kept for layout)                              */
   int max_outer;     /* MIXED: cap on residual replacements                          */
-  int precond;       /* GIPB200_PRECOND_*: GIP's Jacobi (0); MIXED may take AMG (1)  */
+  int precond;       /* GIPB200_PRECOND_*: GIP's Jacobi (0); TOL/MIXED may take AMG  */
 } gipb200_pcg_params;
 
 /* Preconditioners.  JACOBI is GIP's (GIP_LinearSolver.h:70-80).  AMG (no counterpart in
- * the reference; MIXED only): a smoothed-aggregation multigrid V-cycle in FP32, its
- * hierarchy built on the host once at create time from the Jacobi-scaled operator. */
+ * the reference; TOL and MIXED): a smoothed-aggregation multigrid V-cycle, its hierarchy
+ * built on the host once at create time — in FP32 from the Jacobi-scaled operator for
+ * MIXED, in FP64 from the operator itself for TOL. */
 enum { GIPB200_PRECOND_JACOBI = 0, GIPB200_PRECOND_AMG = 1 };
 
 typedef struct {

@@ -186,3 +186,18 @@ def test_engine_mixed_amg_close_to_fp64(gpu, oracle_mod, graph):
     assert np.all(h["iters"] * 4 < hr["iters"]), (h["iters"], hr["iters"])
     for k in ("u", "v", "w"):
         assert rel_err(E.field(k), d.vec[k]) < 1e-6, k
+
+
+def test_engine_fp64_amg_matches_oracle(gpu, oracle_mod):
+    from gip_b200.device import DnsEngine
+    case, _ = cavity.generate(14, re=400.0)
+    E = DnsEngine(case, gamma=1.0 / 400, pcg_mode="tol", maxit=3000, tol=1e-10, precond="amg")
+    E.advance(4)
+    d = oracle_mod.OracleDNS(case, gamma=1.0 / 400, cg_maxit=3000, cg_mode=1, cg_tol=1e-12)
+    hr = d.run(4)
+    h = E.history()
+    assert np.all(h["iters"] * 4 < hr["iters"]), (h["iters"], hr["iters"])
+    for k in ("u", "v", "w"):
+        assert rel_err(E.field(k), d.vec[k]) < 1e-8, k
+    # device-counted launches: per step 10 + init + 2 per iteration + the V-cycles' kernels
+    assert np.all(h["kernels"] > 11 + 2 * h["iters"])

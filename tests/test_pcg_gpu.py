@@ -193,9 +193,19 @@ def test_mixed_amg_preconditioner(gpu, oracle_mod, n, tol):
     assert np.abs(xs - xr).max() / np.abs(xr).max() < 1e4 * tol
 
 
-def test_amg_only_in_mixed_form(gpu):
+def test_fp64_amg_preconditioner_and_fixed_mode_refusal(gpu, oracle_mod):
+    # FP64 tolerance mode with the FP64 V-cycle; FIXED mode (GIP's) keeps GIP's Jacobi
     from gip_b200 import _lib
     from gip_b200 import device as dv
-    L, _ = cavity.poisson_problem(6, seed=1)
+    L, b = cavity.poisson_problem(24, seed=5)
+    A = dv.DeviceMatrix(L)
     with pytest.raises(_lib.GipB200Error):
-        dv.PcgSolver(dv.DeviceMatrix(L), mode="tol", maxit=10, tol=1e-6, precond="amg")
+        dv.PcgSolver(A, mode="fixed", maxit=10, precond="amg")
+    S = dv.PcgSolver(A, mode="tol", maxit=2000, tol=1e-10, precond="amg")
+    x = _t(np.zeros(L.nrows))
+    res = S.solve(_t(b), x, _t(np.zeros(L.nrows)))
+    xr, it, _ = oracle_mod.pcg(L, b, np.zeros(L.nrows), maxit=20000, mode=1, tol=1e-10)
+    assert res["status"] == 0 and res["iterations"] * 5 < it, (res, it)
+    xs = x.cpu().numpy()
+    assert np.linalg.norm(b - L.to_scipy() @ xs) <= 1.5e-10 * np.linalg.norm(b)
+    assert np.abs(xs - xr).max() / np.abs(xr).max() < 1e-6
