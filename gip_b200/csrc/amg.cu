@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <type_traits>
 
 #include "amg.cuh"
 #include "device.cuh"
@@ -406,6 +407,85 @@ __global__ void __launch_bounds__(256, 8) k_amg_smooth_dot(SellView<T> A, const 
   grid_reduce<SumOp, 1>(acc, rs, CycleFinish{S, first});
 }
 
+// Level-0 products from the packed FP32 operator (same FMA order as the plain layout, so
+// the same results): kResid y = b - A x; kSmooth z = x + dinv (r - A x) with r.z and beta.
+template <int NIB, int K, int MODE>
+__global__ void __launch_bounds__(256, 8) k_amgp_spmv(SellView<float> A, PackedView pk,
+                                                      const float* __restrict__ x,
+                                                      const float* __restrict__ b,
+                                                      const float* __restrict__ dinv,
+                                                      float* __restrict__ y, PcgScalars* S,
+                                                      ReduceScratch rs, int first) {
+  if (amg_enter(S)) return;
+  constexpr int NT = 1 << NIB;
+  __shared__ float tab[NT];
+  for (int t = threadIdx.x; t < NT; t += blockDim.x) tab[t] = pk.table[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  double acc[1] = {0.0};
+  for (int s = gw; s < A.nslices; s += nw) {
+    const int i = s * 32 + lane;
+    float sum;
+    if (__ldg(pk.plain + s)) {
+      sum = amg_row<float, 2>(A, x, s, lane);
+    } else {
+      const uint4 d = ld_stream(pk.delta + i);
+      unsigned w0, w1;
+      if (NIB == 4) {
+        w0 = ld_stream(static_cast<const unsigned*>(pk.idx) + i);
+        w1 = 0u;
+      } else {
+        const uint2 w = ld_stream(static_cast<const uint2*>(pk.idx) + i);
+        w0 = w.x;
+        w1 = w.y;
+      }
+      const int4 b0 = __ldg(reinterpret_cast<const int4*>(pk.base) + 2 * s);
+      const int4 b1 = __ldg(reinterpret_cast<const int4*>(pk.base) + 2 * s + 1);
+      const int c[8] = {b0.x + (int)(d.x & 0xffffu), b0.y + (int)(d.x >> 16),
+                        b0.z + (int)(d.y & 0xffffu), b0.w + (int)(d.y >> 16),
+                        b1.x + (int)(d.z & 0xffffu), b1.y + (int)(d.z >> 16),
+                        b1.z + (int)(d.w & 0xffffu), b1.w + (int)(d.w >> 16)};
+      float xv[K];
+#pragma unroll
+      for (int j = 0; j < K; ++j) xv[j] = __ldg(x + c[j]);
+      sum = 0.f;
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        const unsigned id =
+            (NIB == 4) ? (w0 >> (4 * j)) & 15u : ((j < 4 ? w0 : w1) >> (8 * (j & 3))) & 255u;
+        sum = fmaf(xv[j], tab[id], sum);
+      }
+    }
+    if (i < A.nrows) {
+      if (MODE == kResid) {
+        y[i] = b[i] - sum;
+      } else {
+        const float ri = b[i];
+        const float zi = fmaf(dinv[i], ri - sum, x[i]);
+        y[i] = zi;
+        acc[0] += (double)ri * (double)zi;
+      }
+    }
+  }
+  if (MODE == kSmooth) grid_reduce<SumOp, 1>(acc, rs, CycleFinish{S, first});
+}
+
+template <int MODE>
+void launch_amgp(const PackedView& pk, SellView<float> A, int nb, const float* x, const float* b,
+                 const float* dinv, float* y, PcgScalars* S, ReduceScratch rs, int first,
+                 cudaStream_t s) {
+  if (pk.nib == 4 && pk.slots == 7)
+    k_amgp_spmv<4, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first);
+  else if (pk.nib == 4)
+    k_amgp_spmv<4, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first);
+  else if (pk.slots == 7)
+    k_amgp_spmv<8, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first);
+  else
+    k_amgp_spmv<8, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first);
+}
+
 // Coarsest level: x = C b, one warp per row of the dense inverse.
 template <typename T>
 __global__ void __launch_bounds__(256) k_amg_dense(int m, const T* __restrict__ C,
@@ -431,6 +511,15 @@ int vec_blocks(int n) {
 }
 
 }  // namespace
+
+// The packed level-0 products exist for FP32 only.
+template <int MODE, typename T>
+void launch_packed0(const PackedView& pk, SellView<T> A, int nb, const T* x, const T* b,
+                    const T* dinv, T* y, PcgScalars* S, ReduceScratch rs, int first,
+                    cudaStream_t s) {
+  if constexpr (std::is_same<T, float>::value)
+    launch_amgp<MODE>(pk, A, nb, x, b, dinv, y, S, rs, first, s);
+}
 
 template <typename T>
 int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const double* z0,
@@ -515,7 +604,8 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
 
 template <typename T>
 int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScratch rs, int first,
-                     cudaStream_t s) const {
+                     cudaStream_t s, const PackedView* pk) const {
+  const bool packed = pk && pk->on && std::is_same<T, float>::value;
   const int L = (int)lv.size();
   // downward: pre-smooth from zero, residual, restriction
   for (int l = 0; l < L - 1; ++l) {
@@ -524,7 +614,10 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     const T* b = l == 0 ? r : V.b.p;
     const int bn = vec_blocks(V.n), bs = vec_blocks(A.nslices * 32);
     k_amg_jacobi0<T><<<bn, 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
-    k_amg_spmv<T, kResid><<<bs, 256, 0, s>>>(A, V.x.p, b, nullptr, V.t.p, S);
+    if (l == 0 && packed)
+      launch_packed0<kResid>(*pk, A, bs, V.x.p, b, (const T*)nullptr, V.t.p, S, rs, first, s);
+    else
+      k_amg_spmv<T, kResid><<<bs, 256, 0, s>>>(A, V.x.p, b, nullptr, V.t.p, S);
     const SellView<T> R = V.R.view();
     k_amg_spmv<T, kPlain><<<vec_blocks(R.nslices * 32), 256, 0, s>>>(R, V.t.p, nullptr, nullptr,
                                                                      lv[l + 1]->b.p, S);
@@ -541,7 +634,9 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
                                                                    S);
     const SellView<T> A = l == 0 ? A0 : V.A.view();
     const int bs = vec_blocks(A.nslices * 32);
-    if (l == 0)
+    if (l == 0 && packed)
+      launch_packed0<kSmooth>(*pk, A, bs, V.x.p, r, V.dinv.p, z0, S, rs, first, s);
+    else if (l == 0)
       k_amg_smooth_dot<T><<<bs, 256, 0, s>>>(A, V.x.p, r, V.dinv.p, z0, S, rs, first);
     else
       k_amg_spmv<T, kSmooth><<<bs, 256, 0, s>>>(A, V.x.p, V.b.p, V.dinv.p, V.t.p, S);

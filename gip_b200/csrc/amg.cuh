@@ -22,6 +22,18 @@ struct SellT {
   SellView<T> view() const { return {nrows, nslices, sptr.p, col.p, val.p}; }
 };
 
+// The mixed form's packed FP32 operator (see CompressedOp), for the V-cycle's level-0
+// products.  on = false: use the plain sliced view.
+struct PackedView {
+  bool on = false;
+  int nib = 4, slots = 8;
+  const uint4* delta = nullptr;
+  const void* idx = nullptr;
+  const int* base = nullptr;
+  const unsigned char* plain = nullptr;
+  const float* table = nullptr;
+};
+
 template <typename T>
 struct AmgLevel {
   int n = 0;
@@ -50,7 +62,7 @@ struct AmgT {
   // beta = (r.z) / (previous r.z) (0 when `first` or when no previous r.z is stored) and
   // stores r.z in S.
   int enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScratch rs, int first,
-              cudaStream_t s) const;
+              cudaStream_t s, const PackedView* pk = nullptr) const;
 };
 
 using Amg = AmgT<float>;

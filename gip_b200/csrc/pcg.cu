@@ -1356,12 +1356,13 @@ static int add_if(cudaStream_t cs, cudaGraphConditionalHandle h, cudaGraph_t* bo
 }
 
 int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaStream_t s) {
+  const PackedView pk0 = packed();
   cudaGraphConditionalHandle hl;
   GIPB_TRY(make_handle(s, 0, 0, &hl));
   if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 1, hl));
-  if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s));
+  if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s, &pk0));
   cudaGraph_t loop_body;
   GIPB_TRY(add_while(s, hl, &loop_body));
   cudaStream_t os = body_stream[0], is = body_stream[1];
@@ -1393,7 +1394,7 @@ int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaS
       if (rst != GIPB200_OK) return rst;
       if (le != cudaSuccess)
         return fail(GIPB200_ERR_CUDA, "launch in replacement body: %s", cudaGetErrorString(le));
-      if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, os));
+      if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, os, &pk0));
     }
     return GIPB200_OK;
   }();
@@ -1490,10 +1491,11 @@ int Pcg::launch_mixed_residual(const double* b, const double* x, int first, cuda
 
 int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_t s,
                        bool host_sync) {
+  const PackedView pk0 = packed();
   if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 0, 0));
-  if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s));
+  if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s, &pk0));
   const int poll = 16;
   for (int k = 0; k < prm.maxit; ++k) {
     float* pin = (k & 1) ? p32b.p : p32.p;
@@ -1504,7 +1506,7 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
     k_mx_apply<<<blocks_vec, 256, 0, s>>>(n, x, y32.p, scale.p, sc.p);
     GIPB_LAUNCH_CHECK();
     GIPB_TRY(launch_mixed_residual(b, x, 0, s, 0, 0));
-    if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s));
+    if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s, &pk0));
     launches += 4;
     if (host_sync && (k + 1) % poll == 0) {
       int d;

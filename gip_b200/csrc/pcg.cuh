@@ -83,6 +83,18 @@ struct Pcg {
   void launch_pcg_update(double* x, cudaStream_t s);
   int build_compressed(cudaStream_t s);
   SellView<float> a32() const { return {L->nrows, L->nslices, L->sptr.p, col32.p, lhat.p}; }
+  PackedView packed() const {
+    PackedView v;
+    v.on = cop.enabled && !cop.tma;
+    v.nib = cop.index_bits;
+    v.slots = cop.slots;
+    v.delta = cop.delta.p;
+    v.idx = cop.index_bits == 4 ? (const void*)cop.idx4.p : (const void*)cop.idx8.p;
+    v.base = cop.base.p;
+    v.plain = cop.plain.p;
+    v.table = cop.table.p;
+    return v;
+  }
   // Pinned-Neumann structure of L (every row sums to zero except one pinned row p with
   // sum pin > 0): the FP32 inner solve then runs on the pure-Neumann part and the
   // constant mode is restored exactly from the pin equation.

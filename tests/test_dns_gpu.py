@@ -201,3 +201,21 @@ def test_engine_fp64_amg_matches_oracle(gpu, oracle_mod):
         assert rel_err(E.field(k), d.vec[k]) < 1e-8, k
     # device-counted launches: per step 10 + init + 2 per iteration + the V-cycles' kernels
     assert np.all(h["kernels"] > 11 + 2 * h["iters"])
+
+
+def test_amg_packed_level0_is_exact(gpu, monkeypatch):
+    # the V-cycle's level-0 products from the packed operator equal the plain layout's
+    from gip_b200.device import DnsEngine
+    case, _ = cavity.generate(18, re=400.0, permute_seed=3)
+    kw = dict(gamma=1.0 / 400, pcg_mode="mixed", maxit=3000, tol=1e-8, inner_tol=1e-2,
+              max_outer=100, reorder=True, precond="amg")
+    E = DnsEngine(case, **kw)
+    assert E.info()["compressed"] == 1
+    monkeypatch.setenv("GIPB200_NO_COMPRESS", "1")
+    P = DnsEngine(case, **kw)
+    assert P.info()["compressed"] == 0
+    E.advance(3)
+    P.advance(3)
+    assert E.history()["iters"].tolist() == P.history()["iters"].tolist()
+    for k in ("u", "v", "w", "p"):
+        assert np.array_equal(E.field(k), P.field(k)), k
