@@ -273,6 +273,17 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s) {
   S->ncols = A.nc;
   S->nnz = A.nnz();
   S->nslices = (A.nr + 31) / 32;
+  const double avg = (double)A.nnz() / std::max(A.nr, 1);
+  if (avg >= 12.0) {  // long rows: CSR, 8 to 32 threads per row
+    S->lanes = avg >= 48.0 ? 32 : avg >= 24.0 ? 16 : 8;
+    std::vector<T> val(A.v.size());
+    for (size_t k = 0; k < A.v.size(); ++k) val[k] = (T)A.v[k];
+    GIPB_TRY(S->rp.upload(A.rp.data(), A.rp.size(), s));
+    GIPB_TRY(S->col.upload(A.ci.data(), std::max<size_t>(A.ci.size(), 1), s));
+    GIPB_TRY(S->val.upload(val.data(), std::max<size_t>(val.size(), 1), s));
+    GIPB_CUDA(cudaStreamSynchronize(s));
+    return GIPB200_OK;
+  }
   std::vector<long long> sptr((size_t)S->nslices + 1, 0);
   for (int sl = 0; sl < S->nslices; ++sl) {
     int len = 0;
@@ -365,6 +376,60 @@ __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<T> A, const T* __r
       else y[i] = fmat(dinv[i], b[i] - sum, x[i]);
     }
   }
+}
+
+// The same products from the CSR form: LANES threads per row, each summing a strided part
+// of the row, combined by a fixed shuffle tree (deterministic).  The row loop is uniform
+// across the warp (32 / LANES rows per warp per pass), so every lane takes part in the
+// shuffles.
+template <typename T, int MODE, int LANES>
+__global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restrict__ rp,
+                                                 const int* __restrict__ col,
+                                                 const T* __restrict__ val, const T* __restrict__ x,
+                                                 const T* __restrict__ b,
+                                                 const T* __restrict__ dinv, T* __restrict__ y,
+                                                 PcgScalars* S) {
+  if (amg_enter(S)) return;
+  constexpr int RPW = 32 / LANES;  // rows per warp per pass
+  const int lane = threadIdx.x & 31, sub = lane % LANES;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int r0 = gw * RPW; r0 < nrows; r0 += nw * RPW) {
+    const int i = r0 + lane / LANES;
+    T sum = T(0);
+    if (i < nrows)
+      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) sum = fmat(ld_stream(val + k), __ldg(x + ld_stream(col + k)), sum);
+#pragma unroll
+    for (int o = LANES / 2; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o, LANES);
+    if (i < nrows && sub == 0) {
+      if (MODE == kResid) y[i] = b[i] - sum;
+      else if (MODE == kPlain) y[i] = sum;
+      else if (MODE == kAdd) y[i] += sum;
+      else y[i] = fmat(dinv[i], b[i] - sum, x[i]);
+    }
+  }
+}
+
+int vec_blocks(int n);
+
+// y (mode) A x for an AMG operator in either form.
+template <typename T, int MODE>
+void amg_mv(const SellT<T>& M, const T* x, const T* b, const T* dinv, T* y, PcgScalars* S,
+            cudaStream_t s) {
+  if (M.lanes == 0) {
+    k_amg_spmv<T, MODE><<<vec_blocks(M.nslices * 32), 256, 0, s>>>(M.view(), x, b, dinv, y, S);
+    return;
+  }
+  const int nb = vec_blocks((int)std::min<long long>((long long)M.nrows * M.lanes, 1LL << 30));
+  const int* rp = M.rp.p;
+  const int* ci = M.col.p;
+  const T* v = M.val.p;
+  if (M.lanes == 32)
+    k_amg_csr<T, MODE, 32><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
+  else if (M.lanes == 16)
+    k_amg_csr<T, MODE, 16><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
+  else
+    k_amg_csr<T, MODE, 8><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
 }
 
 struct CycleFinish {
@@ -610,17 +675,18 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
   // downward: pre-smooth from zero, residual, restriction
   for (int l = 0; l < L - 1; ++l) {
     const AmgLevel<T>& V = *lv[l];
-    const SellView<T> A = l == 0 ? A0 : V.A.view();
     const T* b = l == 0 ? r : V.b.p;
-    const int bn = vec_blocks(V.n), bs = vec_blocks(A.nslices * 32);
-    k_amg_jacobi0<T><<<bn, 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
-    if (l == 0 && packed)
-      launch_packed0<kResid>(*pk, A, bs, V.x.p, b, (const T*)nullptr, V.t.p, S, rs, first, s);
-    else
-      k_amg_spmv<T, kResid><<<bs, 256, 0, s>>>(A, V.x.p, b, nullptr, V.t.p, S);
-    const SellView<T> R = V.R.view();
-    k_amg_spmv<T, kPlain><<<vec_blocks(R.nslices * 32), 256, 0, s>>>(R, V.t.p, nullptr, nullptr,
-                                                                     lv[l + 1]->b.p, S);
+    k_amg_jacobi0<T><<<vec_blocks(V.n), 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
+    if (l == 0) {
+      const int bs = vec_blocks(A0.nslices * 32);
+      if (packed)
+        launch_packed0<kResid>(*pk, A0, bs, V.x.p, b, (const T*)nullptr, V.t.p, S, rs, first, s);
+      else
+        k_amg_spmv<T, kResid><<<bs, 256, 0, s>>>(A0, V.x.p, b, nullptr, V.t.p, S);
+    } else {
+      amg_mv<T, kResid>(V.A, V.x.p, b, (const T*)nullptr, V.t.p, S, s);
+    }
+    amg_mv<T, kPlain>(V.R, V.t.p, (const T*)nullptr, (const T*)nullptr, lv[l + 1]->b.p, S, s);
   }
   const AmgLevel<T>& C = *lv[L - 1];
   k_amg_dense<T><<<std::min(kMaxReduceBlocks, (nc + 7) / 8), 256, 0, s>>>(nc, cinv.p, C.b.p,
@@ -629,17 +695,16 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
   for (int l = L - 2; l >= 0; --l) {
     const AmgLevel<T>& V = *lv[l];
     const T* xc = (l + 1 == L - 1) ? lv[l + 1]->x.p : lv[l + 1]->t.p;
-    const SellView<T> P = V.P.view();
-    k_amg_spmv<T, kAdd><<<vec_blocks(P.nslices * 32), 256, 0, s>>>(P, xc, nullptr, nullptr, V.x.p,
-                                                                   S);
-    const SellView<T> A = l == 0 ? A0 : V.A.view();
-    const int bs = vec_blocks(A.nslices * 32);
-    if (l == 0 && packed)
-      launch_packed0<kSmooth>(*pk, A, bs, V.x.p, r, V.dinv.p, z0, S, rs, first, s);
-    else if (l == 0)
-      k_amg_smooth_dot<T><<<bs, 256, 0, s>>>(A, V.x.p, r, V.dinv.p, z0, S, rs, first);
-    else
-      k_amg_spmv<T, kSmooth><<<bs, 256, 0, s>>>(A, V.x.p, V.b.p, V.dinv.p, V.t.p, S);
+    amg_mv<T, kAdd>(V.P, xc, (const T*)nullptr, (const T*)nullptr, V.x.p, S, s);
+    if (l == 0) {
+      const int bs = vec_blocks(A0.nslices * 32);
+      if (packed)
+        launch_packed0<kSmooth>(*pk, A0, bs, V.x.p, r, V.dinv.p, z0, S, rs, first, s);
+      else
+        k_amg_smooth_dot<T><<<bs, 256, 0, s>>>(A0, V.x.p, r, V.dinv.p, z0, S, rs, first);
+    } else {
+      amg_mv<T, kSmooth>(V.A, V.x.p, V.b.p, V.dinv.p, V.t.p, S, s);
+    }
   }
   GIPB_LAUNCH_CHECK();
   return GIPB200_OK;

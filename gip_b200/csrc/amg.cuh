@@ -11,7 +11,9 @@ namespace gipb200 {
 
 struct PcgScalars;
 
-// Sliced operator without the extra copies a Sell keeps (values of one precision, no CSR).
+// An AMG operator in one precision: sliced (SELL-32, a thread per row) when its rows are
+// short, CSR with `lanes` threads per row when they are long (restrictions, coarse
+// Galerkin operators), where a thread per row would walk dozens of padded slots alone.
 template <typename T>
 struct SellT {
   int nrows = 0, ncols = 0, nslices = 0;
@@ -19,6 +21,8 @@ struct SellT {
   DevBuf<long long> sptr;
   DevBuf<int> col;
   DevBuf<T> val;
+  int lanes = 0;               // > 0: CSR form (rp, col, val) with this many threads per row
+  DevBuf<int> rp;
   SellView<T> view() const { return {nrows, nslices, sptr.p, col.p, val.p}; }
 };
 
