@@ -63,7 +63,8 @@ class DnsInfo(C.Structure):
 
 class AdjointParams(C.Structure):
     _fields_ = [("rho", C.c_double), ("gamma", C.c_double), ("nu0", C.c_double),
-                ("tol", C.c_double), ("maxit", C.c_int), ("checkpoint_every", C.c_int)]
+                ("tol", C.c_double), ("maxit", C.c_int), ("checkpoint_every", C.c_int),
+                ("precond", C.c_int)]
 
 
 PCG_FIXED, PCG_TOL, PCG_MIXED = 0, 1, 2

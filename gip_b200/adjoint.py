@@ -22,7 +22,7 @@ from .formats import GipCase
 class CavityAdjoint:
     def __init__(self, case: GipCase, lid_cells: np.ndarray, volume: np.ndarray, nu0: float,
                  rho: float = 1.0, gamma: float = 1e-3, tol: float = 1e-12, maxit: int = 20000,
-                 checkpoint_every: int = 10):
+                 checkpoint_every: int = 10, precond: str = "jacobi"):
         keep: list = []
         self._ops = L.DnsOps(**{n: _host_csr(case.ops[n], keep) for n in L.DNS_OPS},
                              n_inner=case.n_inner, n_owned=case.n_owned, n_faces=case.n_faces)
@@ -31,7 +31,8 @@ class CavityAdjoint:
         self.lid_cells = np.ascontiguousarray(lid_cells, np.int32)
         vol = np.ascontiguousarray(volume, np.float64)
         self.nu0 = nu0
-        prm = L.AdjointParams(rho, gamma, nu0, tol, maxit, checkpoint_every)
+        from .device import PRECONDS
+        prm = L.AdjointParams(rho, gamma, nu0, tol, maxit, checkpoint_every, PRECONDS[precond])
         h = C.c_void_p()
         L.call("gipb200_adjoint_create", C.byref(self._ops), _hptr(f["u"]), _hptr(f["v"]),
                _hptr(f["w"]), _hptr(f["dxs"]), _hptr(vol), _hptr(self.lid_cells),

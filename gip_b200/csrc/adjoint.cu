@@ -382,6 +382,7 @@ int gipb200_adjoint_create(const gipb200_dns_ops* ops, const double* h_u0, const
     dp.pcg.mode = GIPB200_PCG_TOL;
     dp.pcg.maxit = prm->maxit;
     dp.pcg.tol = prm->tol;
+    dp.pcg.precond = prm->precond;
     dp.use_graph = 1;
     dp.reorder = 0;
     GIPB_TRY(dns_init(A.E, ops, h_u0, h_v0, h_w0, h_dxs, &dp));
@@ -445,6 +446,7 @@ int gipb200_adjoint_create(const gipb200_dns_ops* ops, const double* h_u0, const
     pp.mode = GIPB200_PCG_TOL;
     pp.maxit = prm->maxit;
     pp.tol = prm->tol;
+    pp.precond = prm->precond;
     GIPB_TRY(A.adj.init(&A.E.L, NO, pp, 0));
     GIPB_CUDA(cudaDeviceSynchronize());
     return GIPB200_OK;

@@ -327,6 +327,7 @@ typedef struct {
   double tol;            /* relative tolerance of every Poisson solve (forward, adjoint) */
   int maxit;             /* PCG iteration cap                                         */
   int checkpoint_every;  /* forward checkpoint spacing, in steps                      */
+  int precond;           /* GIPB200_PRECOND_* of the forward and adjoint Poisson solves */
 } gipb200_adjoint_params;
 
 int gipb200_adjoint_create(const gipb200_dns_ops* ops, const double* h_u0, const double* h_v0,

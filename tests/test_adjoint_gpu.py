@@ -19,13 +19,15 @@ def _setup(n, re, seed=5):
     return case, meta, lid_cells, lid, vol
 
 
-@pytest.mark.parametrize("n,re,steps,every", [(6, 100.0, 5, 2), (8, 400.0, 6, 4)])
-def test_adjoint_matches_torch_autograd(gpu, n, re, steps, every):
+@pytest.mark.parametrize("n,re,steps,every,precond", [(6, 100.0, 5, 2, "jacobi"),
+                                                      (8, 400.0, 6, 4, "jacobi"),
+                                                      (10, 400.0, 5, 3, "amg")])
+def test_adjoint_matches_torch_autograd(gpu, n, re, steps, every, precond):
     from gip_b200.adjoint import CavityAdjoint
     case, meta, lid_cells, lid, vol = _setup(n, re)
     nu0 = 1.0 / re
     A = CavityAdjoint(case, lid_cells, vol, nu0=nu0, gamma=1.0 / re, tol=1e-13,
-                      checkpoint_every=every)
+                      checkpoint_every=every, precond=precond)
     J = A.forward(lid, nu0, steps)
     g_lid, g_nu = A.backward()
     # reference: torch autograd through the same step with the same frozen steps
