@@ -133,6 +133,46 @@ __device__ __forceinline__ void sell_row_f64(const SellView<V>& A, const X* __re
   }
 }
 
+// Two rows products of one operator row with two vectors (sum1 = row.x1, sum2 = row.x2),
+// each summed slot by slot with GIP's rounding: the same results as two sell_row_f64
+// calls, with the row's columns and values streamed once.
+template <typename V, int CH = 4>
+__device__ __forceinline__ void sell_row_f64_pair(const SellView<V>& A, const double* __restrict__ x1,
+                                                  const double* __restrict__ x2, int s, int lane,
+                                                  double& sum1, double& sum2, bool& any) {
+  const long long base = A.sptr[s];
+  const int len = (int)((A.sptr[s + 1] - base) >> 5);
+  const int* cp = A.col + base + lane;
+  const V* vp = A.val + base + lane;
+  for (int j0 = 0; j0 < len; j0 += CH) {
+    int c[CH];
+    V v[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+      if (j0 + t < len) {
+        c[t] = ld_stream(cp + (size_t)(j0 + t) * 32);
+        v[t] = ld_stream(vp + (size_t)(j0 + t) * 32);
+      } else {
+        c[t] = -1;
+        v[t] = V(0);
+      }
+    }
+    double a[CH], b[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+      a[t] = (c[t] >= 0) ? __ldg(x1 + c[t]) : 0.0;
+      b[t] = (c[t] >= 0) ? __ldg(x2 + c[t]) : 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < CH; ++t)
+      if (c[t] >= 0) {
+        sum1 = dadd(sum1, dmul(a[t], (double)v[t]));
+        sum2 = dadd(sum2, dmul(b[t], (double)v[t]));
+        any = true;
+      }
+  }
+}
+
 // FP32 row: FP32 storage and FP32 accumulation (the inner solver of the mixed form).
 template <int CH = 8>
 __device__ __forceinline__ float sell_row_f32(const SellView<float>& A, const float* __restrict__ x,

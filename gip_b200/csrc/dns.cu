@@ -186,20 +186,12 @@ __global__ void __launch_bounds__(256) k_dns_massflux(
   for (int s = gw; s < ns; s += nw) {
     const int f = s * 32 + lane;
     double so = 0, gx = 0, gy = 0, gz = 0, ux = 0, uy = 0, uz = 0;
-    bool a0 = false, ax = false, ay = false, az = false, bx = false, by = false, bz = false;
+    bool a0 = false, ax = false, ay = false, az = false;
     if (s < SO.nslices) sell_row_f64(SO, p, s, lane, so, a0);
-    if (s < SFx.nslices) {
-      sell_row_f64(SFx, gpx, s, lane, gx, ax);
-      sell_row_f64(SFx, u, s, lane, ux, bx);
-    }
-    if (s < SFy.nslices) {
-      sell_row_f64(SFy, gpy, s, lane, gy, ay);
-      sell_row_f64(SFy, v, s, lane, uy, by);
-    }
-    if (s < SFz.nslices) {
-      sell_row_f64(SFz, gpz, s, lane, gz, az);
-      sell_row_f64(SFz, w, s, lane, uz, bz);
-    }
+    // each SF row once, against the pressure gradient and the velocity together
+    if (s < SFx.nslices) sell_row_f64_pair(SFx, gpx, u, s, lane, gx, ux, ax);
+    if (s < SFy.nslices) sell_row_f64_pair(SFy, gpy, v, s, lane, gy, uy, ay);
+    if (s < SFz.nslices) sell_row_f64_pair(SFz, gpz, w, s, lane, gz, uz, az);
     a0 = a0 && f < SO.nrows;
     ax = ax && f < SFx.nrows;
     ay = ay && f < SFy.nrows;
