@@ -370,31 +370,42 @@ int Dns::enqueue_initial_dt(cudaStream_t s) {
 int Dns::enqueue_step(cudaStream_t s, bool host_sync) {
   const DnsHistory H = history();
   const long long pcg_before = pcg.launches;
+  auto mark = [&](int k) {
+    if (phase_events) cudaEventRecord(phase_events[k], s);
+  };
+  mark(0);
   // PredictorVelocity: C's values from the face fluxes, then D/C products and AB2
   GIPB_TRY(launch_csr_spmv(Ec.nrows, Ec.rowptr.p, Ec.csr_col.p, Ec.csr_val.p, mf.p, cval.p, D.pos.p,
                            0.0, 0.0, 0, s));
   k_dns_convdiff<<<grid.convdiff, 256, 0, s>>>(D.view(), cval.p, u.p, v.p, w.p, ax.p, ay.p, az.p);
   k_dns_ab2<<<grid.ab2, 256, 0, s>>>(N, u.p, v.p, w.p, ax.p, ay.p, az.p, ax0.p, ay0.p, az0.p, sc.p);
+  mark(1);
   // PoissonEquation
   k_dns_rhs<<<grid.rhs, 256, 0, s>>>(Mx.view(), My.view(), Mz.view(), u.p, v.p, w.p, rhs.p, sc.p);
   GIPB_LAUNCH_CHECK();
+  mark(2);
   GIPB_TRY(pcg.enqueue(rhs.p, p.p, p0.p, s, host_sync));
+  mark(3);
   k_dns_pcopy<<<blocks_owned, 256, 0, s>>>(N, NO, p.p, p0.p);
   GIPB_LAUNCH_CHECK();
   GIPB_TRY(launch_sell_spmv(Lb, Lb.val.p, p0.p, p.p, 1.0, 1.0, 1, s));
+  mark(4);
   // VelocityCorrection
   k_dns_gradcorr<<<grid.gradcorr, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p, gpx.p, gpy.p,
                                                gpz.p, u.p, v.p, w.p, N, prm.rho, sc.p);
+  mark(5);
   // MassFluxes
   k_dns_massflux<<<grid.massflux, 256, 0, s>>>(SO.view(), SFx.view(), SFy.view(), SFz.view(), p.p,
                                                gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p, prm.rho,
                                                sc.p);
+  mark(6);
   // CFLCondition
   k_dns_massr<<<grid.massr, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
   k_dns_cfl<<<grid.cfl, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p, H,
                                         pcg.sc.p, 1, prm.pcg.mode == GIPB200_PCG_MIXED, dt_seq.p,
                                         dt_seq_len, rs);
   GIPB_LAUNCH_CHECK();
+  mark(7);
   launches += 10 + (pcg.launches - pcg_before);
   return GIPB200_OK;
 }
@@ -760,6 +771,42 @@ int gipb200_dns_destroy(gipb200_dns D) {
 int gipb200_dns_advance(gipb200_dns Dh, int nsteps, void* stream) {
   if (!Dh || nsteps < 0) return fail(GIPB200_ERR_ARG, "bad arguments");
   return dns_advance(Dh->E, nsteps, as_stream(stream));
+}
+
+int gipb200_dns_step_phases(gipb200_dns Dh, void* stream, double* h_ms) {
+  if (!Dh || !h_ms) return fail(GIPB200_ERR_ARG, "null argument");
+  Dns& E = Dh->E;
+  cudaStream_t s = as_stream(stream);
+  GIPB_TRY(E.grow_history(E.steps_enqueued + 1, s));
+  if (!E.started) {
+    GIPB_TRY(E.enqueue_initial_dt(s));
+    E.started = true;
+  }
+  cudaEvent_t ev[8];
+  int made = 0;
+  int st = GIPB200_OK;
+  for (; made < 8; ++made)
+    if (cudaEventCreate(&ev[made]) != cudaSuccess) {
+      st = fail(GIPB200_ERR_CUDA, "cudaEventCreate failed");
+      break;
+    }
+  if (st == GIPB200_OK) {
+    E.phase_events = ev;
+    st = E.enqueue_step(s, true);
+    E.phase_events = nullptr;
+    if (st == GIPB200_OK) {
+      E.steps_enqueued += 1;
+      if (cudaEventSynchronize(ev[7]) != cudaSuccess) st = fail(GIPB200_ERR_CUDA, "step failed");
+      for (int k = 0; k < 7 && st == GIPB200_OK; ++k) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ev[k], ev[k + 1]) != cudaSuccess)
+          st = fail(GIPB200_ERR_CUDA, "cudaEventElapsedTime failed");
+        h_ms[k] = ms;
+      }
+    }
+  }
+  for (int k = 0; k < made; ++k) cudaEventDestroy(ev[k]);
+  return st;
 }
 
 int gipb200_dns_history(gipb200_dns Dh, int* steps, double* t, double* dt, double* massr,

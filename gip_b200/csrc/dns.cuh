@@ -55,6 +55,7 @@ struct Dns {
   DevBuf<double> staging;
   long long launches = 0;        // kernels launched (graph launches count their kernels)
   long long graph_kernels = 0;   // kernels in the captured step graph
+  cudaEvent_t* phase_events = nullptr;  // when set: recorded at the step's phase boundaries
   // device-side snapshot of the whole timestep state (checkpoint / resume)
   std::vector<DevBuf<double>*> snap;
   DevBuf<DnsScalars> snap_sc;

@@ -263,6 +263,15 @@ class DnsEngine:
                _hptr(out["outer"]), _hptr(out["kernels"]))
         return out
 
+    PHASES = ("predictor", "poisson_rhs", "pcg", "ghost_copy", "correction", "mass_fluxes",
+              "cfl")
+
+    def step_phases(self, stream=None) -> Dict[str, float]:
+        """Advance one timestep (host-driven loops) and return each GIP_DNS phase's ms."""
+        out = np.zeros(7)
+        L.call("gipb200_dns_step_phases", self.handle, _stream(stream), _hptr(out))
+        return dict(zip(self.PHASES, out.tolist()))
+
     def field(self, name: str) -> np.ndarray:
         n = self.n_faces if name == "mf" else self.n_owned
         out = np.zeros(n)

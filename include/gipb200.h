@@ -238,6 +238,13 @@ int gipb200_dns_advance(gipb200_dns E, int nsteps, void* stream);
 int gipb200_dns_history(gipb200_dns E, int* steps_taken, double* h_time, double* h_dt,
                         double* h_massr, int* h_iters, double* h_rr, int* h_outer,
                         int* h_kernels);
+/* Per-phase timing report (what a GIP_TimerB200 channel per phase would give): advances
+ * one timestep with host-driven loops (no graph) and CUDA events on `stream` between
+ * GIP_DNS's phases, and writes their durations in ms to h_ms[7]: predictor (Ec, D/C
+ * products, AB2; GIP_DNS.h:309-338), Poisson right-hand side (:341-348), PCG, ghost copy
+ * (:350-354), velocity correction (:357-376), mass fluxes (:379-391), massr and CFL
+ * (:394-414).  The step is a real step (state and history advance). */
+int gipb200_dns_step_phases(gipb200_dns E, void* stream, double* h_ms);
 /* Copies a field to the host: "u","v","w","p","p0","mf","ax0","ay0","az0","gpx",... */
 int gipb200_dns_get_field(gipb200_dns E, const char* name, double* h_out, int n);
 /* Copies h_in[0:n) into a field at `offset` on `stream` (no host synchronisation; the

@@ -219,3 +219,20 @@ def test_amg_packed_level0_is_exact(gpu, monkeypatch):
     assert E.history()["iters"].tolist() == P.history()["iters"].tolist()
     for k in ("u", "v", "w", "p"):
         assert np.array_equal(E.field(k), P.field(k)), k
+
+
+def test_step_phases_report_and_advance_like_a_step(gpu):
+    # the per-phase report times a real step: same state as a graph-launched step
+    from gip_b200.device import DnsEngine
+    case, _ = cavity.generate(10, re=400.0)
+    E = DnsEngine(case, gamma=1.0 / 400, pcg_mode="tol", maxit=2000, tol=1e-9)
+    G = DnsEngine(case, gamma=1.0 / 400, pcg_mode="tol", maxit=2000, tol=1e-9)
+    E.advance(2)
+    G.advance(2)
+    ph = E.step_phases()
+    G.advance(1)
+    assert list(ph) == list(DnsEngine.PHASES) and all(v >= 0.0 for v in ph.values())
+    assert ph["pcg"] > 0.0
+    assert len(E.history()["time"]) == 3
+    for k in ("u", "v", "w", "p", "mf"):
+        assert np.array_equal(E.field(k), G.field(k)), k
