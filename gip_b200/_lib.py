@@ -58,7 +58,8 @@ class DnsInfo(C.Structure):
     _fields_ = [("reordered", C.c_int), ("pin_row", C.c_int), ("compressed", C.c_int),
                 ("value_table", C.c_int), ("compressed_fraction", C.c_double),
                 ("slots_L", C.c_longlong), ("nnz_L", C.c_longlong), ("amg_levels", C.c_int),
-                ("amg_complexity", C.c_double), ("amg_setup_s", C.c_double)]
+                ("amg_complexity", C.c_double), ("amg_setup_s", C.c_double),
+                ("iteration_bytes", C.c_double), ("replacement_bytes", C.c_double)]
 
 
 class AdjointParams(C.Structure):

@@ -710,6 +710,25 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
   return GIPB200_OK;
 }
 
+template <typename T>
+double AmgT<T>::cycle_bytes(double a0_stream_bytes) const {
+  const double w = sizeof(T);
+  const int L = (int)lv.size();
+  double b = 0.0;
+  for (int l = 0; l < L - 1; ++l) {
+    const AmgLevel<T>& V = *lv[l];
+    const double n = V.n, nn = lv[l + 1]->n;
+    const double a = l == 0 ? a0_stream_bytes : stream_bytes(V.A);
+    b += 3.0 * n * w;                                    // x = dinv b
+    b += a + 3.0 * n * w;                                // t = b - A x
+    b += stream_bytes(V.R) + (n + nn) * w;               // b_next = R t
+    b += stream_bytes(V.P) + (nn + 2.0 * n) * w;         // x += P x_next
+    b += a + 4.0 * n * w;                                // smoothed x
+  }
+  b += ((double)nc * nc + 2.0 * nc) * w;                 // dense coarsest
+  return b;
+}
+
 template struct AmgT<float>;
 template struct AmgT<double>;
 

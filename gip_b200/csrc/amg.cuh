@@ -67,7 +67,18 @@ struct AmgT {
   // stores r.z in S.
   int enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScratch rs, int first,
               cudaStream_t s, const PackedView* pk = nullptr) const;
+  // Algorithmic bytes of one V-cycle: every operator's stored words once per use and every
+  // vector read or written once per kernel; level 0's operator stream is given (packed or
+  // plain, the caller's operator).
+  double cycle_bytes(double a0_stream_bytes) const;
 };
+
+// Stored bytes one product streams from an AMG operator.
+template <typename T>
+double stream_bytes(const SellT<T>& M) {
+  if (M.lanes > 0) return (double)M.nnz * (4.0 + sizeof(T)) + (M.nrows + 1.0) * 4.0;
+  return (double)M.nslots * (4.0 + sizeof(T)) + (M.nslices + 1.0) * 8.0;
+}
 
 using Amg = AmgT<float>;
 using Amg64 = AmgT<double>;

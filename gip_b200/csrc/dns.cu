@@ -934,6 +934,8 @@ int gipb200_dns_get_info(gipb200_dns Dh, gipb200_dns_info* info) {
   info->amg_levels = amg ? (int)amg->lv.size() : amg64 ? (int)amg64->lv.size() : 0;
   info->amg_complexity = amg ? amg->op_complexity : amg64 ? amg64->op_complexity : 0.0;
   info->amg_setup_s = amg ? amg->setup_s : amg64 ? amg64->setup_s : 0.0;
+  info->iteration_bytes = E.pcg.iteration_bytes();
+  info->replacement_bytes = E.pcg.replacement_bytes();
   return GIPB200_OK;
 }
 

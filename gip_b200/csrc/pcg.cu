@@ -1208,6 +1208,33 @@ int Pcg::build_compressed(cudaStream_t s) {
   return GIPB200_OK;
 }
 
+double Pcg::iteration_bytes() const {
+  const double nn = n, nnz = L->nnz;
+  if (prm.mode == GIPB200_PCG_MIXED) {
+    // plain FP32 operator stream: column + value per slot, slice offsets
+    const double plain = (double)L->nslots * 8.0 + (L->nslices + 1.0) * 8.0;
+    const double spmv = cop.enabled ? cop.bytes_per_launch : plain + 16.0 * nn;
+    double b = spmv + 24.0 * nn;  // SpMV-dot (direction formed inside), y/r update
+    if (amg) b += amg->cycle_bytes(cop.enabled ? cop.bytes_per_launch - 16.0 * nn : plain);
+    return b;
+  }
+  const double spmv = 12.0 * nnz + 16.0 * nn;
+  if (amg64) {  // update (x, r read and written; p, Ap read), cycle, p = z + beta p
+    const double a0 = (double)L->nslots * 12.0 + (L->nslices + 1.0) * 8.0;
+    return spmv + 48.0 * nn + amg64->cycle_bytes(a0) + 24.0 * nn;
+  }
+  return spmv + 56.0 * nn + 32.0 * nn;  // GIP's loop: x, r, z, dots; p = z + beta p
+}
+
+double Pcg::replacement_bytes() const {
+  if (prm.mode != GIPB200_PCG_MIXED) return 0.0;
+  const double nn = n;
+  // FP64 r = b - L x with the FP32 restart (L, x gathered, b, scale read, r^ written) and
+  // the fold x += S y + kappa, y = 0
+  return 12.0 * L->nnz + (L->nslices + 1.0) * 8.0 + 8.0 * n_all + 16.0 * nn + 4.0 * nn +
+         (16.0 + 8.0 + 4.0 + 4.0) * nn;
+}
+
 int Pcg::set_launch(int spmv_blocks, int vec_blocks) {
   if (spmv_blocks < 0 || vec_blocks < 0 || spmv_blocks > kMaxReduceBlocks ||
       vec_blocks > kMaxReduceBlocks)

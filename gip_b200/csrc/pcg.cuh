@@ -79,6 +79,10 @@ struct Pcg {
   std::unique_ptr<Amg64> amg64;
   DevBuf<double> z64;
   int build_amg64(cudaStream_t s);
+  // Algorithmic bytes of one PCG iteration (CG products and updates, plus the V-cycle with
+  // AMG) and of one MIXED residual replacement (FP64 residual and the fold of y into x).
+  double iteration_bytes() const;
+  double replacement_bytes() const;
   int sort_fp32_rows(cudaStream_t s);
   void launch_pcg_update(double* x, cudaStream_t s);
   int build_compressed(cudaStream_t s);

@@ -271,6 +271,8 @@ typedef struct {
   int amg_levels;              /* AMG: levels of the hierarchy (0: no AMG)               */
   double amg_complexity;       /* AMG: operator nonzeros of all levels / of the finest    */
   double amg_setup_s;          /* AMG: host setup time                                   */
+  double iteration_bytes;      /* algorithmic bytes of one PCG iteration (with V-cycle)   */
+  double replacement_bytes;    /* MIXED: bytes of one FP64 residual replacement           */
 } gipb200_dns_info;
 int gipb200_dns_get_info(gipb200_dns E, gipb200_dns_info* info);
 
