@@ -267,7 +267,8 @@ bool dense_inverse(int m, std::vector<double>& M, std::vector<double>& inv) {
 }
 
 template <typename T>
-int upload(const HCsr& A, SellT<T>* S, cudaStream_t s) {
+int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false) {
+  S->half = half;
   GIPB_TRY(validate_csr(A.nr, A.nc, (int)A.nnz(), A.rp.data(), A.ci.data(), A.nc, "AMG operator"));
   S->nrows = A.nr;
   S->ncols = A.nc;
@@ -276,11 +277,17 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s) {
   const double avg = (double)A.nnz() / std::max(A.nr, 1);
   if (avg >= 12.0) {  // long rows: CSR, 8 to 32 threads per row
     S->lanes = avg >= 48.0 ? 32 : avg >= 24.0 ? 16 : 8;
-    std::vector<T> val(A.v.size());
-    for (size_t k = 0; k < A.v.size(); ++k) val[k] = (T)A.v[k];
     GIPB_TRY(S->rp.upload(A.rp.data(), A.rp.size(), s));
     GIPB_TRY(S->col.upload(A.ci.data(), std::max<size_t>(A.ci.size(), 1), s));
-    GIPB_TRY(S->val.upload(val.data(), std::max<size_t>(val.size(), 1), s));
+    if (half) {
+      std::vector<__half> hv(std::max<size_t>(A.v.size(), 1), __float2half_rn(0.0f));
+      for (size_t k = 0; k < A.v.size(); ++k) hv[k] = __float2half_rn((float)A.v[k]);
+      GIPB_TRY(S->hval.upload(hv.data(), hv.size(), s));
+    } else {
+      std::vector<T> val(std::max<size_t>(A.v.size(), 1), T(0));
+      for (size_t k = 0; k < A.v.size(); ++k) val[k] = (T)A.v[k];
+      GIPB_TRY(S->val.upload(val.data(), val.size(), s));
+    }
     GIPB_CUDA(cudaStreamSynchronize(s));
     return GIPB200_OK;
   }
@@ -305,7 +312,13 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s) {
   }
   GIPB_TRY(S->sptr.upload(sptr.data(), sptr.size(), s));
   GIPB_TRY(S->col.upload(col.data(), col.size(), s));
-  GIPB_TRY(S->val.upload(val.data(), val.size(), s));
+  if (half) {
+    std::vector<__half> hv(val.size());
+    for (size_t k = 0; k < val.size(); ++k) hv[k] = __float2half_rn((float)val[k]);
+    GIPB_TRY(S->hval.upload(hv.data(), hv.size(), s));
+  } else {
+    GIPB_TRY(S->val.upload(val.data(), val.size(), s));
+  }
   GIPB_CUDA(cudaStreamSynchronize(s));  // host staging goes out of scope
   return GIPB200_OK;
 }
@@ -320,13 +333,18 @@ __device__ __forceinline__ bool amg_enter(PcgScalars* S) {
 __device__ __forceinline__ float fmat(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ double fmat(double a, double b, double c) { return fma(a, b, c); }
 
+// Stored operator values to the arithmetic type (FP16-stored transfer operators).
+__device__ __forceinline__ float to_arith(__half v) { return __half2float(v); }
+__device__ __forceinline__ float to_arith(float v) { return v; }
+__device__ __forceinline__ double to_arith(double v) { return v; }
+
 // One row of a sliced operator, summed slot by slot (padding: column -1, skipped).
-template <typename T, int CH>
-__device__ __forceinline__ T amg_row(const SellView<T>& A, const T* __restrict__ x, int s, int lane) {
+template <typename T, int CH, typename V = T>
+__device__ __forceinline__ T amg_row(const SellView<V>& A, const T* __restrict__ x, int s, int lane) {
   const long long base = A.sptr[s];
   const int len = (int)((A.sptr[s + 1] - base) >> 5);
   const int* cp = A.col + base + lane;
-  const T* vp = A.val + base + lane;
+  const V* vp = A.val + base + lane;
   T sum = T(0);
   for (int j0 = 0; j0 < len; j0 += CH) {
     int c[CH];
@@ -334,7 +352,7 @@ __device__ __forceinline__ T amg_row(const SellView<T>& A, const T* __restrict__
 #pragma unroll
     for (int t = 0; t < CH; ++t) {
       c[t] = (j0 + t < len) ? ld_stream(cp + (size_t)(j0 + t) * 32) : -1;
-      v[t] = (j0 + t < len) ? ld_stream(vp + (size_t)(j0 + t) * 32) : T(0);
+      v[t] = (j0 + t < len) ? (T)to_arith(ld_stream(vp + (size_t)(j0 + t) * 32)) : T(0);
     }
     T xv[CH];
 #pragma unroll
@@ -357,8 +375,8 @@ __global__ void __launch_bounds__(256) k_amg_jacobi0(int n, const T* __restrict_
 
 enum { kResid = 0, kPlain = 1, kAdd = 2, kSmooth = 3 };
 // kResid: y = b - A x;  kPlain: y = A x;  kAdd: y += A x;  kSmooth: y = x + dinv (b - A x)
-template <typename T, int MODE>
-__global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<T> A, const T* __restrict__ x,
+template <typename T, int MODE, typename V = T>
+__global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __restrict__ x,
                                                      const T* __restrict__ b,
                                                      const T* __restrict__ dinv,
                                                      T* __restrict__ y, PcgScalars* S) {
@@ -367,7 +385,7 @@ __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<T> A, const T* __r
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int s = gw; s < A.nslices; s += nw) {
-    const T sum = amg_row<T, 4>(A, x, s, lane);
+    const T sum = amg_row<T, 4, V>(A, x, s, lane);
     const int i = s * 32 + lane;
     if (i < A.nrows) {
       if (MODE == kResid) y[i] = b[i] - sum;
@@ -382,10 +400,10 @@ __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<T> A, const T* __r
 // of the row, combined by a fixed shuffle tree (deterministic).  The row loop is uniform
 // across the warp (32 / LANES rows per warp per pass), so every lane takes part in the
 // shuffles.
-template <typename T, int MODE, int LANES>
+template <typename T, int MODE, int LANES, typename V = T>
 __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restrict__ rp,
                                                  const int* __restrict__ col,
-                                                 const T* __restrict__ val, const T* __restrict__ x,
+                                                 const V* __restrict__ val, const T* __restrict__ x,
                                                  const T* __restrict__ b,
                                                  const T* __restrict__ dinv, T* __restrict__ y,
                                                  PcgScalars* S) {
@@ -398,7 +416,8 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
     const int i = r0 + lane / LANES;
     T sum = T(0);
     if (i < nrows)
-      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES) sum = fmat(ld_stream(val + k), __ldg(x + ld_stream(col + k)), sum);
+      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES)
+        sum = fmat((T)to_arith(ld_stream(val + k)), __ldg(x + ld_stream(col + k)), sum);
 #pragma unroll
     for (int o = LANES / 2; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o, LANES);
     if (i < nrows && sub == 0) {
@@ -413,23 +432,34 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
 int vec_blocks(int n);
 
 // y (mode) A x for an AMG operator in either form.
-template <typename T, int MODE>
-void amg_mv(const SellT<T>& M, const T* x, const T* b, const T* dinv, T* y, PcgScalars* S,
-            cudaStream_t s) {
+template <typename T, int MODE, typename V>
+void amg_mv_v(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const T* b,
+              const T* dinv, T* y, PcgScalars* S, cudaStream_t s) {
   if (M.lanes == 0) {
-    k_amg_spmv<T, MODE><<<vec_blocks(M.nslices * 32), 256, 0, s>>>(M.view(), x, b, dinv, y, S);
+    k_amg_spmv<T, MODE, V><<<vec_blocks(M.nslices * 32), 256, 0, s>>>(view, x, b, dinv, y, S);
     return;
   }
   const int nb = vec_blocks((int)std::min<long long>((long long)M.nrows * M.lanes, 1LL << 30));
   const int* rp = M.rp.p;
   const int* ci = M.col.p;
-  const T* v = M.val.p;
   if (M.lanes == 32)
-    k_amg_csr<T, MODE, 32><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
+    k_amg_csr<T, MODE, 32, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
   else if (M.lanes == 16)
-    k_amg_csr<T, MODE, 16><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
+    k_amg_csr<T, MODE, 16, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
   else
-    k_amg_csr<T, MODE, 8><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
+    k_amg_csr<T, MODE, 8, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
+}
+
+template <typename T, int MODE>
+void amg_mv(const SellT<T>& M, const T* x, const T* b, const T* dinv, T* y, PcgScalars* S,
+            cudaStream_t s) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (M.half) {
+      amg_mv_v<T, MODE, __half>(M, M.hview(), M.hval.p, x, b, dinv, y, S, s);
+      return;
+    }
+  }
+  amg_mv_v<T, MODE, T>(M, M.view(), M.val.p, x, b, dinv, y, S, s);
 }
 
 struct CycleFinish {
@@ -654,8 +684,11 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
     HCsr AP, Ac;
     GIPB_TRY(spgemm(A, P, AP));
     GIPB_TRY(spgemm(R, AP, Ac));
-    GIPB_TRY(upload(P, &L.P, s));
-    GIPB_TRY(upload(R, &L.R, s));
+    // the FP32 cycle keeps its transfer operators in FP16 (R = P^T still holds exactly:
+    // both round the same values), halving their value stream
+    const bool half = std::is_same<T, float>::value;
+    GIPB_TRY(upload(P, &L.P, s, half));
+    GIPB_TRY(upload(R, &L.R, s, half));
     lv.push_back(std::move(Lp));
     A = std::move(Ac);
     z = nrm;

@@ -2,6 +2,8 @@
 // the mixed form's inner CG (an addition beyond GIP, whose solver is Jacobi-PCG).
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include <memory>
 #include <vector>
 
@@ -23,7 +25,10 @@ struct SellT {
   DevBuf<T> val;
   int lanes = 0;               // > 0: CSR form (rp, col, val) with this many threads per row
   DevBuf<int> rp;
+  bool half = false;           // values stored in FP16 (hval) instead of T (val)
+  DevBuf<__half> hval;
   SellView<T> view() const { return {nrows, nslices, sptr.p, col.p, val.p}; }
+  SellView<__half> hview() const { return {nrows, nslices, sptr.p, col.p, hval.p}; }
 };
 
 // The mixed form's packed FP32 operator (see CompressedOp), for the V-cycle's level-0
@@ -76,8 +81,9 @@ struct AmgT {
 // Stored bytes one product streams from an AMG operator.
 template <typename T>
 double stream_bytes(const SellT<T>& M) {
-  if (M.lanes > 0) return (double)M.nnz * (4.0 + sizeof(T)) + (M.nrows + 1.0) * 4.0;
-  return (double)M.nslots * (4.0 + sizeof(T)) + (M.nslices + 1.0) * 8.0;
+  const double w = M.half ? 2.0 : (double)sizeof(T);
+  if (M.lanes > 0) return (double)M.nnz * (4.0 + w) + (M.nrows + 1.0) * 4.0;
+  return (double)M.nslots * (4.0 + w) + (M.nslices + 1.0) * 8.0;
 }
 
 using Amg = AmgT<float>;
