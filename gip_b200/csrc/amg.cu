@@ -10,7 +10,8 @@
 //   P0         tentative prolongator: P0[i, agg(i)] = z_i / |z restricted to agg(i)|
 //   P          smoothed: (I - w D^-1 A) P0, w = 4 / (3 rho), rho = the Gershgorin bound of
 //              D^-1 A; coarse near-null vector = the aggregate norms (so P z_c = z)
-//   A_c        Galerkin: R A P with R = P^T
+//   A_c        Galerkin: R A P with R = P^T, then sparsified: couplings below
+//              kDrop sqrt(a_ii a_jj) lumped onto the diagonal along z (A_c z unchanged)
 // The coarsest level (<= kCoarse unknowns) is inverted densely; for the pinned-Neumann
 // inner system (A z = 0) the inverse is taken of A + sigma z z^T / |z|^2, which solves
 // consistent right-hand sides exactly.
@@ -20,6 +21,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <type_traits>
 
 #include "amg.cuh"
@@ -33,6 +35,7 @@ namespace {
 constexpr int kCoarse = 1024;    // largest level inverted densely
 constexpr int kMaxLevels = 16;
 constexpr double kTheta = 0.0;   // strength threshold: every nonzero coupling is strong
+constexpr double kDrop = 0.02;   // coarse-operator drop threshold (sparsify); env GIPB200_AMG_DROP
 
 struct HCsr {
   int nr = 0, nc = 0;
@@ -179,6 +182,72 @@ HCsr transpose(const HCsr& A) {
       T.v[o] = A.v[k];
     }
   return T;
+}
+
+// Sparsified coarse operator (non-Galerkin): off-diagonal couplings with
+// |a_ij| < theta sqrt(a_ii a_jj) are dropped and lumped onto the diagonal weighted by the
+// near-null vector, a_ii += a_ij z_j / z_i, so that A z is unchanged.  The values are made
+// exactly symmetric first ((A + A^T) / 2 on the common pattern), so the decision and the
+// result are symmetric; a row or column whose z entry is 0 keeps its couplings.  Returns
+// false, leaving A as it was, when A's pattern is not symmetric or a diagonal is missing.
+bool sparsify(HCsr& A, const std::vector<double>& z, double theta) {
+  const int n = A.nr;
+  if (A.nc != n) return false;
+  HCsr S = A;
+#pragma omp parallel
+  {
+    std::vector<std::pair<int, double>> e;
+#pragma omp for schedule(static)
+    for (int i = 0; i < n; ++i) {  // columns in increasing order, as the transpose has them
+      e.clear();
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) e.emplace_back(A.ci[k], A.v[k]);
+      std::sort(e.begin(), e.end(),
+                [](const std::pair<int, double>& a, const std::pair<int, double>& b) {
+                  return a.first < b.first;
+                });
+      for (size_t q = 0; q < e.size(); ++q) {
+        S.ci[A.rp[i] + q] = e[q].first;
+        S.v[A.rp[i] + q] = e[q].second;
+      }
+    }
+  }
+  const HCsr T = transpose(S);
+  if (T.rp != S.rp || T.ci != S.ci) return false;
+  std::vector<double> d((size_t)n, 0.0);
+  std::vector<int> dk((size_t)n, -1);
+  for (int i = 0; i < n; ++i)
+    for (int k = S.rp[i]; k < S.rp[i + 1]; ++k) {
+      S.v[k] = 0.5 * (S.v[k] + T.v[k]);
+      if (S.ci[k] == i) dk[i] = k;
+    }
+  for (int i = 0; i < n; ++i) {
+    if (dk[i] < 0 || !(S.v[dk[i]] > 0.0)) return false;
+    d[i] = S.v[dk[i]];
+  }
+  HCsr O;
+  O.nr = O.nc = n;
+  O.rp.assign((size_t)n + 1, 0);
+  O.ci.reserve(S.ci.size());
+  O.v.reserve(S.v.size());
+  for (int i = 0; i < n; ++i) {
+    double lump = 0.0;
+    int diag_at = -1;
+    for (int k = S.rp[i]; k < S.rp[i + 1]; ++k) {
+      const int j = S.ci[k];
+      const double a = S.v[k];
+      if (j != i && z[i] != 0.0 && z[j] != 0.0 && std::fabs(a) < theta * std::sqrt(d[i] * d[j])) {
+        lump += a * z[j] / z[i];
+        continue;
+      }
+      if (j == i) diag_at = (int)O.ci.size();
+      O.ci.push_back(j);
+      O.v.push_back(a);
+    }
+    O.v[diag_at] += lump;
+    O.rp[i + 1] = (int)O.ci.size();
+  }
+  A = std::move(O);
+  return true;
 }
 
 // Smoothed prolongator (I - w D^-1 A) P0 with P0[i, agg(i)] = p0[i].
@@ -627,6 +696,8 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
   A.v.assign(v, v + rp[n]);
   std::vector<double> z(z0, z0 + n);
   lv.clear();
+  double drop = kDrop;
+  if (const char* e = getenv("GIPB200_AMG_DROP")) drop = atof(e);
   const double nnz0 = (double)A.nnz();
   double nnz_all = 0.0;
   for (int l = 0; l < kMaxLevels; ++l) {
@@ -684,6 +755,7 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
     HCsr AP, Ac;
     GIPB_TRY(spgemm(A, P, AP));
     GIPB_TRY(spgemm(R, AP, Ac));
+    if (drop > 0.0) sparsify(Ac, nrm, drop);
     // the FP32 cycle keeps its transfer operators in FP16 (R = P^T still holds exactly:
     // both round the same values), halving their value stream
     const bool half = std::is_same<T, float>::value;

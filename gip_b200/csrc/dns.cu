@@ -9,7 +9,9 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cmath>
 #include <string>
+#include <vector>
 
 #include "device.cuh"
 #include "dns.cuh"
@@ -210,6 +212,17 @@ __global__ void __launch_bounds__(256) k_dns_massflux(
   }
 }
 
+// ------------------------------------------------------------------ phase stamps
+// Device time at phase boundary `mark` of the current step (the one-thread kernel runs
+// after the previous phase's kernels and before the next phase's).  The boundary after the
+// CFL kernel, which has already advanced the step counter, belongs to the step before.
+__global__ void k_dns_stamp(const DnsScalars* __restrict__ S, DnsHistory H, int mark) {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  const int k = S->step - (mark == kPhaseMarks - 1 ? 1 : 0);
+  if (k >= 0 && k < H.capacity) H.stamps[(size_t)k * kPhaseMarks + mark] = t;
+}
+
 // ------------------------------------------------------------------ CFLCondition
 struct MassrFinish {
   const DnsScalars* S;
@@ -289,8 +302,8 @@ struct CflStepFinish {
         // the step's 10 kernels and the PCG's: init + 3 per iteration in the FP64 forms
         // (2 with AMG, whose V-cycle and direction kernels count themselves on the device),
         // all counted on the device in the mixed form
-        H.kernels[k] = 10 + (pcg_mixed ? P->kernels
-                                       : 1 + (P->kernels ? 2 : 3) * P->iter + P->kernels);
+        H.kernels[k] = 10 + H.stamp_kernels +
+                       (pcg_mixed ? P->kernels : 1 + (P->kernels ? 2 : 3) * P->iter + P->kernels);
       }
       S->step = k + 1;
     }
@@ -320,6 +333,9 @@ int Dns::grow_history(int need, cudaStream_t s) {
   int cap = std::max(need, std::max(1024, capacity * 2));
   DevBuf<double> t, d, m, r;
   DevBuf<int> it, ou, kn;
+  DevBuf<unsigned long long> st;
+  GIPB_TRY(st.alloc((size_t)cap * kPhaseMarks));
+  GIPB_CUDA(cudaMemsetAsync(st.p, 0, (size_t)cap * kPhaseMarks * 8, s));
   GIPB_TRY(ou.alloc(cap));
   GIPB_TRY(kn.alloc(cap));
   GIPB_TRY(t.alloc(cap));
@@ -335,8 +351,10 @@ int Dns::grow_history(int need, cudaStream_t s) {
     GIPB_CUDA(cudaMemcpyAsync(it.p, h_iters.p, capacity * 4, cudaMemcpyDeviceToDevice, s));
     GIPB_CUDA(cudaMemcpyAsync(ou.p, h_outer.p, capacity * 4, cudaMemcpyDeviceToDevice, s));
     GIPB_CUDA(cudaMemcpyAsync(kn.p, h_kernels.p, capacity * 4, cudaMemcpyDeviceToDevice, s));
-    GIPB_CUDA(cudaStreamSynchronize(s));
+    GIPB_CUDA(cudaMemcpyAsync(st.p, h_stamps.p, (size_t)capacity * kPhaseMarks * 8,
+                              cudaMemcpyDeviceToDevice, s));
   }
+  GIPB_CUDA(cudaStreamSynchronize(s));
   std::swap(h_time.p, t.p);
   std::swap(h_dt.p, d.p);
   std::swap(h_massr.p, m.p);
@@ -344,18 +362,13 @@ int Dns::grow_history(int need, cudaStream_t s) {
   std::swap(h_iters.p, it.p);
   std::swap(h_outer.p, ou.p);
   std::swap(h_kernels.p, kn.p);
+  std::swap(h_stamps.p, st.p);
   h_time.n = h_dt.n = h_massr.n = h_rr.n = h_iters.n = h_outer.n = h_kernels.n = cap;
   t.n = d.n = m.n = r.n = it.n = ou.n = kn.n = capacity;
+  h_stamps.n = (size_t)cap * kPhaseMarks;
+  st.n = (size_t)capacity * kPhaseMarks;
   capacity = cap;
-  // a captured graph refers to the old history arrays
-  if (exec) {
-    cudaGraphExecDestroy(exec);
-    exec = nullptr;
-  }
-  if (graph) {
-    cudaGraphDestroy(graph);
-    graph = nullptr;
-  }
+  drop_graph();  // a captured graph refers to the old history arrays
   return GIPB200_OK;
 }
 
@@ -372,6 +385,7 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync) {
   const long long pcg_before = pcg.launches;
   auto mark = [&](int k) {
     if (phase_events) cudaEventRecord(phase_events[k], s);
+    if (stamps_on) k_dns_stamp<<<1, 1, 0, s>>>(sc.p, H, k);
   };
   mark(0);
   // PredictorVelocity: C's values from the face fluxes, then D/C products and AB2
@@ -406,7 +420,8 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync) {
                                         dt_seq_len, rs);
   GIPB_LAUNCH_CHECK();
   mark(7);
-  launches += 10 + (pcg.launches - pcg_before);
+  GIPB_LAUNCH_CHECK();
+  launches += 10 + H.stamp_kernels + (pcg.launches - pcg_before);
   return GIPB200_OK;
 }
 
@@ -807,6 +822,38 @@ int gipb200_dns_step_phases(gipb200_dns Dh, void* stream, double* h_ms) {
   }
   for (int k = 0; k < made; ++k) cudaEventDestroy(ev[k]);
   return st;
+}
+
+int gipb200_dns_phase_stamps(gipb200_dns Dh, int on) {
+  if (!Dh) return fail(GIPB200_ERR_ARG, "null engine");
+  Dns& E = Dh->E;
+  if (E.stamps_on != (on != 0)) {
+    GIPB_CUDA(cudaDeviceSynchronize());  // a launched graph may still run
+    E.stamps_on = on != 0;
+    E.drop_graph();  // the next advance captures the step with (or without) the stamps
+  }
+  return GIPB200_OK;
+}
+
+int gipb200_dns_phase_history(gipb200_dns Dh, int max_steps, double* h_ms, int* steps_out) {
+  if (!Dh || max_steps < 0 || (max_steps > 0 && !h_ms)) return fail(GIPB200_ERR_ARG, "bad arguments");
+  Dns& E = Dh->E;
+  GIPB_CUDA(cudaDeviceSynchronize());
+  DnsScalars S;
+  GIPB_CUDA(cudaMemcpy(&S, E.sc.p, sizeof(S), cudaMemcpyDeviceToHost));
+  const int n = std::min(std::min(S.step, E.capacity), max_steps);
+  if (steps_out) *steps_out = n;
+  if (n <= 0) return GIPB200_OK;
+  std::vector<unsigned long long> st((size_t)n * kPhaseMarks);
+  GIPB_CUDA(cudaMemcpy(st.data(), E.h_stamps.p, st.size() * 8, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < n; ++k)
+    for (int ph = 0; ph < kPhaseMarks - 1; ++ph) {
+      const unsigned long long a = st[(size_t)k * kPhaseMarks + ph];
+      const unsigned long long b = st[(size_t)k * kPhaseMarks + ph + 1];
+      h_ms[(size_t)k * (kPhaseMarks - 1) + ph] =
+          (a && b && b >= a) ? (double)(b - a) * 1e-6 : std::nan("");
+    }
+  return GIPB200_OK;
 }
 
 int gipb200_dns_history(gipb200_dns Dh, int* steps, double* t, double* dt, double* massr,

@@ -22,8 +22,13 @@ struct DnsHistory {
   double* rr;
   int* outer;
   int* kernels;  // kernels the step launched (early exits included)
+  unsigned long long* stamps;  // kPhaseMarks device times per step (phase stamps on)
   int capacity;
+  int stamp_kernels;  // phase-stamp kernels each step adds (0 when stamps are off)
 };
+
+// Device timestamps at the step's 8 phase boundaries (kPhaseMarks per step, ns).
+constexpr int kPhaseMarks = 8;
 
 struct Dns {
   int N = 0, NO = 0, NF = 0;
@@ -35,6 +40,8 @@ struct Dns {
   DevBuf<DnsScalars> sc;
   DevBuf<double> h_time, h_dt, h_massr, h_rr;
   DevBuf<int> h_iters, h_outer, h_kernels;
+  DevBuf<unsigned long long> h_stamps;  // capacity x kPhaseMarks, 0 = not recorded
+  bool stamps_on = false;               // stamp the phase boundaries on the device
   int capacity = 0;
   DevBuf<double> partials;
   DevBuf<unsigned> ticket;
@@ -71,7 +78,15 @@ struct Dns {
     if (cap_stream) cudaStreamDestroy(cap_stream);
   }
   DnsHistory history() const {
-    return {h_time.p, h_dt.p, h_massr.p, h_iters.p, h_rr.p, h_outer.p, h_kernels.p, capacity};
+    return {h_time.p,    h_dt.p,     h_massr.p, h_iters.p,
+            h_rr.p,      h_outer.p,  h_kernels.p, h_stamps.p,
+            capacity,    stamps_on ? kPhaseMarks : 0};
+  }
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
   }
   int grow_history(int need, cudaStream_t s);
   int enqueue_step(cudaStream_t s, bool host_sync);

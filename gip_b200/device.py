@@ -272,6 +272,21 @@ class DnsEngine:
         L.call("gipb200_dns_step_phases", self.handle, _stream(stream), _hptr(out))
         return dict(zip(self.PHASES, out.tolist()))
 
+    def phase_stamps(self, on: bool = True) -> None:
+        """Stamp the device clock at every step's phase boundaries (graph steps included)."""
+        L.call("gipb200_dns_phase_stamps", self.handle, int(bool(on)))
+
+    def phase_history(self) -> Dict[str, np.ndarray]:
+        """Per-step phase durations in ms (NaN for steps taken with stamps off)."""
+        steps = C.c_int()
+        L.call("gipb200_dns_history", self.handle, C.byref(steps), None, None, None, None, None,
+               None, None)
+        out = np.zeros((steps.value, 7))
+        got = C.c_int()
+        L.call("gipb200_dns_phase_history", self.handle, steps.value, _hptr(out), C.byref(got))
+        out = out[:got.value]
+        return {name: out[:, k].copy() for k, name in enumerate(self.PHASES)}
+
     def field(self, name: str) -> np.ndarray:
         n = self.n_faces if name == "mf" else self.n_owned
         out = np.zeros(n)

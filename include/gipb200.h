@@ -245,6 +245,16 @@ int gipb200_dns_history(gipb200_dns E, int* steps_taken, double* h_time, double*
  * (:350-354), velocity correction (:357-376), mass fluxes (:379-391), massr and CFL
  * (:394-414).  The step is a real step (state and history advance). */
 int gipb200_dns_step_phases(gipb200_dns E, void* stream, double* h_ms);
+/* Per-phase timing of every step, graph-launched steps included (GIP_Timer channels per
+ * phase, src/AbstractInterfaces/GIP_Timer.h, kept on the device): with `on` set, each
+ * step also launches 8 one-thread kernels that store the device clock (%globaltimer, ns)
+ * at the phase boundaries of gipb200_dns_step_phases; the captured step graph is rebuilt
+ * at the next advance.  Off by default. */
+int gipb200_dns_phase_stamps(gipb200_dns E, int on);
+/* The 7 phase durations (ms, same order as gipb200_dns_step_phases) of the first
+ * min(steps taken, max_steps) steps into h_ms[step * 7 + phase]; NaN for steps taken
+ * with stamps off.  *steps_out (may be NULL) = steps written.  Synchronises the device. */
+int gipb200_dns_phase_history(gipb200_dns E, int max_steps, double* h_ms, int* steps_out);
 /* Copies a field to the host: "u","v","w","p","p0","mf","ax0","ay0","az0","gpx",... */
 int gipb200_dns_get_field(gipb200_dns E, const char* name, double* h_out, int n);
 /* Copies h_in[0:n) into a field at `offset` on `stream` (no host synchronisation; the

@@ -236,3 +236,39 @@ def test_step_phases_report_and_advance_like_a_step(gpu):
     assert len(E.history()["time"]) == 3
     for k in ("u", "v", "w", "p", "mf"):
         assert np.array_equal(E.field(k), G.field(k)), k
+
+
+@pytest.mark.parametrize("mode", ["fixed", "mixed"])
+def test_phase_stamps_time_graph_steps_without_changing_them(gpu, mode):
+    # device clock stamps at the phase boundaries of graph-launched steps: 8 more kernels
+    # per step, identical fields, and one finite duration per phase for stamped steps only
+    from gip_b200.device import DnsEngine
+    case, _ = cavity.generate(10, re=400.0)
+    # FIXED runs exactly maxit iterations: GIP's 100 (far more would run past convergence)
+    kw = dict(gamma=1.0 / 400, pcg_mode=mode, maxit=100 if mode == "fixed" else 2000, tol=1e-9,
+              inner_tol=0.01, max_outer=50, use_graph=True)
+    E = DnsEngine(case, **kw)
+    G = DnsEngine(case, **kw)
+    E.advance(2)
+    G.advance(2)
+    E.phase_stamps(True)
+    E.advance(3)
+    G.advance(3)
+    hE, hG = E.history(), G.history()
+    assert hE["iters"].tolist() == hG["iters"].tolist()
+    assert (hE["kernels"][2:] - hG["kernels"][2:]).tolist() == [8, 8, 8]
+    assert hE["kernels"][:2].tolist() == hG["kernels"][:2].tolist()
+    for k in ("u", "v", "w", "p", "mf"):
+        assert np.isfinite(G.field(k)).all() and np.array_equal(E.field(k), G.field(k)), k
+    ph = E.phase_history()
+    assert list(ph) == list(DnsEngine.PHASES)
+    for name, v in ph.items():
+        assert v.shape == (5,), name
+        assert np.isnan(v[:2]).all(), name
+        assert np.isfinite(v[2:]).all() and (v[2:] >= 0).all(), name
+    assert (ph["pcg"][2:] > 0).all()
+    E.phase_stamps(False)
+    E.advance(1)
+    G.advance(1)
+    ph = E.phase_history()
+    assert np.isnan(ph["pcg"][5]) and E.history()["kernels"][5] == G.history()["kernels"][5]
