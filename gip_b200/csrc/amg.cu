@@ -188,8 +188,9 @@ HCsr transpose(const HCsr& A) {
 // |a_ij| < theta sqrt(a_ii a_jj) are dropped and lumped onto the diagonal weighted by the
 // near-null vector, a_ii += a_ij z_j / z_i, so that A z is unchanged.  The values are made
 // exactly symmetric first ((A + A^T) / 2 on the common pattern), so the decision and the
-// result are symmetric; a row or column whose z entry is 0 keeps its couplings.  Returns
-// false, leaving A as it was, when A's pattern is not symmetric or a diagonal is missing.
+// result are symmetric; a row or column whose z entry is 0 keeps its couplings, and so
+// does a row whose diagonal would lose more than half.  Returns false, leaving A as it
+// was, when A's pattern is not symmetric or a diagonal is missing or not positive.
 bool sparsify(HCsr& A, const std::vector<double>& z, double theta) {
   const int n = A.nr;
   if (A.nc != n) return false;
@@ -224,6 +225,23 @@ bool sparsify(HCsr& A, const std::vector<double>& z, double theta) {
     if (dk[i] < 0 || !(S.v[dk[i]] > 0.0)) return false;
     d[i] = S.v[dk[i]];
   }
+  // A row whose diagonal would lose more than half to the lumping keeps its couplings,
+  // and so do its partners' entries for it (a coupling goes only when both rows let it go)
+  std::vector<char> keep_row((size_t)n, 0);
+  auto droppable = [&](int i, int j, double a) {
+    return j != i && z[i] != 0.0 && z[j] != 0.0 && !keep_row[i] && !keep_row[j] &&
+           std::fabs(a) < theta * std::sqrt(d[i] * d[j]);
+  };
+  auto lumped = [&](int i) {
+    double lump = 0.0;
+    for (int k = S.rp[i]; k < S.rp[i + 1]; ++k)
+      if (droppable(i, S.ci[k], S.v[k])) lump += S.v[k] * z[S.ci[k]] / z[i];
+    return lump;
+  };
+  for (int i = 0; i < n; ++i)
+    if (!(d[i] + lumped(i) > 0.5 * d[i])) keep_row[i] = 1;
+  for (int i = 0; i < n; ++i)  // fewer drops can move a lump either way: check again
+    if (!keep_row[i] && !(d[i] + lumped(i) > 0.5 * d[i])) return false;
   HCsr O;
   O.nr = O.nc = n;
   O.rp.assign((size_t)n + 1, 0);
@@ -235,7 +253,7 @@ bool sparsify(HCsr& A, const std::vector<double>& z, double theta) {
     for (int k = S.rp[i]; k < S.rp[i + 1]; ++k) {
       const int j = S.ci[k];
       const double a = S.v[k];
-      if (j != i && z[i] != 0.0 && z[j] != 0.0 && std::fabs(a) < theta * std::sqrt(d[i] * d[j])) {
+      if (droppable(i, j, a)) {
         lump += a * z[j] / z[i];
         continue;
       }

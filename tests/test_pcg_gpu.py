@@ -193,6 +193,28 @@ def test_mixed_amg_preconditioner(gpu, oracle_mod, n, tol):
     assert np.abs(xs - xr).max() / np.abs(xr).max() < 1e4 * tol
 
 
+def test_amg_coarse_sparsification_thresholds(gpu, monkeypatch):
+    # coarse operators lose their weak couplings (lumped onto the diagonal): fewer stored
+    # nonzeros at the default threshold, and a large threshold still builds (rows whose
+    # diagonal would lose more than half keep their couplings) and converges (its sparser
+    # level 1 aggregates into more, denser levels below, so complexity is not monotone)
+    from gip_b200 import device as dv
+    L, b = cavity.poisson_problem(40, seed=7)
+    A = dv.DeviceMatrix(L)
+    cx = {}
+    for th in ("0", "0.02", "0.1"):
+        monkeypatch.setenv("GIPB200_AMG_DROP", th)
+        S = dv.PcgSolver(A, mode="mixed", maxit=2000, tol=1e-8, inner_tol=1e-3, max_outer=100,
+                         precond="amg")
+        cx[th] = S.info()["amg_complexity"]
+        x = _t(np.zeros(L.nrows))
+        res = S.solve(_t(b), x, _t(np.zeros(L.nrows)))
+        assert res["status"] == 0 and res["iterations"] < 200, (th, res)
+        xs = x.cpu().numpy()
+        assert np.linalg.norm(b - L.to_scipy() @ xs) <= 1e-8 * np.linalg.norm(b) * 1.0001, th
+    assert cx["0.02"] < cx["0"], cx
+
+
 def test_fp64_amg_preconditioner_and_fixed_mode_refusal(gpu, oracle_mod):
     # FP64 tolerance mode with the FP64 V-cycle; FIXED mode (GIP's) keeps GIP's Jacobi
     from gip_b200 import _lib
