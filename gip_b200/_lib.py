@@ -131,6 +131,8 @@ _SIGNATURES = {
     "gipb200_dns_history": (_I, [_VP, C.POINTER(_I), _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "gipb200_dns_step_phases": (_I, [_VP, _VP, _VP]),
     "gipb200_dns_phase_stamps": (_I, [_VP, _I]),
+    "gipb200_amg_host_levels": (_I, [_I, _VP, _VP, _VP, _VP, _I, C.c_double, _I, C.POINTER(_I),
+                                     _VP, _VP, _VP]),
     "gipb200_dns_phase_history": (_I, [_VP, _I, _VP, C.POINTER(_I)]),
     "gipb200_dns_get_field": (_I, [_VP, C.c_char_p, _VP, _I]),
     "gipb200_dns_field_ptr": (_I, [_VP, C.c_char_p, C.POINTER(_VP), C.POINTER(_I)]),

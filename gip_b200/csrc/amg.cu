@@ -703,41 +703,41 @@ void launch_packed0(const PackedView& pk, SellView<T> A, int nb, const T* x, con
     launch_amgp<MODE>(pk, A, nb, x, b, dinv, y, S, rs, first, s);
 }
 
-template <typename T>
-int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const double* z0,
-                   bool singular, int x0_len, cudaStream_t s) {
-  const auto t0 = std::chrono::steady_clock::now();
+namespace {
+
+// One level of the host hierarchy, handed to the consumer as soon as it is built.
+struct HostLevel {
+  int l = 0;
+  const HCsr* A = nullptr;                 // the level's operator
+  const std::vector<double>* d = nullptr;  // its diagonal
+  const std::vector<double>* z = nullptr;  // its near-null vector
+  double w = 0.0;                          // Jacobi weight 4 / (3 rho)
+  const HCsr* P = nullptr;                 // prolongation / restriction (not on the coarsest)
+  const HCsr* R = nullptr;
+  const std::vector<double>* cinv = nullptr;  // coarsest only: dense (pseudo-)inverse
+};
+
+// The smoothed-aggregation hierarchy of the n x n operator (host CSR, FP64), built on the
+// host level by level; emit(const HostLevel&) consumes each level (returns a status).
+template <typename F>
+int host_hierarchy(int n, const int* rp, const int* ci, const double* v, const double* z0,
+                   bool singular, double drop, F&& emit) {
   HCsr A;
   A.nr = A.nc = n;
   A.rp.assign(rp, rp + n + 1);
   A.ci.assign(ci, ci + rp[n]);
   A.v.assign(v, v + rp[n]);
   std::vector<double> z(z0, z0 + n);
-  lv.clear();
-  double drop = kDrop;
-  if (const char* e = getenv("GIPB200_AMG_DROP")) drop = atof(e);
-  const double nnz0 = (double)A.nnz();
-  double nnz_all = 0.0;
   for (int l = 0; l < kMaxLevels; ++l) {
-    std::unique_ptr<AmgLevel<T>> Lp(new AmgLevel<T>());
-    AmgLevel<T>& L = *Lp;
-    L.n = A.nr;
+    HostLevel H;
+    H.l = l;
+    H.A = &A;
+    H.z = &z;
     const std::vector<double> d = diagonal(A);
+    H.d = &d;
     for (int i = 0; i < A.nr; ++i)
       if (!(d[i] > 0.0)) return fail(GIPB200_ERR_ARG, "AMG: level %d row %d has no positive diagonal", l, i);
-    const double rho = rho_bound(A, d);
-    const double w = 4.0 / (3.0 * rho);
-    std::vector<T> dinv((size_t)A.nr);
-    for (int i = 0; i < A.nr; ++i) dinv[i] = (T)(w / d[i]);
-    GIPB_TRY(L.dinv.upload(dinv.data(), dinv.size(), s));
-    GIPB_TRY(L.x.alloc((size_t)(l == 0 ? std::max(A.nr, x0_len) : A.nr)));
-    GIPB_TRY(L.x.zero(s));  // level 0: entries past n are gathered (as zero) by A0
-    GIPB_TRY(L.t.alloc((size_t)A.nr));
-    if (l > 0) {
-      GIPB_TRY(L.b.alloc((size_t)A.nr));
-      GIPB_TRY(upload(A, &L.A, s));
-    }
-    nnz_all += (double)A.nnz();
+    H.w = 4.0 / (3.0 * rho_bound(A, d));
     if (A.nr <= kCoarse && l > 0) {  // coarsest: dense inverse
       const int m = A.nr;
       std::vector<double> M((size_t)m * m, 0.0);
@@ -753,11 +753,8 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
       std::vector<double> inv;
       if (!dense_inverse(m, M, inv))
         return fail(GIPB200_ERR_ARG, "AMG: coarsest operator (%d) is not positive definite", m);
-      std::vector<T> cf(inv.begin(), inv.end());
-      GIPB_TRY(cinv.upload(cf.data(), cf.size(), s));
-      nc = m;
-      lv.push_back(std::move(Lp));
-      break;
+      H.cinv = &inv;
+      return emit(H);
     }
     std::vector<int> agg;
     const int na = aggregate(A, d, agg);
@@ -768,22 +765,66 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
     for (auto& q : nrm) q = std::sqrt(q);
     std::vector<double> p0((size_t)A.nr);
     for (int i = 0; i < A.nr; ++i) p0[i] = nrm[agg[i]] > 0.0 ? z[i] / nrm[agg[i]] : 0.0;
-    HCsr P = smoothed_prolongator(A, d, agg, p0, na, w);
+    HCsr P = smoothed_prolongator(A, d, agg, p0, na, H.w);
     HCsr R = transpose(P);
     HCsr AP, Ac;
     GIPB_TRY(spgemm(A, P, AP));
     GIPB_TRY(spgemm(R, AP, Ac));
     if (drop > 0.0) sparsify(Ac, nrm, drop);
-    // the FP32 cycle keeps its transfer operators in FP16 (R = P^T still holds exactly:
-    // both round the same values), halving their value stream
-    const bool half = std::is_same<T, float>::value;
-    GIPB_TRY(upload(P, &L.P, s, half));
-    GIPB_TRY(upload(R, &L.R, s, half));
-    lv.push_back(std::move(Lp));
+    H.P = &P;
+    H.R = &R;
+    GIPB_TRY(emit(H));
     A = std::move(Ac);
-    z = nrm;
+    z = std::move(nrm);
   }
-  if (nc == 0) return fail(GIPB200_ERR_ARG, "AMG: more than %d levels", kMaxLevels);
+  return fail(GIPB200_ERR_ARG, "AMG: more than %d levels", kMaxLevels);
+}
+
+double amg_drop() {
+  const char* e = getenv("GIPB200_AMG_DROP");
+  return e ? atof(e) : kDrop;
+}
+
+}  // namespace
+
+template <typename T>
+int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const double* z0,
+                   bool singular, int x0_len, cudaStream_t s) {
+  const auto t0 = std::chrono::steady_clock::now();
+  lv.clear();
+  nc = 0;
+  const double nnz0 = (double)rp[n];
+  double nnz_all = 0.0;
+  GIPB_TRY(host_hierarchy(n, rp, ci, v, z0, singular, amg_drop(), [&](const HostLevel& H) -> int {
+    std::unique_ptr<AmgLevel<T>> Lp(new AmgLevel<T>());
+    AmgLevel<T>& L = *Lp;
+    const HCsr& A = *H.A;
+    L.n = A.nr;
+    std::vector<T> dinv((size_t)A.nr);
+    for (int i = 0; i < A.nr; ++i) dinv[i] = (T)(H.w / (*H.d)[i]);
+    GIPB_TRY(L.dinv.upload(dinv.data(), dinv.size(), s));
+    GIPB_TRY(L.x.alloc((size_t)(H.l == 0 ? std::max(A.nr, x0_len) : A.nr)));
+    GIPB_TRY(L.x.zero(s));  // level 0: entries past n are gathered (as zero) by A0
+    GIPB_TRY(L.t.alloc((size_t)A.nr));
+    if (H.l > 0) {  // level 0 runs on the solver's own operator
+      GIPB_TRY(L.b.alloc((size_t)A.nr));
+      GIPB_TRY(upload(A, &L.A, s));
+    }
+    nnz_all += (double)A.nnz();
+    if (H.cinv) {
+      std::vector<T> cf(H.cinv->begin(), H.cinv->end());
+      GIPB_TRY(cinv.upload(cf.data(), cf.size(), s));
+      nc = A.nr;
+    } else {
+      // the FP32 cycle keeps its transfer operators in FP16 (R = P^T still holds exactly:
+      // both round the same values), halving their value stream
+      const bool half = std::is_same<T, float>::value;
+      GIPB_TRY(upload(*H.P, &L.P, s, half));
+      GIPB_TRY(upload(*H.R, &L.R, s, half));
+    }
+    lv.push_back(std::move(Lp));
+    return GIPB200_OK;
+  }));
   op_complexity = nnz_all / std::max(nnz0, 1.0);
   GIPB_CUDA(cudaStreamSynchronize(s));
   setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -855,4 +896,68 @@ double AmgT<T>::cycle_bytes(double a0_stream_bytes) const {
 template struct AmgT<float>;
 template struct AmgT<double>;
 
+namespace {
+
+// max |a_ij - a_ji| / max |a| over the stored pattern (1 when the pattern is not symmetric).
+double asymmetry(const HCsr& A) {
+  HCsr S = A;
+  for (int i = 0; i < S.nr; ++i) {
+    std::vector<std::pair<int, double>> e;
+    for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) e.emplace_back(A.ci[k], A.v[k]);
+    std::sort(e.begin(), e.end(),
+              [](const std::pair<int, double>& a, const std::pair<int, double>& b) {
+                return a.first < b.first;
+              });
+    for (size_t q = 0; q < e.size(); ++q) {
+      S.ci[A.rp[i] + q] = e[q].first;
+      S.v[A.rp[i] + q] = e[q].second;
+    }
+  }
+  const HCsr T = transpose(S);
+  if (T.rp != S.rp || T.ci != S.ci) return 1.0;
+  double big = 0.0, diff = 0.0;
+  for (size_t k = 0; k < S.v.size(); ++k) {
+    big = std::max(big, std::fabs(S.v[k]));
+    diff = std::max(diff, std::fabs(S.v[k] - T.v[k]));
+  }
+  return big > 0.0 ? diff / big : 0.0;
+}
+
+}  // namespace
+
 }  // namespace gipb200
+
+using namespace gipb200;
+
+extern "C" int gipb200_amg_host_levels(int n, const int* rowptr, const int* col, const double* val,
+                                       const double* z, int singular, double drop, int max_levels,
+                                       int* levels, int* rows, long long* nnz, double* checks) {
+  if (n <= 0 || !rowptr || !col || !val || !z || max_levels < 1 || !levels || !rows || !nnz ||
+      !checks)
+    return fail(GIPB200_ERR_ARG, "bad arguments");
+  GIPB_TRY(validate_csr(n, n, rowptr[n], rowptr, col, n, "AMG operator"));
+  int count = 0;
+  const int st = host_hierarchy(n, rowptr, col, val, z, singular != 0, drop, [&](const HostLevel& H) -> int {
+    if (count >= max_levels) return GIPB200_OK;
+    const HCsr& A = *H.A;
+    const std::vector<double>& zl = *H.z;
+    double amax = 0.0, zmax = 0.0, res = 0.0, dmin = HUGE_VAL;
+    for (double a : A.v) amax = std::max(amax, std::fabs(a));
+    for (double q : zl) zmax = std::max(zmax, std::fabs(q));
+    for (int i = 0; i < A.nr; ++i) {
+      double t = 0.0;
+      for (int k = A.rp[i]; k < A.rp[i + 1]; ++k) t += A.v[k] * zl[A.ci[k]];
+      res = std::max(res, std::fabs(t));
+      dmin = std::min(dmin, (*H.d)[i]);
+    }
+    rows[count] = A.nr;
+    nnz[count] = A.nnz();
+    checks[3 * count + 0] = asymmetry(A);
+    checks[3 * count + 1] = (amax > 0.0 && zmax > 0.0) ? res / (amax * zmax) : 0.0;
+    checks[3 * count + 2] = dmin;
+    ++count;
+    return GIPB200_OK;
+  });
+  *levels = count;
+  return st;
+}

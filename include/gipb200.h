@@ -193,6 +193,18 @@ int gipb200_pcg_solve_static(int n, int n_all, const int* d_rowptr, const int* d
                              const double* d_x0, int mode, int maxit, double tol,
                              double* d_stats, void* stream);
 
+/* Host-side setup of the AMG preconditioner alone (no counterpart in the reference, whose
+ * solver is Jacobi-PCG; no device work, so it runs without a GPU): builds the hierarchy
+ * that precond = GIPB200_PRECOND_AMG builds for the n x n host CSR operator (columns < n)
+ * with near-null vector z (singular != 0: the operator annihilates z), coarse operators
+ * sparsified at `drop` (0: plain Galerkin), and reports its first min(levels, max_levels)
+ * levels: rows[l], nnz[l], and checks[3 l + 0..2] = max |a_ij - a_ji| / max |a| (1 when
+ * the pattern is not symmetric), max |(A z)_i| / (max |a| max |z|), and the smallest
+ * diagonal entry.  *levels = levels reported. */
+int gipb200_amg_host_levels(int n, const int* rowptr, const int* col, const double* val,
+                            const double* z, int singular, double drop, int max_levels,
+                            int* levels, int* rows, long long* nnz, double* checks);
+
 /* ------------------------------------------------------------------ timestep engine */
 typedef struct gipb200_dns_s* gipb200_dns;
 
