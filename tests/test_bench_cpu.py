@@ -1,0 +1,31 @@
+"""bench.py's reference arm and JSON contract, on the host (GIP's own CPU build)."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from conftest import REF_BIN, REPO
+
+
+@pytest.mark.skipif(not os.path.exists(REF_BIN), reason="GIP CPU build not built")
+def test_reference_arm_line():
+    r = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference",
+                        "--n", "12", "--steps", "2", "--warmup", "1"],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "ms/timestep"
+    assert d["higher_is_better"] is False and d["value"] > 0
+    assert d["steps"] == 2 and d["warmup"] == 1
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
+    assert d["config"]["cells"] == 12 ** 3
+    # GIP's own per-step line after the untimed and the timed steps (3 timesteps of dt 0.1)
+    for s in d["samples"].values():
+        assert s["last_line"].startswith("time 3.000000e-01")
