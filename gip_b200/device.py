@@ -162,8 +162,9 @@ PRECONDS = {"jacobi": 0, "amg": 1}
 def pcg_params(mode: str = "fixed", maxit: int = 100, tol: float = 1e-6,
                inner_tol: float = 1e-3, inner_maxit: int = 2000, max_outer: int = 30,
                precond: str = "jacobi") -> L.PcgParams:
-    """precond: "jacobi" (GIP's) or "amg" (mixed mode only: an FP32 smoothed-aggregation
-    V-cycle, hierarchy built on the host at create time)."""
+    """precond: "jacobi" (GIP's) or "amg" (tolerance and mixed modes: a smoothed-aggregation
+    V-cycle, FP64 in the tolerance mode and FP32 in the mixed one, its hierarchy built on
+    the host at create time; the fixed mode is GIP's and keeps Jacobi)."""
     return L.PcgParams(MODES[mode], maxit, tol, inner_tol, inner_maxit, max_outer,
                        PRECONDS[precond])
 

@@ -110,3 +110,47 @@ def test_struct_layout_matches_header(cname):
             assert pytype is STRUCTS[ctype.replace("const ", "")], name
         else:
             assert pytype is KIND[ctype], (name, ctype)
+
+
+def _enums():
+    vals = {}
+    for body in re.findall(r"enum\s*\{(.*?)\}", _source(), flags=re.S):
+        nxt = 0
+        for item in body.split(","):
+            item = item.strip()
+            if not item:
+                continue
+            name, _, v = item.partition("=")
+            nxt = int(v) if v.strip() else nxt
+            vals[name.strip()] = nxt
+            nxt += 1
+    return vals
+
+
+def test_enum_values_match_header():
+    from gip_b200 import device
+    e = _enums()
+    assert [e[f"GIPB200_PCG_{m.upper()}"] for m in ("fixed", "tol", "mixed")] == \
+        [device.MODES[m] for m in ("fixed", "tol", "mixed")]
+    assert {k: e[f"GIPB200_PRECOND_{k.upper()}"] for k in device.PRECONDS} == device.PRECONDS
+    assert [e[n] for n in ("GIPB200_OK", "GIPB200_ERR_ARG", "GIPB200_ERR_CUDA",
+                           "GIPB200_ERR_BREAKDOWN", "GIPB200_ERR_TIMEOUT", "GIPB200_ERR_NOMEM",
+                           "GIPB200_ERR_NOT_CONVERGED", "GIPB200_ERR_STATE")] == \
+        [_lib.STATUS_OK, _lib.ERR_ARG, _lib.ERR_CUDA, _lib.ERR_BREAKDOWN, _lib.ERR_TIMEOUT,
+         _lib.ERR_NOMEM, _lib.ERR_NOT_CONVERGED, _lib.ERR_STATE]
+
+
+def test_parameter_builders():
+    from gip_b200 import device
+    p = device.pcg_params("mixed", maxit=50, tol=1e-7, inner_tol=0.01, max_outer=9,
+                          precond="amg")
+    assert (p.mode, p.maxit, p.tol, p.inner_tol, p.max_outer, p.precond) == \
+        (_lib.PCG_MIXED, 50, 1e-7, 0.01, 9, 1)
+    d = device.dns_params(gamma=0.0025, pcg_mode="tol", tol=1e-9, use_graph=False,
+                          reorder=True)
+    assert (d.rho, d.gamma, d.pcg.mode, d.pcg.tol, d.pcg.precond, d.use_graph, d.reorder) == \
+        (1.0, 0.0025, _lib.PCG_TOL, 1e-9, 0, 0, 1)
+    with pytest.raises(KeyError):
+        device.pcg_params("cg")
+    with pytest.raises(KeyError):
+        device.pcg_params("tol", precond="ilu")
