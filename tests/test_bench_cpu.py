@@ -29,3 +29,39 @@ def test_reference_arm_line():
     # GIP's own per-step line after the untimed and the timed steps (3 timesteps of dt 0.1)
     for s in d["samples"].values():
         assert s["last_line"].startswith("time 3.000000e-01")
+
+
+def test_clock_sampler_parses_samples_and_reasons():
+    sys.path.insert(0, REPO)
+    import bench
+
+    class Done:
+        def terminate(self):
+            pass
+
+        def wait(self, timeout=None):
+            return 0
+
+    cs = bench.ClockSampler(0)
+    cs.proc = Done()
+    rows = ["0, 1965, 1965, 512.30, 0x0, Not Active, Not Active, Not Active, Not Active",
+            "0, 1950, 1965, 990.10, 0x4, Not Active, Not Active, Not Active, Active",
+            "0, 1965, 1965, [N/A], 0x0, Not Active, Not Active, Not Active, Not Active",
+            "garbage line"]
+    cs.out.write(("\n".join(rows) + "\n").encode())
+    cs.out.flush()
+    r = cs.stop()
+    assert r["samples"] == 3 and r["sm_mhz"] == 1965.0 and r["sm_max_mhz"] == 1965.0
+    assert r["power_w_max"] == 990.1 and r["reasons"] == ["sw_power_cap"]
+
+
+def test_peaks_and_traffic_helpers(tmp_path, monkeypatch):
+    sys.path.insert(0, REPO)
+    import bench
+    p = bench.peaks()
+    assert p["hbm_gbs"] > 0 and p["source"] in ("measured", "fallback")
+    t = bench.ncu_traffic("k_mxp_spmv_dot", 1000)
+    assert t is None or t > 0
+    monkeypatch.setattr(bench, "REPO", str(tmp_path))
+    assert bench.peaks() == {"hbm_gbs": 6650.0, "source": "fallback"}
+    assert bench.ncu_traffic("k_mxp_spmv_dot", 1000) is None
