@@ -62,6 +62,11 @@ class DnsInfo(C.Structure):
                 ("iteration_bytes", C.c_double), ("replacement_bytes", C.c_double)]
 
 
+class CgScalars(C.Structure):
+    _fields_ = [("rz", C.c_double), ("pAp", C.c_double), ("alpha", C.c_double),
+                ("beta", C.c_double), ("rr", C.c_double)]
+
+
 class AdjointParams(C.Structure):
     _fields_ = [("rho", C.c_double), ("gamma", C.c_double), ("nu0", C.c_double),
                 ("tol", C.c_double), ("maxit", C.c_int), ("checkpoint_every", C.c_int),
@@ -103,6 +108,9 @@ _SIGNATURES = {
     "gipb200_matrix_spmv_values": (_I, [_VP, _VP, _VP, _D, _D, _I, _VP]),
     "gipb200_matrix_get_values": (_I, [_VP, _VP]),
     "gipb200_matrix_inverse_diagonal": (_I, [_VP, _VP, C.POINTER(_I)]),
+    "gipb200_matrix_spmv_dot": (_I, [_VP, _VP, _VP, _I, _VP, _VP]),
+    "gipb200_cg_update_dot": (_I, [_VP, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "gipb200_cg_direction": (_I, [_I, _VP, _VP, _VP, _VP]),
     "gipb200_pcg_create": (_I, [_VP, _I, C.POINTER(PcgParams), C.POINTER(_VP)]),
     "gipb200_pcg_destroy": (_I, [_VP]),
     "gipb200_pcg_get_info": (_I, [_VP, C.POINTER(PcgInfo)]),
@@ -138,6 +146,10 @@ _SIGNATURES = {
     "gipb200_dns_field_ptr": (_I, [_VP, C.c_char_p, C.POINTER(_VP), C.POINTER(_I)]),
     "gipb200_dns_copy_field": (_I, [_VP, C.c_char_p, _VP, _I, _VP]),
     "gipb200_dns_scalars": (_I, [_VP, C.POINTER(_D), C.POINTER(_D), C.POINTER(_D)]),
+    "gipb200_dns_set_time": (_I, [_VP, _D, _VP]),
+    "gipb200_dns_phase_bytes": (_I, [_VP, _VP]),
+    "gipb200_dns_vcycle_profile": (_I, [_VP, _I, _VP, _I, C.POINTER(_I), _VP, _VP, _VP, _VP]),
+    "gipb200_pcg_vcycle_profile": (_I, [_VP, _I, _VP, _I, C.POINTER(_I), _VP, _VP, _VP, _VP]),
     "gipb200_dns_set_field": (_I, [_VP, C.c_char_p, _VP, _I, _I, _VP]),
     "gipb200_dns_launch_count": (_I, [_VP, C.POINTER(C.c_longlong)]),
     "gipb200_dns_kernel_time": (_I, [_VP, _I, _I, _VP, C.POINTER(_D), C.POINTER(_D)]),

@@ -831,16 +831,49 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
   return GIPB200_OK;
 }
 
+int CycleTrace::mark(cudaStream_t s, int lvl, int knd, double by) {
+  cudaEvent_t e;
+  GIPB_CUDA(cudaEventCreate(&e));
+  ev.push_back(e);
+  GIPB_CUDA(cudaEventRecord(e, s));
+  level.push_back(lvl);
+  kind.push_back(knd);
+  bytes.push_back(by);
+  return GIPB200_OK;
+}
+
+int CycleTrace::close(cudaStream_t s) {
+  cudaEvent_t e;
+  GIPB_CUDA(cudaEventCreate(&e));
+  ev.push_back(e);
+  GIPB_CUDA(cudaEventRecord(e, s));
+  return GIPB200_OK;
+}
+
+CycleTrace::~CycleTrace() {
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+}
+
 template <typename T>
 int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScratch rs, int first,
-                     cudaStream_t s, const PackedView* pk) const {
+                     cudaStream_t s, const PackedView* pk, CycleTrace* tr,
+                     double a0_stream_bytes) const {
   const bool packed = pk && pk->on && std::is_same<T, float>::value;
   const int L = (int)lv.size();
+  const double w = sizeof(T);
+  // bytes of each kernel as cycle_bytes counts them (profiling marks only)
+  auto mark = [&](int l, int kind, double by) -> int {
+    return tr ? tr->mark(s, l, kind, by) : GIPB200_OK;
+  };
+  auto a_bytes = [&](int l) { return l == 0 ? a0_stream_bytes : stream_bytes(lv[l]->A); };
   // downward: pre-smooth from zero, residual, restriction
   for (int l = 0; l < L - 1; ++l) {
     const AmgLevel<T>& V = *lv[l];
     const T* b = l == 0 ? r : V.b.p;
+    const double n = V.n, nn = lv[l + 1]->n;
+    GIPB_TRY(mark(l, GIPB200_CYCLE_JACOBI0, 3.0 * n * w));
     k_amg_jacobi0<T><<<vec_blocks(V.n), 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
+    GIPB_TRY(mark(l, GIPB200_CYCLE_RESIDUAL, a_bytes(l) + 3.0 * n * w));
     if (l == 0) {
       const int bs = vec_blocks(A0.nslices * 32);
       if (packed)
@@ -850,16 +883,21 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     } else {
       amg_mv<T, kResid>(V.A, V.x.p, b, (const T*)nullptr, V.t.p, S, s);
     }
+    GIPB_TRY(mark(l, GIPB200_CYCLE_RESTRICT, stream_bytes(V.R) + (n + nn) * w));
     amg_mv<T, kPlain>(V.R, V.t.p, (const T*)nullptr, (const T*)nullptr, lv[l + 1]->b.p, S, s);
   }
   const AmgLevel<T>& C = *lv[L - 1];
+  GIPB_TRY(mark(L - 1, GIPB200_CYCLE_DENSE, ((double)nc * nc + 2.0 * nc) * w));
   k_amg_dense<T><<<std::min(kMaxReduceBlocks, (nc + 7) / 8), 256, 0, s>>>(nc, cinv.p, C.b.p,
                                                                             C.x.p, S);
   // upward: prolongation, post-smoothing (level 0 also reduces r.z)
   for (int l = L - 2; l >= 0; --l) {
     const AmgLevel<T>& V = *lv[l];
     const T* xc = (l + 1 == L - 1) ? lv[l + 1]->x.p : lv[l + 1]->t.p;
+    const double n = V.n, nn = lv[l + 1]->n;
+    GIPB_TRY(mark(l, GIPB200_CYCLE_PROLONG, stream_bytes(V.P) + (nn + 2.0 * n) * w));
     amg_mv<T, kAdd>(V.P, xc, (const T*)nullptr, (const T*)nullptr, V.x.p, S, s);
+    GIPB_TRY(mark(l, GIPB200_CYCLE_SMOOTH, a_bytes(l) + 4.0 * n * w));
     if (l == 0) {
       const int bs = vec_blocks(A0.nslices * 32);
       if (packed)
@@ -870,6 +908,7 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
       amg_mv<T, kSmooth>(V.A, V.x.p, V.b.p, V.dinv.p, V.t.p, S, s);
     }
   }
+  if (tr) GIPB_TRY(tr->close(s));
   GIPB_LAUNCH_CHECK();
   return GIPB200_OK;
 }

@@ -43,6 +43,18 @@ struct PackedView {
   const float* table = nullptr;
 };
 
+// Per-kernel timing of V-cycles (profiling only): an event is recorded before every
+// kernel and one after the last, and each kernel is tagged with its level, its kind
+// (GIPB200_CYCLE_*) and its algorithmic bytes.
+struct CycleTrace {
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> level, kind;
+  std::vector<double> bytes;
+  int mark(cudaStream_t s, int lvl, int knd, double by);  // before a kernel
+  int close(cudaStream_t s);                              // after the last one
+  ~CycleTrace();
+};
+
 template <typename T>
 struct AmgLevel {
   int n = 0;
@@ -71,7 +83,8 @@ struct AmgT {
   // beta = (r.z) / (previous r.z) (0 when `first` or when no previous r.z is stored) and
   // stores r.z in S.
   int enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScratch rs, int first,
-              cudaStream_t s, const PackedView* pk = nullptr) const;
+              cudaStream_t s, const PackedView* pk = nullptr, CycleTrace* tr = nullptr,
+              double a0_stream_bytes = 0.0) const;
   // Algorithmic bytes of one V-cycle: every operator's stored words once per use and every
   // vector read or written once per kernel; level 0's operator stream is given (packed or
   // plain, the caller's operator).

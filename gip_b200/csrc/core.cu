@@ -489,6 +489,7 @@ int gipb200_matrix_create(int nrows, int ncols, int nnz, const int* rp, const in
   gipb200_matrix A = new (std::nothrow) gipb200_matrix_s();
   if (!A) return fail(GIPB200_ERR_NOMEM, "host allocation failed");
   int st = sell_build(&A->S, nrows, ncols, nnz, rp, col, val, 0);
+  if (st == GIPB200_OK) st = reduce_scratch_alloc(&A->partials, &A->ticket, &A->rs);
   if (st != GIPB200_OK) {
     delete A;
     return st;

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <string>
 #include <vector>
 
@@ -423,6 +424,24 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync) {
   GIPB_LAUNCH_CHECK();
   launches += 10 + H.stamp_kernels + (pcg.launches - pcg_before);
   return GIPB200_OK;
+}
+
+// Compulsory traffic: every stored value and index once, slice offsets, each gathered
+// vector once, each written vector once (a row without stored nonzeros writes nothing).
+void Dns::phase_bytes(double out[7]) const {
+  auto op = [](const Sell& M) { return 12.0 * M.nnz + 8.0 * (M.nslices + 1.0); };
+  const double n = N, no = NO, nf = NF;
+  // predictor: C's values = Ec mf (CSR, rows scattered into C's slots), D/C products, AB2
+  const double ec = 12.0 * Ec.nnz + 4.0 * (Ec.nrows + 1.0) + 4.0 * Ec.nrows + 8.0 * nf +
+                    8.0 * Ec.nrows;
+  const double cd = op(D) + 8.0 * D.nnz + 24.0 * no + 24.0 * n;
+  out[0] = ec + cd + 120.0 * n;
+  out[1] = op(Mx) + op(My) + op(Mz) + 24.0 * no + 8.0 * n;          // rhs
+  out[2] = 0.0;                                                      // PCG
+  out[3] = 16.0 * no + op(Lb) + 24.0 * Lb.nnz;                       // p0/p copies, ghosts
+  out[4] = op(Gx) + op(Gy) + op(Gz) + 8.0 * no + 24.0 * no + 48.0 * n;  // gp, u -= gp
+  out[5] = op(SO) + op(SFx) + op(SFy) + op(SFz) + 56.0 * no + 16.0 * nf;  // mf
+  out[6] = op(Mres) + 8.0 * nf + 8.0 * n + 32.0 * n;                 // massr, CFL
 }
 
 double* Dns::field(const std::string& name, int* n) {
@@ -1026,10 +1045,37 @@ int gipb200_dns_launch_count(gipb200_dns Dh, long long* count) {
 int gipb200_dns_kernel_time(gipb200_dns Dh, int kernel, int reps, void* stream, double* avg_ms,
                             double* bytes) {
   if (!Dh || !avg_ms || !bytes) return fail(GIPB200_ERR_ARG, "null argument");
+  if (kernel == GIPB200_KERNEL_MIXED_UPDATE)
+    return Dh->E.pcg.time_update(reps, as_stream(stream), avg_ms, bytes);
   if (kernel != GIPB200_KERNEL_PCG_SPMV_DOT && kernel != GIPB200_KERNEL_MIXED_SPMV_DOT)
     return fail(GIPB200_ERR_ARG, "unknown kernel id %d", kernel);
   return Dh->E.pcg.time_spmv(kernel == GIPB200_KERNEL_MIXED_SPMV_DOT, reps, as_stream(stream),
                              avg_ms, bytes);
+}
+
+int gipb200_dns_phase_bytes(gipb200_dns Dh, double* h_bytes) {
+  if (!Dh || !h_bytes) return fail(GIPB200_ERR_ARG, "null argument");
+  Dh->E.phase_bytes(h_bytes);
+  return GIPB200_OK;
+}
+
+int gipb200_dns_vcycle_profile(gipb200_dns Dh, int reps, void* stream, int cap, int* n_kernels,
+                               int* h_level, int* h_kind, double* h_ms, double* h_bytes) {
+  if (!Dh) return fail(GIPB200_ERR_ARG, "null engine");
+  return Dh->E.pcg.profile_vcycle(reps, as_stream(stream), cap, n_kernels, h_level, h_kind, h_ms,
+                                  h_bytes);
+}
+
+int gipb200_dns_set_time(gipb200_dns Dh, double time, void* stream) {
+  if (!Dh) return fail(GIPB200_ERR_ARG, "null engine");
+  if (!std::isfinite(time)) return fail(GIPB200_ERR_ARG, "time must be finite");
+  Dns& E = Dh->E;
+  // ordered on `stream` after the work already queued there; the host value is read
+  // before the call returns
+  GIPB_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(E.sc.p) + offsetof(DnsScalars, time), &time,
+                            sizeof(double), cudaMemcpyHostToDevice, as_stream(stream)));
+  GIPB_CUDA(cudaStreamSynchronize(as_stream(stream)));
+  return GIPB200_OK;
 }
 
 int gipb200_dns_scalars(gipb200_dns Dh, double* dt, double* sigma, double* time) {

@@ -89,6 +89,9 @@ struct Dns {
     graph = nullptr;
   }
   int grow_history(int need, cudaStream_t s);
+  // Algorithmic bytes of each phase of one timestep, in gipb200_dns_step_phases order
+  // (the PCG entry is 0: its bytes are iterations x iteration_bytes + replacements).
+  void phase_bytes(double out[7]) const;
   int enqueue_step(cudaStream_t s, bool host_sync);
   int enqueue_initial_dt(cudaStream_t s);
   double* field(const std::string& name, int* n);

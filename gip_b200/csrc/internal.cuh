@@ -162,4 +162,9 @@ int grid_blocks(int threads, int work_items, int per_thread, int max_blocks, int
 
 struct gipb200_matrix_s {
   gipb200::Sell S;
+  // reduction scratch of the fused operations called on this handle (spmv_dot,
+  // cg_update_dot): calls that share a handle must be ordered on one stream
+  gipb200::DevBuf<double> partials;
+  gipb200::DevBuf<unsigned> ticket;
+  gipb200::ReduceScratch rs{};
 };

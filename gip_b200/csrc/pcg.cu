@@ -1544,6 +1544,35 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
   return GIPB200_OK;
 }
 
+int Pcg::time_update(int reps, cudaStream_t s, double* avg_ms, double* bytes) {
+  if (reps <= 0) return fail(GIPB200_ERR_ARG, "reps must be positive");
+  if (prm.mode != GIPB200_PCG_MIXED)
+    return fail(GIPB200_ERR_STATE, "the FP32 update exists only in the mixed form");
+  // zeroed scratch scalars: alpha = 0, so y += 0 p and r -= 0 Ap rewrite y and r unchanged,
+  // and the kernel's decisions land in the scratch scalars
+  DevBuf<PcgScalars> tsc;
+  GIPB_TRY(tsc.alloc(1));
+  GIPB_TRY(tsc.zero(s));
+  cudaEvent_t e0, e1;
+  GIPB_CUDA(cudaEventCreate(&e0));
+  GIPB_CUDA(cudaEventCreate(&e1));
+  for (int k = 0; k <= reps; ++k) {
+    if (k == 1) GIPB_CUDA(cudaEventRecord(e0, s));
+    k_mx_update<<<blocks_vec, 256, 0, s>>>(n, y32.p, r32.p, p32.p, Ap32.p, tsc.p, rs,
+                                           prm.inner_tol, prm.maxit, -1, scale.p, 0, 0, amg ? 1 : 0);
+  }
+  GIPB_LAUNCH_CHECK();
+  GIPB_CUDA(cudaEventRecord(e1, s));
+  GIPB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  GIPB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *avg_ms = (double)ms / reps;
+  *bytes = 24.0 * n;  // y and r read and written, p and Ap read (FP32)
+  return GIPB200_OK;
+}
+
 int Pcg::time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* bytes) {
   if (reps <= 0) return fail(GIPB200_ERR_ARG, "reps must be positive");
   if (mixed && prm.mode != GIPB200_PCG_MIXED)
@@ -1588,6 +1617,50 @@ int Pcg::time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* 
   *bytes = (double)L->nnz * (vbytes + 4.0) + (double)(L->nslices + 1) * 8.0 +
            (double)L->nrows * (mixed ? 4.0 : 2.0) * vbytes;
   if (mixed && cop.enabled) *bytes = cop.bytes_per_launch;
+  return GIPB200_OK;
+}
+
+int Pcg::profile_vcycle(int reps, cudaStream_t s, int cap, int* n_kernels, int* level, int* kind,
+                        double* ms, double* bytes) {
+  if (reps <= 0 || cap < 0 || !n_kernels) return fail(GIPB200_ERR_ARG, "bad arguments");
+  if (!amg && !amg64) return fail(GIPB200_ERR_STATE, "the solver has no AMG preconditioner");
+  // scratch scalars: the cycle's kernels run only while `done` is 0, and its last kernel
+  // writes beta and r.z, which must not touch the solver's own scalars
+  DevBuf<PcgScalars> tsc;
+  GIPB_TRY(tsc.alloc(1));
+  GIPB_TRY(tsc.zero(s));
+  const PackedView pk0 = packed();
+  const double plain32 = (double)L->nslots * 8.0 + (L->nslices + 1.0) * 8.0;
+  const double a0 = amg ? (cop.enabled ? cop.bytes_per_launch - 16.0 * n : plain32)
+                        : (double)L->nslots * 12.0 + (L->nslices + 1.0) * 8.0;
+  std::vector<double> sum;
+  int nk = 0;
+  for (int k = 0; k <= reps; ++k) {  // cycle 0 is untimed
+    CycleTrace tr;
+    if (amg)
+      GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, tsc.p, rs, 1, s, &pk0, &tr, a0));
+    else
+      GIPB_TRY(amg64->enqueue(L->view(), r.p, z64.p, tsc.p, rs, 1, s, nullptr, &tr, a0));
+    GIPB_CUDA(cudaEventSynchronize(tr.ev.back()));
+    nk = (int)tr.kind.size();
+    if (k == 0) {
+      sum.assign(nk, 0.0);
+      for (int j = 0; j < std::min(nk, cap); ++j) {
+        if (level) level[j] = tr.level[j];
+        if (kind) kind[j] = tr.kind[j];
+        if (bytes) bytes[j] = tr.bytes[j];
+      }
+      continue;
+    }
+    for (int j = 0; j < nk; ++j) {
+      float t = 0.f;
+      GIPB_CUDA(cudaEventElapsedTime(&t, tr.ev[j], tr.ev[j + 1]));
+      sum[j] += t;
+    }
+  }
+  *n_kernels = nk;
+  if (ms)
+    for (int j = 0; j < std::min(nk, cap); ++j) ms[j] = sum[j] / reps;
   return GIPB200_OK;
 }
 
@@ -1661,6 +1734,13 @@ int gipb200_pcg_kernel_time(gipb200_pcg S, int reps, void* stream, double* avg_m
   if (!S || !avg_ms || !bytes) return fail(GIPB200_ERR_ARG, "null argument");
   return S->P.time_spmv(S->P.prm.mode == GIPB200_PCG_MIXED, reps, as_stream(stream), avg_ms,
                         bytes);
+}
+
+int gipb200_pcg_vcycle_profile(gipb200_pcg S, int reps, void* stream, int cap, int* n_kernels,
+                               int* h_level, int* h_kind, double* h_ms, double* h_bytes) {
+  if (!S) return fail(GIPB200_ERR_ARG, "null solver");
+  return S->P.profile_vcycle(reps, as_stream(stream), cap, n_kernels, h_level, h_kind, h_ms,
+                             h_bytes);
 }
 
 int gipb200_pcg_solve(gipb200_pcg S, const double* b, double* x, const double* x0, void* stream,

@@ -126,6 +126,11 @@ struct Pcg {
   int result(cudaStream_t s, gipb200_pcg_result* out);
   // Times `reps` launches of the SpMV+dot kernel of the current mode on scratch scalars.
   int time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* bytes);
+  // Times `reps` launches of the mixed form's FP32 update kernel (scratch scalars, alpha 0).
+  int time_update(int reps, cudaStream_t s, double* avg_ms, double* bytes);
+  // Per-kernel profile of `reps` V-cycles on the current residual (scratch scalars).
+  int profile_vcycle(int reps, cudaStream_t s, int cap, int* n_kernels, int* level, int* kind,
+                     double* ms, double* bytes);
 
  private:
   int enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t s, bool host_sync);

@@ -15,12 +15,18 @@
 //    (262144), else the call fails with GIPB200_ERR_ARG before launching anything;
 //  - every call uses the same array: two calls whose kernels overlap on the GPU (other
 //    streams, other host threads) race and corrupt each other.  Serialise them;
-//  - the array keeps the last call's contents; the reduction counters are cleared on
-//    the first call on each device and return to zero at the end of every reduction.
+//  - the array keeps the last call's contents; every call clears the reduction counter
+//    on its own stream before its first kernel (a 4-byte cudaMemsetAsync, ordered with the
+//    caller's work on that stream, non-blocking streams included), and every reduction
+//    returns it to zero.
 //
 // Set-up: the first call on a device (with that device current) resolves the array's
-// device address with cudaGetSymbolAddress and clears the counters; make that first call
-// before any stream capture.
+// device address with cudaGetSymbolAddress; make that first call before any stream
+// capture.
+//
+// TOL mode stops on the device; the host polls the stop flag every kPollEvery iterations
+// (a 4-byte copy into a host variable and a wait on the caller's stream), so a solve that
+// converges early launches about 3 * kPollEvery kernels past convergence, not 3 * maxit.
 //
 // The arithmetic is the FP64 PCG of GIP_LinearSolver::solve (src/Algorithms/
 // GIP_LinearSolver.h:44-117) with GIP's CPU rounding, one thread per CSR row.
@@ -35,6 +41,7 @@ namespace gipb200 {
 namespace {
 
 constexpr int kStaticMaxCells = 262144;
+constexpr int kPollEvery = 32;     // TOL mode: iterations between host reads of the stop flag
 constexpr int kStaticBlocks = 1024;  // grid cap; partials for 3 sums per block
 struct StaticScalars {
   double rz, pAp, alpha, beta, rr, bb;
@@ -261,7 +268,8 @@ extern "C" int gipb200_pcg_solve_static(int n, int n_all, const int* d_rowptr, c
                                         const double* d_val, const double* d_b, double* d_x,
                                         const double* d_x0, int mode, int maxit, double tol,
                                         double* d_stats, void* stream) {
-  if (n < 0 || n_all < n || !d_rowptr || !d_b || !d_x || !d_x0 || !d_stats)
+  if (n < 0 || n_all < n || !d_rowptr || !d_b || !d_x || !d_x0 || !d_stats ||
+      (n > 0 && (!d_col || !d_val)))
     return fail(GIPB200_ERR_ARG, "gipb200_pcg_solve_static: bad sizes or null pointer");
   if (n_all > kStaticMaxCells)
     return fail(GIPB200_ERR_ARG,
@@ -282,8 +290,6 @@ extern "C" int gipb200_pcg_solve_static(int n, int n_all, const int* d_rowptr, c
     if (!slot.ready) {
       void* ptr = nullptr;
       GIPB_CUDA(cudaGetSymbolAddress(&ptr, g_static_scratch));
-      // the reduction counter must start at zero; everything else is written before use
-      GIPB_CUDA(cudaMemset(ptr, 0, sizeof(double) * kStaticDoubles));
       slot.base = reinterpret_cast<double*>(ptr);
       slot.ready = true;
     }
@@ -299,6 +305,9 @@ extern "C" int gipb200_pcg_solve_static(int n, int n_all, const int* d_rowptr, c
   unsigned* ticket = reinterpret_cast<unsigned*>(reinterpret_cast<double*>(W.S) + kScalarSlots);
   W.rs.ticket = ticket;
 
+  // the reduction counter starts at zero, ordered on the caller's stream; everything else
+  // in the array is written before it is read
+  GIPB_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
   // x = x0 and p = x0 over all cells (GIP_LinearSolver.h:56,67): plain copies, no allocation
   GIPB_CUDA(cudaMemcpyAsync(d_x, d_x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemcpyAsync(W.p, d_x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
@@ -308,6 +317,12 @@ extern "C" int gipb200_pcg_solve_static(int n, int n_all, const int* d_rowptr, c
                                    tol);
   GIPB_LAUNCH_CHECK();
   for (int k = 0; k < maxit; ++k) {
+    if (mode == GIPB200_PCG_TOL && k > 0 && k % kPollEvery == 0) {
+      int done = 0;  // the device's stop flag, read into a host variable (no allocation)
+      GIPB_CUDA(cudaMemcpyAsync(&done, &W.S->done, sizeof(int), cudaMemcpyDeviceToHost, s));
+      GIPB_CUDA(cudaStreamSynchronize(s));
+      if (done) break;
+    }
     k_st_spmv_dot<<<blocks, 256, 0, s>>>(n, d_rowptr, d_col, d_val, W, ticket, mode);
     k_st_update<<<blocks, 256, 0, s>>>(n, d_x, W, ticket, mode, maxit, tol);
     k_st_pupdate<<<blocks, 256, 0, s>>>(n, W);

@@ -143,6 +143,14 @@ class DeviceMatrix:
         L.call("gipb200_matrix_inverse_diagonal", self.handle, _dptr(d), C.byref(miss))
         return d, miss.value
 
+    def spmv_dot(self, x: torch.Tensor, y: torch.Tensor, out: torch.Tensor, n_dot: int = None,
+                 stream=None) -> torch.Tensor:
+        """y = A x and out[0] = x[:n_dot].y[:n_dot] (device scalar, no host wait)."""
+        self._check(x, self.nrows, y)
+        L.call("gipb200_matrix_spmv_dot", self.handle, _dptr(x), _dptr(y),
+               self.nrows if n_dot is None else n_dot, _dptr(out), _stream(stream))
+        return out
+
     def close(self) -> None:
         if getattr(self, "handle", None):
             L.load().gipb200_matrix_destroy(self.handle)
@@ -167,6 +175,22 @@ def pcg_params(mode: str = "fixed", maxit: int = 100, tol: float = 1e-6,
     the host at create time; the fixed mode is GIP's and keeps Jacobi)."""
     return L.PcgParams(MODES[mode], maxit, tol, inner_tol, inner_maxit, max_outer,
                        PRECONDS[precond])
+
+
+CYCLE_KINDS = ("jacobi0", "residual", "restrict", "dense", "prolong", "smooth")
+
+
+def _vcycle_profile(fn: str, handle, reps: int, stream) -> list:
+    cap = 128
+    nk = C.c_int()
+    lvl = np.zeros(cap, np.int32)
+    kind = np.zeros(cap, np.int32)
+    ms = np.zeros(cap)
+    by = np.zeros(cap)
+    L.call(fn, handle, reps, _stream(stream), cap, C.byref(nk), _hptr(lvl), _hptr(kind),
+           _hptr(ms), _hptr(by))
+    return [{"level": int(lvl[k]), "kind": CYCLE_KINDS[kind[k]], "ms": float(ms[k]),
+             "bytes": float(by[k])} for k in range(min(nk.value, cap))]
 
 
 class PcgSolver:
@@ -195,6 +219,10 @@ class PcgSolver:
         return {"iterations": res.iterations, "outer": res.outer, "status": res.status,
                 "rr": res.rr, "bb": res.bb}
 
+    def vcycle_profile(self, reps: int = 10, stream=None) -> list:
+        """Per-kernel profile of the AMG V-cycle: [{level, kind, ms, bytes}] in launch order."""
+        return _vcycle_profile("gipb200_pcg_vcycle_profile", self.handle, reps, stream)
+
     def kernel_time(self, reps: int = 20, stream=None) -> tuple:
         """(mean ms, streamed bytes) of the solver's SpMV-dot kernel over `reps` launches."""
         ms, nb = C.c_double(), C.c_double()
@@ -217,6 +245,45 @@ class PcgSolver:
             self.close()
         except Exception:
             pass
+
+
+def cg_update_dot(A: DeviceMatrix, n: int, x, r, z, p, q, dinv, sc: torch.Tensor, stream=None):
+    """alpha = rz/pAp; x += alpha p; r -= alpha q; z = dinv r; rz, rr, beta into `sc`
+    (a float64 device tensor laid out as gipb200_cg_scalars: rz, pAp, alpha, beta, rr)."""
+    L.call("gipb200_cg_update_dot", A.handle, n, _dptr(x), _dptr(r), _dptr(z), _dptr(p),
+           _dptr(q), _dptr(dinv), _dptr(sc), _stream(stream))
+
+
+def cg_direction(n: int, p, z, sc: torch.Tensor, stream=None):
+    """p = z + beta p, beta from `sc` on the device."""
+    L.call("gipb200_cg_direction", n, _dptr(p), _dptr(z), _dptr(sc), _stream(stream))
+
+
+def host_loop_pcg(A: DeviceMatrix, Dg: DeviceMatrix, dinv: torch.Tensor, b: torch.Tensor,
+                  x: torch.Tensor, x0: torch.Tensor, maxit: int, stream=None) -> torch.Tensor:
+    """GIP_LinearSolver::solve (GIP_LinearSolver.h:44-117) driven from the host over the fused
+    entry points: the set-up with GIP's copies, SpMV and axpy, the Jacobi application as
+    the diagonal operator `Dg`'s SpMV fused with r.z, then `maxit` iterations of
+    spmv_dot / cg_update_dot / cg_direction with no host wait.  x (n_all) receives the
+    solution; returns the device scalars (rz, pAp, alpha, beta, rr)."""
+    n, n_all = A.nrows, x.numel()
+    s = _stream(stream)
+    sc = torch.zeros(5, dtype=torch.float64, device=x.device)
+    p = x0.clone()                     # dp = x0 (ALL)
+    Ax = x0.clone()                    # dAx = x0 (ALL)
+    r = torch.empty(n_all, dtype=torch.float64, device=x.device)
+    r[:n] = b[:n]                      # dr = b (INNER)
+    z = torch.zeros(n_all, dtype=torch.float64, device=x.device)
+    x.copy_(x0)                        # dx = x0 (ALL)
+    A.spmv(x, Ax, stream=stream)       # dAx = A x
+    L.call("gipb200_daxpy", n, _dptr(r), _dptr(Ax), -1.0, s)  # dr += -1 dAx
+    Dg.spmv_dot(r, p, sc, n_dot=n, stream=stream)              # dp = D r; r1 = r.dp
+    pAp = C.c_void_p(sc.data_ptr() + 8)
+    for _ in range(maxit):
+        L.call("gipb200_matrix_spmv_dot", A.handle, _dptr(p), _dptr(Ax), n, pAp, s)
+        cg_update_dot(A, n, x, r, z, p, Ax, dinv, sc, stream)
+        cg_direction(n, p, z, sc, stream)
+    return sc
 
 
 # ----------------------------------------------------------------------------- timestep
@@ -300,6 +367,19 @@ class DnsEngine:
         L.call("gipb200_dns_field_ptr", self.handle, name.encode(), C.byref(p), C.byref(n))
         return p.value, n.value
 
+    def copy_field(self, name: str, out: torch.Tensor, stream=None) -> torch.Tensor:
+        """Device-to-device copy of a field in the caller's numbering into `out` (float64,
+        at least the field's length), on `stream` with no host wait."""
+        if out.dtype != torch.float64 or not out.is_cuda:
+            raise TypeError("out must be a float64 device tensor")
+        L.call("gipb200_dns_copy_field", self.handle, name.encode(), _dptr(out), out.numel(),
+               _stream(stream))
+        return out
+
+    def set_time(self, time: float, stream=None) -> None:
+        """Set the simulated time (GIP_DNS's `time` member)."""
+        L.call("gipb200_dns_set_time", self.handle, float(time), _stream(stream))
+
     def set_field(self, name: str, values: np.ndarray, offset: int = 0, stream=None) -> None:
         """Asynchronous host->device copy into a field (keep `values` alive and, for a
         truly asynchronous copy, pinned, until the stream has passed it)."""
@@ -308,9 +388,19 @@ class DnsEngine:
         L.call("gipb200_dns_set_field", self.handle, name.encode(), _hptr(values), offset,
                values.size, _stream(stream))
 
+    def vcycle_profile(self, reps: int = 10, stream=None) -> list:
+        """Per-kernel profile of the AMG V-cycle: [{level, kind, ms, bytes}] in launch order."""
+        return _vcycle_profile("gipb200_dns_vcycle_profile", self.handle, reps, stream)
+
+    def phase_bytes(self) -> Dict[str, float]:
+        """Algorithmic bytes of each timestep phase (the PCG's is 0: see info())."""
+        out = np.zeros(7)
+        L.call("gipb200_dns_phase_bytes", self.handle, _hptr(out))
+        return dict(zip(self.PHASES, out.tolist()))
+
     def kernel_time(self, kernel: str = "mixed", reps: int = 20, stream=None) -> tuple:
         """Mean CUDA-event time (ms) and compulsory bytes of one PCG SpMV+dot launch."""
-        kid = {"fp64": 0, "mixed": 1}[kernel]
+        kid = {"fp64": 0, "mixed": 1, "mixed_update": 2}[kernel]
         ms, by = C.c_double(), C.c_double()
         L.call("gipb200_dns_kernel_time", self.handle, kid, reps, _stream(stream), C.byref(ms),
                C.byref(by))

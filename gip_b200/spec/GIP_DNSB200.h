@@ -1,9 +1,14 @@
 // Optional: GIP_DNS<B200 types>::integrate handed to the fused device engine
 // (libgipb200 gipb200_dns_*): the same fractional step as GIP_DNS.h:99-414, with every
 // phase fused, dt/sigma/time on the device and each step one CUDA graph.  GIP_DNS's
-// setUp still loads the operators and fields through the B200 Specification; integrate
-// then builds the engine from them, prints GIP's per-step line, and writes the fields
-// back into GIP_DNS's vectors.  Include after GIP_DNS.h and B200.h.
+// setUp still loads the operators and fields through the B200 Specification.  Each
+// integrate() builds an engine from GIP_DNS's current state -- the velocities, the AB2
+// history ax0/ay0/az0, the face mass fluxes mf, the pressure p and its warm start p0, and
+// the simulated time -- so consecutive calls continue exactly like GIP's own integrate()
+// (which starts each call with a fresh CFL dt from u, v, w, GIP_DNS.h:102-103).  C's
+// values need no upload: every predictor rebuilds them from mf (GIP_DNS.h:311).  The
+// engine prints GIP's per-step line and writes every field back into GIP_DNS's vectors.
+// Include after GIP_DNS.h and B200.h.
 #ifndef _gip_dns_b200_
 #define _gip_dns_b200_
 #include <mpi.h>
@@ -70,6 +75,19 @@ inline void GIP_DNS<GIP_MatrixB200, GIP_VectorB200, GIP_ArchB200, GIP_NonLinearB
   gipb200_require(gipb200_dns_create(&ops, u.getHostPtr(), v.getHostPtr(), w.getHostPtr(),
                                      dxs.getHostPtr(), &prm, &E),
                   "gipb200_dns_create");
+  // the state earlier integrate() calls (or the caller) left in GIP_DNS's members
+  struct {
+    const char* name;
+    GIP_VectorB200* vec;
+    int n;
+  } state[] = {{"ax0", &ax0, ops.n_owned}, {"ay0", &ay0, ops.n_owned},
+               {"az0", &az0, ops.n_owned}, {"p", &p, ops.n_owned},
+               {"p0", &p0, ops.n_owned},   {"mf", &mf, ops.n_faces}};
+  for (size_t k = 0; k < sizeof(state) / sizeof(state[0]); ++k)
+    gipb200_require(gipb200_dns_set_field(E, state[k].name, state[k].vec->getHostPtr(), 0,
+                                          state[k].n, 0),
+                    "gipb200_dns_set_field");
+  gipb200_require(gipb200_dns_set_time(E, time, 0), "gipb200_dns_set_time");
   gipb200_require(gipb200_dns_advance(E, maxIt, 0), "gipb200_dns_advance");
   int steps = 0;
   std::vector<double> t(maxIt > 0 ? maxIt : 1), dtv(t.size()), mr(t.size()), rr(t.size());
@@ -99,6 +117,12 @@ inline void GIP_DNS<GIP_MatrixB200, GIP_VectorB200, GIP_ArchB200, GIP_NonLinearB
                                            back[k].vec->getSize(), 0),
                     "gipb200_dns_copy_field");
   }
+  // u0 <- u over the inner cells at every step's end (GIP_DNS.h:410-412)
+  GIP_VectorB200* now[] = {&u, &v, &w};
+  GIP_VectorB200* old_[] = {&u0, &v0, &w0};
+  for (int k = 0; k < 3; ++k)
+    gipb200_require(gipb200_dcopy(ops.n_inner, old_[k]->getDevicePtr(), now[k]->getDevicePtr(), 0),
+                    "gipb200_dcopy");
   gipb200_require(gipb200_stream_sync(0), "sync");
   gipb200_dns_destroy(E);
 }

@@ -6,6 +6,10 @@
 #include "GIP_VectorB200.h"
 
 GIP_MatrixB200::GIP_MatrixB200() : h(0) {
+  ss.op = 0;
+  ss.maxit = ss.n = ss.n_all = 0;
+  ss.pcg = 0;
+  ss.work = 0;
   csrValA = 0;
   csrColIndA = 0;
   csrRowIndA = 0;
@@ -15,6 +19,7 @@ GIP_MatrixB200::GIP_MatrixB200() : h(0) {
 }
 
 GIP_MatrixB200::~GIP_MatrixB200() {
+  release_solver_state();
   if (h) gipb200_matrix_destroy(h);
   delete[] csrValA;
   delete[] csrColIndA;
@@ -99,7 +104,17 @@ void GIP_MatrixB200::spmv(GIP_Vector* x, GIP_Matrix* target, double alpha, doubl
 // The Jacobi diagonal as a one-entry-per-row matrix, as GIP builds it
 // (GIP_MatrixMulticore::setUpDiagonal, GIP_MatrixMulticore.cpp:177-210): 1/A_ii, the last
 // diagonal entry of a row wins.  A row without a diagonal becomes an empty row.
+void GIP_MatrixB200::release_solver_state() {
+  if (ss.pcg) gipb200_pcg_destroy(ss.pcg);
+  if (ss.work) gipb200_free(ss.work);
+  ss.op = 0;
+  ss.maxit = ss.n = ss.n_all = 0;
+  ss.pcg = 0;
+  ss.work = 0;
+}
+
 void GIP_MatrixB200::setUpDiagonal(GIP_Matrix* A) {
+  release_solver_state();  // a new setUp: the solver's device state is rebuilt on demand
   num_rows = A->getNumRows();
   num_cols = A->getNumRows();
   const double* va = A->getCsrValA();

@@ -23,8 +23,22 @@ class GIP_MatrixB200 : public GIP_Matrix {
   double* getCsrValADevice() { return 0; }
   gipb200_matrix handle() const { return h; }
 
+  // Device state of the fused solver variants.  GIP_LinearSolver owns its Jacobi diagonal
+  // as a Matrix member (GIP_LinearSolver.h:20) and builds it in setUp (:40), so a state
+  // kept here lives exactly as long as the solver object and is dropped when setUp runs
+  // again: no table keyed by addresses, nothing outlives its operator's solver.
+  struct SolverState {
+    gipb200_matrix op;  // operator the state was built for (the solver's dA)
+    int maxit, n, n_all;
+    gipb200_pcg pcg;    // device-resident PCG (GIPB200_FUSED_PCG)
+    double* work;       // host-driven fused loop (GIPB200_FUSED_OPS): p Ap r z | dinv | scalars
+  };
+  SolverState& solver_state() { return ss; }
+  void release_solver_state();
+
  protected:
   void upload();
   gipb200_matrix h;
+  SolverState ss;
 };
 #endif

@@ -109,6 +109,38 @@ int gipb200_matrix_get_values(gipb200_matrix A, double* h_val);
  * *missing = rows without a diagonal entry (their dinv is 0). */
 int gipb200_matrix_inverse_diagonal(gipb200_matrix A, double* d_dinv, int* missing);
 
+/* ------------------------------------------------------------------ fused CG operations */
+/* For hosts that drive GIP's solver loop themselves (GIP_LinearSolver.h:85-116): one
+ * iteration is gipb200_matrix_spmv_dot, gipb200_cg_update_dot, gipb200_cg_direction --
+ * three launches in place of GIP's SpMV, two dots, diagonal SpMV and three axpys
+ * (libgpu.cu:75-203), with every scalar kept in device memory so the host never waits.
+ * Element arithmetic follows GIP's CPU rounding; the dots sum in a fixed two-level
+ * order.  Calls that share a matrix handle share its reduction scratch: order them on
+ * one stream. */
+typedef struct {
+  double rz;     /* r.z: the previous value on entry to cg_update_dot, the new one after */
+  double pAp;    /* p.Ap (point gipb200_matrix_spmv_dot's d_dot here)                    */
+  double alpha;  /* rz / pAp, written by cg_update_dot                                   */
+  double beta;   /* new rz / previous rz, written by cg_update_dot                       */
+  double rr;     /* r.r after the update                                                 */
+} gipb200_cg_scalars;
+/* GIP_cudaDCsrSpMV + GIP_cudaDdot (libgpu.cu:89-96, 187-203), the pair at
+ * GIP_LinearSolver.h:89-91: y = A x (rows without nonzeros keep y) and
+ * *d_dot = sum_{i < n_dot} x_i y_i, written to DEVICE memory.  x and y must not alias. */
+int gipb200_matrix_spmv_dot(gipb200_matrix A, const double* d_x, double* d_y, int n_dot,
+                            double* d_dot, void* stream);
+/* GIP_cudaDaxpy x2 + diagonal SpMV + GIP_cudaDdot (libgpu.cu:133-139, 89-96, 187-203), the
+ * sequence at GIP_LinearSolver.h:93-111: alpha = rz/pAp; x += alpha p; r -= alpha q;
+ * z = dinv r; then rz (new), rr = r.r, beta and alpha into *d_sc.  n <= rows of A (A
+ * supplies only the reduction scratch).  A row whose dinv is 0 gets z = 0. */
+int gipb200_cg_update_dot(gipb200_matrix A, int n, double* d_x, double* d_r, double* d_z,
+                          const double* d_p, const double* d_q, const double* d_dinv,
+                          gipb200_cg_scalars* d_sc, void* stream);
+/* GIP_cudaDaxpy(alpha,beta) (libgpu.cu:152-158) at GIP_LinearSolver.h:113:
+ * p = 1.0 z + beta p with beta read from *d_sc on the device. */
+int gipb200_cg_direction(int n, double* d_p, const double* d_z, const gipb200_cg_scalars* d_sc,
+                         void* stream);
+
 /* ------------------------------------------------------------------ PCG */
 typedef struct gipb200_pcg_s* gipb200_pcg;
 
@@ -176,18 +208,39 @@ int gipb200_pcg_get_info(gipb200_pcg S, gipb200_pcg_info* info);
 int gipb200_pcg_kernel_time(gipb200_pcg S, int reps, void* stream, double* avg_ms,
                             double* bytes);
 
+/* No counterpart in the reference (GIP has no multigrid): per-kernel profile of the AMG
+ * preconditioner.  Runs `reps` V-cycles on the solver's current residual after one
+ * untimed cycle, with a CUDA event on `stream` before every kernel, and reports each
+ * kernel of one cycle in launch order: its level, its kind (GIPB200_CYCLE_*), its mean
+ * time in ms and its algorithmic bytes (stored operator words once, every vector read
+ * or written once).  At most `cap` kernels are written; *n_kernels = kernels per cycle.
+ * Leaves the solution untouched; solve once first so the residual is set. */
+enum {
+  GIPB200_CYCLE_JACOBI0 = 0,   /* x = D^-1 b (pre-smoothing from zero)           */
+  GIPB200_CYCLE_RESIDUAL = 1,  /* t = b - A x                                    */
+  GIPB200_CYCLE_RESTRICT = 2,  /* b_coarse = R t                                 */
+  GIPB200_CYCLE_DENSE = 3,     /* coarsest level: x = A^-1 b (dense inverse)     */
+  GIPB200_CYCLE_PROLONG = 4,   /* x += P x_coarse                                */
+  GIPB200_CYCLE_SMOOTH = 5     /* x + D^-1 (b - A x) (level 0: with r.z)         */
+};
+int gipb200_pcg_vcycle_profile(gipb200_pcg S, int reps, void* stream, int cap, int* n_kernels,
+                               int* h_level, int* h_kind, double* h_ms, double* h_bytes);
+
 /* No counterpart in the reference.  A Jacobi-PCG solve for callers that cannot allocate
  * device memory at solve time (a framework-owned arena or caching allocator, code that
  * must not call cudaMalloc because it synchronises the device, embedders without
  * library handles).  The caller passes a device CSR operator (n rows), b (n), x and x0
  * (n_all = inner plus ghost cells, ghosts copied from x0), and d_stats (4 doubles out:
  * iterations, r.r, b.b, status).  mode: GIPB200_PCG_FIXED (exactly maxit iterations, as
- * GIP's solver) or GIPB200_PCG_TOL (stop at tol; maxit masked iterations are launched).
- * The solver's vectors and reductions use one file-scope device array of 8 MiB that
- * every GPU loading the library keeps until exit: n_all above 262144 is rejected with
- * GIPB200_ERR_ARG.  All calls share that array, so calls that overlap on the GPU race;
- * serialise them.  The first call on a device (with that device current) resolves the
- * array's address and clears it; make that first call before any stream capture. */
+ * GIP's solver) or GIPB200_PCG_TOL (stops on the device at tol; the host reads the stop
+ * flag every 32 iterations, waiting on `stream` each time).  Every column index must be
+ * below n_all; a row without a diagonal entry gets a zero Jacobi entry, as in
+ * gipb200_pcg_solve.  The solver's vectors and reductions use one file-scope device array
+ * of 8 MiB that every GPU loading the library keeps until exit: n_all above 262144 is
+ * rejected with GIPB200_ERR_ARG.  All calls share that array, so calls that overlap on
+ * the GPU race; serialise them.  Each call clears the array's reduction counter on its own
+ * stream.  The first call on a device (with that device current) resolves the array's
+ * address; make that first call before any stream capture. */
 int gipb200_pcg_solve_static(int n, int n_all, const int* d_rowptr, const int* d_col,
                              const double* d_val, const double* d_b, double* d_x,
                              const double* d_x0, int mode, int maxit, double tol,
@@ -279,6 +332,10 @@ int gipb200_dns_set_field(gipb200_dns E, const char* name, const double* h_in, i
 int gipb200_dns_field_ptr(gipb200_dns E, const char* name, double** d_ptr, int* n);
 /* Device-to-device copy of a field in the caller's numbering, on `stream`. */
 int gipb200_dns_copy_field(gipb200_dns E, const char* name, double* d_out, int n, void* stream);
+/* GIP_DNS's `time` member (GIP_DNS.h:400): sets the engine's simulated time, so an engine
+ * built from a GIP_DNS state continues GIP's clock; ordered on `stream`, returns once the
+ * value is on the device. */
+int gipb200_dns_set_time(gipb200_dns E, double time, void* stream);
 /* Current dt, sigma=1/dt and simulated time. */
 int gipb200_dns_scalars(gipb200_dns E, double* dt, double* sigma, double* time);
 
@@ -309,13 +366,23 @@ int gipb200_dns_snapshot(gipb200_dns E, int restore, void* stream);
  * step re-captures its graph. */
 int gipb200_dns_set_launch(gipb200_dns E, int spmv_blocks, int vec_blocks);
 
+/* Algorithmic bytes of each phase of one timestep, in the order of
+ * gipb200_dns_step_phases (h_bytes[7]; stored operator values and indices once, gathered
+ * vectors once, written vectors once).  The PCG entry is 0: a solve moves iterations x
+ * iteration_bytes plus replacements x replacement_bytes (gipb200_dns_get_info). */
+int gipb200_dns_phase_bytes(gipb200_dns E, double* h_bytes);
+/* gipb200_pcg_vcycle_profile for the engine's pressure solver (precond = AMG). */
+int gipb200_dns_vcycle_profile(gipb200_dns E, int reps, void* stream, int cap, int* n_kernels,
+                               int* h_level, int* h_kind, double* h_ms, double* h_bytes);
+
 /* Number of this library's kernels the engine has launched so far (a graph launch counts
  * the kernels it holds). */
 int gipb200_dns_launch_count(gipb200_dns E, long long* count);
 
 enum {
-  GIPB200_KERNEL_PCG_SPMV_DOT = 0,  /* FP64 PCG: Ap = L p fused with p.Ap           */
-  GIPB200_KERNEL_MIXED_SPMV_DOT = 1 /* FP32 inner PCG: Ap = (S L S) p fused with p.Ap */
+  GIPB200_KERNEL_PCG_SPMV_DOT = 0,   /* FP64 PCG: Ap = L p fused with p.Ap              */
+  GIPB200_KERNEL_MIXED_SPMV_DOT = 1, /* FP32 inner PCG: Ap = (S L S) p fused with p.Ap  */
+  GIPB200_KERNEL_MIXED_UPDATE = 2    /* FP32 inner PCG: y += alpha p, r -= alpha Ap, r.r */
 };
 /* Times `reps` back-to-back launches of one PCG kernel on the engine's resident operator
  * with CUDA events on `stream`; returns the mean launch time and the kernel's compulsory

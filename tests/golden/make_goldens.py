@@ -10,7 +10,8 @@ checkout exists; the fixtures then travel with the repository).
 It also writes the merged C100K single-rank set to ``oracle/_ref/c100k`` (git-ignored;
 it travels with the tree for the GPU known-answer test).
 
-Usage: python tests/golden/make_goldens.py [--reference /root/reference]
+Usage: python tests/golden/make_goldens.py --reference <GIP checkout>
+(or with the checkout's path in the GIP_REFERENCE environment variable)
 """
 from __future__ import annotations
 
@@ -47,8 +48,11 @@ def run_ref(cwd: str, case: str, nranks: int, steps: int = 10, dump: str = "-", 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("GIP_REFERENCE"),
+                    help="the GIP checkout (default: $GIP_REFERENCE)")
     a = ap.parse_args()
+    if not a.reference:
+        ap.error("--reference <GIP checkout> (or GIP_REFERENCE) is required")
     subprocess.check_call(["make", "-s", "-C", os.path.join(REPO, "oracle"), "all",
                            f"REF={a.reference}"])
     readme = open(os.path.join(a.reference, "README.md")).read().splitlines()

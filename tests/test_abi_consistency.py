@@ -95,7 +95,8 @@ KIND = {"int": C.c_int, "double": C.c_double, "long long": C.c_longlong}
 STRUCTS = {"gipb200_host_csr": _lib.HostCsr, "gipb200_dns_ops": _lib.DnsOps,
            "gipb200_pcg_params": _lib.PcgParams, "gipb200_pcg_result": _lib.PcgResult,
            "gipb200_dns_params": _lib.DnsParams, "gipb200_pcg_info": _lib.PcgInfo,
-           "gipb200_dns_info": _lib.DnsInfo, "gipb200_adjoint_params": _lib.AdjointParams}
+           "gipb200_dns_info": _lib.DnsInfo, "gipb200_adjoint_params": _lib.AdjointParams,
+           "gipb200_cg_scalars": _lib.CgScalars}
 
 
 @pytest.mark.parametrize("cname", sorted(STRUCTS))

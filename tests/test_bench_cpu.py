@@ -26,6 +26,11 @@ def test_reference_arm_line():
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
     assert d["config"]["cells"] == 12 ** 3
+    # the headline is GIP's stock step, measured as it ships (100 PCG iterations), and the
+    # config says what ran: FP64, GIP's Jacobi, GIP's own decomposition
+    assert d["pcg_iterations_per_step"] == 100 and "fixed 100" in d["config"]["pcg"]
+    assert d["config"]["precond"] == "jacobi" and d["config"]["form"].startswith("FP64")
+    assert d["value"] == d["samples"]["100"]["ms_per_step"]
     # GIP's own per-step line after the untimed and the timed steps (3 timesteps of dt 0.1)
     for s in d["samples"].values():
         assert s["last_line"].startswith("time 3.000000e-01")
