@@ -97,6 +97,8 @@ _SIGNATURES = {
     "gipb200_daxpy": (_I, [_I, _VP, _VP, _D, _VP]),
     "gipb200_daxpby": (_I, [_I, _VP, _VP, _D, _D, _VP]),
     "gipb200_dfill": (_I, [_I, _VP, _D, _VP]),
+    "gipb200_gather": (_I, [_I, _VP, _VP, _VP, _VP]),
+    "gipb200_scatter": (_I, [_I, _VP, _VP, _VP, _VP]),
     "gipb200_ddot": (_I, [_I, _VP, _VP, C.POINTER(_D), _VP]),
     "gipb200_dnorminf": (_I, [_I, _VP, C.POINTER(_D), _VP]),
     "gipb200_cfl": (_I, [_I, _VP, _VP, _VP, _VP, _D, _D, C.POINTER(_D), _VP]),

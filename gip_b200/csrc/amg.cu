@@ -460,13 +460,14 @@ __global__ void __launch_bounds__(256) k_amg_jacobi0(int n, const T* __restrict_
     x[i] = dinv[i] * b[i];
 }
 
-enum { kResid = 0, kPlain = 1, kAdd = 2, kSmooth = 3 };
-// kResid: y = b - A x;  kPlain: y = A x;  kAdd: y += A x;  kSmooth: y = x + dinv (b - A x)
+enum { kResid = 0, kPlain = 1, kAdd = 2, kSmooth = 3, kScaleAdd = 4 };
+// kResid: y = b - A x;  kPlain: y = A x;  kAdd: y += A x;  kSmooth: y = x + dinv (b - A x);
+// kScaleAdd: y = w b + A x (the level-0 prolongation onto x0 = w r, never formed)
 template <typename T, int MODE, typename V = T>
 __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __restrict__ x,
                                                      const T* __restrict__ b,
                                                      const T* __restrict__ dinv,
-                                                     T* __restrict__ y, PcgScalars* S) {
+                                                     T* __restrict__ y, PcgScalars* S, T w) {
   if (amg_enter(S)) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -475,9 +476,10 @@ __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __r
     const T sum = amg_row<T, 4, V>(A, x, s, lane);
     const int i = s * 32 + lane;
     if (i < A.nrows) {
-      if (MODE == kResid) y[i] = b[i] - sum;
+      if (MODE == kResid) y[i] = (w == T(1)) ? b[i] - sum : fmat(-w, sum, b[i]);
       else if (MODE == kPlain) y[i] = sum;
       else if (MODE == kAdd) y[i] += sum;
+      else if (MODE == kScaleAdd) y[i] = fmat(w, b[i], sum);
       else y[i] = fmat(dinv[i], b[i] - sum, x[i]);
     }
   }
@@ -493,7 +495,7 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
                                                  const V* __restrict__ val, const T* __restrict__ x,
                                                  const T* __restrict__ b,
                                                  const T* __restrict__ dinv, T* __restrict__ y,
-                                                 PcgScalars* S) {
+                                                 PcgScalars* S, T w) {
   if (amg_enter(S)) return;
   constexpr int RPW = 32 / LANES;  // rows per warp per pass
   const int lane = threadIdx.x & 31, sub = lane % LANES;
@@ -508,9 +510,10 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
 #pragma unroll
     for (int o = LANES / 2; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o, LANES);
     if (i < nrows && sub == 0) {
-      if (MODE == kResid) y[i] = b[i] - sum;
+      if (MODE == kResid) y[i] = (w == T(1)) ? b[i] - sum : fmat(-w, sum, b[i]);
       else if (MODE == kPlain) y[i] = sum;
       else if (MODE == kAdd) y[i] += sum;
+      else if (MODE == kScaleAdd) y[i] = fmat(w, b[i], sum);
       else y[i] = fmat(dinv[i], b[i] - sum, x[i]);
     }
   }
@@ -521,32 +524,32 @@ int vec_blocks(int n);
 // y (mode) A x for an AMG operator in either form.
 template <typename T, int MODE, typename V>
 void amg_mv_v(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const T* b,
-              const T* dinv, T* y, PcgScalars* S, cudaStream_t s) {
+              const T* dinv, T* y, PcgScalars* S, cudaStream_t s, T w) {
   if (M.lanes == 0) {
-    k_amg_spmv<T, MODE, V><<<vec_blocks(M.nslices * 32), 256, 0, s>>>(view, x, b, dinv, y, S);
+    k_amg_spmv<T, MODE, V><<<vec_blocks(M.nslices * 32), 256, 0, s>>>(view, x, b, dinv, y, S, w);
     return;
   }
   const int nb = vec_blocks((int)std::min<long long>((long long)M.nrows * M.lanes, 1LL << 30));
   const int* rp = M.rp.p;
   const int* ci = M.col.p;
   if (M.lanes == 32)
-    k_amg_csr<T, MODE, 32, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
+    k_amg_csr<T, MODE, 32, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
   else if (M.lanes == 16)
-    k_amg_csr<T, MODE, 16, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
+    k_amg_csr<T, MODE, 16, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
   else
-    k_amg_csr<T, MODE, 8, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S);
+    k_amg_csr<T, MODE, 8, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
 }
 
 template <typename T, int MODE>
 void amg_mv(const SellT<T>& M, const T* x, const T* b, const T* dinv, T* y, PcgScalars* S,
-            cudaStream_t s) {
+            cudaStream_t s, T w = T(1)) {
   if constexpr (std::is_same<T, float>::value) {
     if (M.half) {
-      amg_mv_v<T, MODE, __half>(M, M.hview(), M.hval.p, x, b, dinv, y, S, s);
+      amg_mv_v<T, MODE, __half>(M, M.hview(), M.hval.p, x, b, dinv, y, S, s, w);
       return;
     }
   }
-  amg_mv_v<T, MODE, T>(M, M.view(), M.val.p, x, b, dinv, y, S, s);
+  amg_mv_v<T, MODE, T>(M, M.view(), M.val.p, x, b, dinv, y, S, s, w);
 }
 
 struct CycleFinish {
@@ -564,13 +567,14 @@ struct CycleFinish {
   }
 };
 
-// Level 0 post-smoothing with the dot: z = x + dinv (r - A x), r.z, beta.
+// Level 0 post-smoothing with the dot: z = x + d (r - A x), r.z, beta; d = dinv[i], or the
+// constant w when dinv is null (unit-diagonal level 0).
 template <typename T>
 __global__ void __launch_bounds__(256, 8) k_amg_smooth_dot(SellView<T> A, const T* __restrict__ x,
                                                            const T* __restrict__ r,
                                                            const T* __restrict__ dinv,
                                                            T* __restrict__ z, PcgScalars* S,
-                                                           ReduceScratch rs, int first) {
+                                                           ReduceScratch rs, int first, T w) {
   if (amg_enter(S)) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -581,7 +585,7 @@ __global__ void __launch_bounds__(256, 8) k_amg_smooth_dot(SellView<T> A, const 
     const int i = s * 32 + lane;
     if (i < A.nrows) {
       const T ri = r[i];
-      const T zi = fmat(dinv[i], ri - sum, x[i]);
+      const T zi = fmat(dinv ? dinv[i] : w, ri - sum, x[i]);
       z[i] = zi;
       acc[0] += (double)ri * (double)zi;
     }
@@ -590,14 +594,15 @@ __global__ void __launch_bounds__(256, 8) k_amg_smooth_dot(SellView<T> A, const 
 }
 
 // Level-0 products from the packed FP32 operator (same FMA order as the plain layout, so
-// the same results): kResid y = b - A x; kSmooth z = x + dinv (r - A x) with r.z and beta.
+// the same results): kResid y = b - w A x; kSmooth z = x + d (r - A x) with r.z and beta,
+// d = dinv[i], or the constant w when dinv is null (unit-diagonal level 0).
 template <int NIB, int K, int MODE>
 __global__ void __launch_bounds__(256, 8) k_amgp_spmv(SellView<float> A, PackedView pk,
                                                       const float* __restrict__ x,
                                                       const float* __restrict__ b,
                                                       const float* __restrict__ dinv,
                                                       float* __restrict__ y, PcgScalars* S,
-                                                      ReduceScratch rs, int first) {
+                                                      ReduceScratch rs, int first, float w) {
   if (amg_enter(S)) return;
   constexpr int NT = 1 << NIB;
   __shared__ float tab[NT];
@@ -642,10 +647,10 @@ __global__ void __launch_bounds__(256, 8) k_amgp_spmv(SellView<float> A, PackedV
     }
     if (i < A.nrows) {
       if (MODE == kResid) {
-        y[i] = b[i] - sum;
+        y[i] = (w == 1.0f) ? b[i] - sum : fmaf(-w, sum, b[i]);
       } else {
         const float ri = b[i];
-        const float zi = fmaf(dinv[i], ri - sum, x[i]);
+        const float zi = fmaf(dinv ? dinv[i] : w, ri - sum, x[i]);
         y[i] = zi;
         acc[0] += (double)ri * (double)zi;
       }
@@ -657,15 +662,15 @@ __global__ void __launch_bounds__(256, 8) k_amgp_spmv(SellView<float> A, PackedV
 template <int MODE>
 void launch_amgp(const PackedView& pk, SellView<float> A, int nb, const float* x, const float* b,
                  const float* dinv, float* y, PcgScalars* S, ReduceScratch rs, int first,
-                 cudaStream_t s) {
+                 cudaStream_t s, float w) {
   if (pk.nib == 4 && pk.slots == 7)
-    k_amgp_spmv<4, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first);
+    k_amgp_spmv<4, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w);
   else if (pk.nib == 4)
-    k_amgp_spmv<4, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first);
+    k_amgp_spmv<4, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w);
   else if (pk.slots == 7)
-    k_amgp_spmv<8, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first);
+    k_amgp_spmv<8, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w);
   else
-    k_amgp_spmv<8, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first);
+    k_amgp_spmv<8, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w);
 }
 
 // Coarsest level: x = C b, one warp per row of the dense inverse.
@@ -698,9 +703,9 @@ int vec_blocks(int n) {
 template <int MODE, typename T>
 void launch_packed0(const PackedView& pk, SellView<T> A, int nb, const T* x, const T* b,
                     const T* dinv, T* y, PcgScalars* S, ReduceScratch rs, int first,
-                    cudaStream_t s) {
+                    cudaStream_t s, T w = T(1)) {
   if constexpr (std::is_same<T, float>::value)
-    launch_amgp<MODE>(pk, A, nb, x, b, dinv, y, S, rs, first, s);
+    launch_amgp<MODE>(pk, A, nb, x, b, dinv, y, S, rs, first, s, w);
 }
 
 namespace {
@@ -802,6 +807,14 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
     L.n = A.nr;
     std::vector<T> dinv((size_t)A.nr);
     for (int i = 0; i < A.nr; ++i) dinv[i] = (T)(H.w / (*H.d)[i]);
+    if (H.l == 0) {
+      // the residual then gathers r (length n) where it gathered x0 (length x0_len): only
+      // when level 0's operator gathers no column past n
+      bool unit = A.nr > 0 && x0_len <= A.nr && !getenv("GIPB200_AMG_ROWDIAG");
+      for (int i = 0; i < A.nr && unit; ++i) unit = std::fabs((*H.d)[i] - 1.0) <= 0.1;
+      unit0 = unit;
+      omega0 = H.w;
+    }
     GIPB_TRY(L.dinv.upload(dinv.data(), dinv.size(), s));
     GIPB_TRY(L.x.alloc((size_t)(H.l == 0 ? std::max(A.nr, x0_len) : A.nr)));
     GIPB_TRY(L.x.zero(s));  // level 0: entries past n are gathered (as zero) by A0
@@ -867,19 +880,25 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
   };
   auto a_bytes = [&](int l) { return l == 0 ? a0_stream_bytes : stream_bytes(lv[l]->A); };
   // downward: pre-smooth from zero, residual, restriction
+  const bool u0 = unit0;  // level 0 never forms x0 = omega0 r
   for (int l = 0; l < L - 1; ++l) {
     const AmgLevel<T>& V = *lv[l];
     const T* b = l == 0 ? r : V.b.p;
     const double n = V.n, nn = lv[l + 1]->n;
-    GIPB_TRY(mark(l, GIPB200_CYCLE_JACOBI0, 3.0 * n * w));
-    k_amg_jacobi0<T><<<vec_blocks(V.n), 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
-    GIPB_TRY(mark(l, GIPB200_CYCLE_RESIDUAL, a_bytes(l) + 3.0 * n * w));
+    const bool skip = l == 0 && u0;
+    if (!skip) {
+      GIPB_TRY(mark(l, GIPB200_CYCLE_JACOBI0, 3.0 * n * w));
+      k_amg_jacobi0<T><<<vec_blocks(V.n), 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
+    }
+    GIPB_TRY(mark(l, GIPB200_CYCLE_RESIDUAL, a_bytes(l) + (skip ? 2.0 : 3.0) * n * w));
     if (l == 0) {
       const int bs = vec_blocks(A0.nslices * 32);
       if (packed)
-        launch_packed0<kResid>(*pk, A0, bs, V.x.p, b, (const T*)nullptr, V.t.p, S, rs, first, s);
+        launch_packed0<kResid>(*pk, A0, bs, skip ? r : V.x.p, b, (const T*)nullptr, V.t.p, S, rs,
+                               first, s, skip ? (T)omega0 : T(1));
       else
-        k_amg_spmv<T, kResid><<<bs, 256, 0, s>>>(A0, V.x.p, b, nullptr, V.t.p, S);
+        k_amg_spmv<T, kResid><<<bs, 256, 0, s>>>(A0, skip ? r : V.x.p, b, nullptr, V.t.p, S,
+                                                  skip ? (T)omega0 : T(1));
     } else {
       amg_mv<T, kResid>(V.A, V.x.p, b, (const T*)nullptr, V.t.p, S, s);
     }
@@ -895,15 +914,21 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     const AmgLevel<T>& V = *lv[l];
     const T* xc = (l + 1 == L - 1) ? lv[l + 1]->x.p : lv[l + 1]->t.p;
     const double n = V.n, nn = lv[l + 1]->n;
+    const bool skip = l == 0 && u0;
     GIPB_TRY(mark(l, GIPB200_CYCLE_PROLONG, stream_bytes(V.P) + (nn + 2.0 * n) * w));
-    amg_mv<T, kAdd>(V.P, xc, (const T*)nullptr, (const T*)nullptr, V.x.p, S, s);
-    GIPB_TRY(mark(l, GIPB200_CYCLE_SMOOTH, a_bytes(l) + 4.0 * n * w));
+    if (skip)  // x0 = omega0 r + P x1
+      amg_mv<T, kScaleAdd>(V.P, xc, r, (const T*)nullptr, V.x.p, S, s, (T)omega0);
+    else
+      amg_mv<T, kAdd>(V.P, xc, (const T*)nullptr, (const T*)nullptr, V.x.p, S, s);
+    GIPB_TRY(mark(l, GIPB200_CYCLE_SMOOTH, a_bytes(l) + (skip ? 3.0 : 4.0) * n * w));
     if (l == 0) {
       const int bs = vec_blocks(A0.nslices * 32);
       if (packed)
-        launch_packed0<kSmooth>(*pk, A0, bs, V.x.p, r, V.dinv.p, z0, S, rs, first, s);
+        launch_packed0<kSmooth>(*pk, A0, bs, V.x.p, r, skip ? (const T*)nullptr : V.dinv.p, z0,
+                                S, rs, first, s, (T)omega0);
       else
-        k_amg_smooth_dot<T><<<bs, 256, 0, s>>>(A0, V.x.p, r, V.dinv.p, z0, S, rs, first);
+        k_amg_smooth_dot<T><<<bs, 256, 0, s>>>(A0, V.x.p, r, skip ? (const T*)nullptr : V.dinv.p,
+                                               z0, S, rs, first, (T)omega0);
     } else {
       amg_mv<T, kSmooth>(V.A, V.x.p, V.b.p, V.dinv.p, V.t.p, S, s);
     }
@@ -922,11 +947,12 @@ double AmgT<T>::cycle_bytes(double a0_stream_bytes) const {
     const AmgLevel<T>& V = *lv[l];
     const double n = V.n, nn = lv[l + 1]->n;
     const double a = l == 0 ? a0_stream_bytes : stream_bytes(V.A);
-    b += 3.0 * n * w;                                    // x = dinv b
-    b += a + 3.0 * n * w;                                // t = b - A x
+    const bool skip = l == 0 && unit0;                   // x0 = omega0 r not formed
+    if (!skip) b += 3.0 * n * w;                         // x = dinv b
+    b += a + (skip ? 2.0 : 3.0) * n * w;                 // t = b - A x
     b += stream_bytes(V.R) + (n + nn) * w;               // b_next = R t
     b += stream_bytes(V.P) + (nn + 2.0 * n) * w;         // x += P x_next
-    b += a + 4.0 * n * w;                                // smoothed x
+    b += a + (skip ? 3.0 : 4.0) * n * w;                 // smoothed x
   }
   b += ((double)nc * nc + 2.0 * nc) * w;                 // dense coarsest
   return b;

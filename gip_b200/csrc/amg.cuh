@@ -71,6 +71,12 @@ struct AmgT {
   int nc = 0;             // coarsest size: solved with a dense (pseudo-)inverse
   DevBuf<T> cinv;         // nc x nc, row-major
   double op_complexity = 0.0, setup_s = 0.0;
+  // Level 0 has a unit diagonal (the Jacobi-scaled operator, to within 10%): its smoother
+  // is the constant weight omega0 = w, so the cycle never forms x0 = omega0 r (the residual
+  // gathers r and scales the product) and reads no diagonal.  A fixed symmetric smoother
+  // like the per-row one, so the cycle stays a symmetric positive definite operator.
+  bool unit0 = false;
+  double omega0 = 0.0;
 
   // Hierarchy of the n x n operator (host CSR, FP64 values; columns < n), near-null
   // vector z.  singular: the operator annihilates z (pinned-Neumann inner system), so the

@@ -219,6 +219,17 @@ __global__ void k_axpby(int n, double* __restrict__ y, const double* __restrict_
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     y[i] = dadd(dmul(a, x[i]), dmul(b, y[i]));
 }
+// GIP_Topo::pack / unpack (GIP_Topo.cpp:109-122) kept in device memory
+__global__ void k_gather(int n, const int* __restrict__ idx, const double* __restrict__ x,
+                         double* __restrict__ buf) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    buf[k] = x[idx[k]];
+}
+__global__ void k_scatter(int n, const int* __restrict__ idx, const double* __restrict__ buf,
+                          double* __restrict__ x) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    x[idx[k]] = buf[k];
+}
 __global__ void k_fill(int n, double* __restrict__ y, double v) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = v;
 }
@@ -425,6 +436,28 @@ int gipb200_dfill(int n, double* y, double v, void* stream) {
   int b;
   GIPB_TRY(grid_blocks(256, n, 4, 0, &b));
   k_fill<<<b, 256, 0, as_stream(stream)>>>(n, y, v);
+  GIPB_LAUNCH_CHECK();
+  return GIPB200_OK;
+}
+
+int gipb200_gather(int n, const int* d_idx, const double* d_x, double* d_buf, void* stream) {
+  if (n < 0 || (n > 0 && (!d_idx || !d_x || !d_buf)))
+    return fail(GIPB200_ERR_ARG, "gather: bad size or null pointer");
+  if (n == 0) return GIPB200_OK;
+  int b;
+  GIPB_TRY(grid_blocks(256, n, 4, 0, &b));
+  k_gather<<<b, 256, 0, as_stream(stream)>>>(n, d_idx, d_x, d_buf);
+  GIPB_LAUNCH_CHECK();
+  return GIPB200_OK;
+}
+
+int gipb200_scatter(int n, const int* d_idx, const double* d_buf, double* d_x, void* stream) {
+  if (n < 0 || (n > 0 && (!d_idx || !d_x || !d_buf)))
+    return fail(GIPB200_ERR_ARG, "scatter: bad size or null pointer");
+  if (n == 0) return GIPB200_OK;
+  int b;
+  GIPB_TRY(grid_blocks(256, n, 4, 0, &b));
+  k_scatter<<<b, 256, 0, as_stream(stream)>>>(n, d_idx, d_buf, d_x);
   GIPB_LAUNCH_CHECK();
   return GIPB200_OK;
 }

@@ -129,6 +129,8 @@ class GipCase:
     fields: Dict[str, np.ndarray]
     topo_cols: Topo
     topo_faces: Topo
+    # global id of every local cell (split_ranks sets it: local cell k is global cell_ids[k])
+    cell_ids: Optional[np.ndarray] = None
 
     @property
     def n_inner(self) -> int:
@@ -470,7 +472,7 @@ def split_ranks(c: GipCase, cell_part: np.ndarray, nparts: int) -> List[GipCase]
         z = np.zeros(nparts + 1, np.int32)
         tf = Topo(fr.size, fr.size, ni, nif, nb, nh, np.zeros(0, np.int32), z,
                   np.zeros(0, np.int32), z.copy())
-        parts.append(GipCase(ops, fields, tc, tf))
+        parts.append(GipCase(ops, fields, tc, tf, cell_ids=order.copy()))
     return parts
 
 

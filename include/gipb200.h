@@ -75,6 +75,12 @@ int gipb200_daxpby(int n, double* d_y, const double* d_x, double alpha, double b
                    void* stream);
 /* GIP_VectorCuda::operator=(int) (GIP_VectorCuda.cpp:190-195): y[0:n) = value */
 int gipb200_dfill(int n, double* d_y, double value, void* stream);
+/* GIP_Topo::pack (src/BasicInterfaces/GIP_Topo.cpp:109-115) in device memory:
+ * d_buf[k] = d_x[d_idx[k]] for k < n (the interface cells a neighbour reads). */
+int gipb200_gather(int n, const int* d_idx, const double* d_x, double* d_buf, void* stream);
+/* GIP_Topo::unpack (GIP_Topo.cpp:116-122) in device memory: d_x[d_idx[k]] = d_buf[k]
+ * (the halo cells received); indices must be distinct. */
+int gipb200_scatter(int n, const int* d_idx, const double* d_buf, double* d_x, void* stream);
 /* GIP_cudaDdot (libgpu.cu:160-203): *h_result = sum x[i]*y[i], one pass, deterministic
  * two-level order; blocks until the result is on the host. */
 int gipb200_ddot(int n, const double* d_x, const double* d_y, double* h_result, void* stream);

@@ -87,4 +87,4 @@ def test_adjoint_config_64cube_50_steps(gpu):
         fd = (A.forward(lid + eps * d[:-1], nu0 + eps * d[-1], steps) -
               A.forward(lid - eps * d[:-1], nu0 - eps * d[-1], steps)) / (2 * eps)
         errs.append(abs(fd - g @ d) / max(abs(fd), 1e-300))
-    assert max(errs) < 1e-5, errs
+    assert max(errs) < 1e-6, errs
