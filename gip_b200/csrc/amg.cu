@@ -353,8 +353,10 @@ bool dense_inverse(int m, std::vector<double>& M, std::vector<double>& inv) {
   return true;
 }
 
+// compact: a long-row (CSR) operator whose column offsets from the row all fit in int16 is
+// stored with 16-bit offsets and FP16 values (the FP32 cycle's coarse operators).
 template <typename T>
-int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false) {
+int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool compact = false) {
   S->half = half;
   GIPB_TRY(validate_csr(A.nr, A.nc, (int)A.nnz(), A.rp.data(), A.ci.data(), A.nc, "AMG operator"));
   S->nrows = A.nr;
@@ -365,7 +367,20 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false) {
   if (avg >= 12.0) {  // long rows: CSR, 8 to 32 threads per row
     S->lanes = avg >= 48.0 ? 32 : avg >= 24.0 ? 16 : 8;
     GIPB_TRY(S->rp.upload(A.rp.data(), A.rp.size(), s));
-    GIPB_TRY(S->col.upload(A.ci.data(), std::max<size_t>(A.ci.size(), 1), s));
+    bool fits = compact && std::is_same<T, float>::value;
+    for (int r = 0; r < A.nr && fits; ++r)
+      for (int k = A.rp[r]; k < A.rp[r + 1] && fits; ++k)
+        fits = std::abs(A.ci[k] - r) <= 32767;
+    if (fits) {
+      S->short_cols = true;
+      S->half = half = true;
+      std::vector<short> dc(std::max<size_t>(A.ci.size(), 1), 0);
+      for (int r = 0; r < A.nr; ++r)
+        for (int k = A.rp[r]; k < A.rp[r + 1]; ++k) dc[k] = (short)(A.ci[k] - r);
+      GIPB_TRY(S->dcol.upload(dc.data(), dc.size(), s));
+    } else {
+      GIPB_TRY(S->col.upload(A.ci.data(), std::max<size_t>(A.ci.size(), 1), s));
+    }
     if (half) {
       std::vector<__half> hv(std::max<size_t>(A.v.size(), 1), __float2half_rn(0.0f));
       for (size_t k = 0; k < A.v.size(); ++k) hv[k] = __float2half_rn((float)A.v[k]);
@@ -425,11 +440,11 @@ __device__ __forceinline__ float to_arith(__half v) { return __half2float(v); }
 __device__ __forceinline__ float to_arith(float v) { return v; }
 __device__ __forceinline__ double to_arith(double v) { return v; }
 
-// One row of a sliced operator, summed slot by slot (padding: column -1, skipped).
+// One row of a sliced operator whose slice starts at slot `base` and has `len` slots,
+// summed slot by slot (padding: column -1, skipped).
 template <typename T, int CH, typename V = T>
-__device__ __forceinline__ T amg_row(const SellView<V>& A, const T* __restrict__ x, int s, int lane) {
-  const long long base = A.sptr[s];
-  const int len = (int)((A.sptr[s + 1] - base) >> 5);
+__device__ __forceinline__ T amg_row_at(const SellView<V>& A, const T* __restrict__ x,
+                                        long long base, int len, int lane) {
   const int* cp = A.col + base + lane;
   const V* vp = A.val + base + lane;
   T sum = T(0);
@@ -450,6 +465,12 @@ __device__ __forceinline__ T amg_row(const SellView<V>& A, const T* __restrict__
   return sum;
 }
 
+template <typename T, int CH, typename V = T>
+__device__ __forceinline__ T amg_row(const SellView<V>& A, const T* __restrict__ x, int s, int lane) {
+  const long long base = A.sptr[s];
+  return amg_row_at<T, CH, V>(A, x, base, (int)((A.sptr[s + 1] - base) >> 5), lane);
+}
+
 // x = dinv b
 template <typename T>
 __global__ void __launch_bounds__(256) k_amg_jacobi0(int n, const T* __restrict__ dinv,
@@ -467,16 +488,25 @@ template <typename T, int MODE, typename V = T>
 __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __restrict__ x,
                                                      const T* __restrict__ b,
                                                      const T* __restrict__ dinv,
-                                                     T* __restrict__ y, PcgScalars* S, T w) {
+                                                     T* __restrict__ y, PcgScalars* S, T w,
+                                                     const int* __restrict__ yperm = nullptr) {
   if (amg_enter(S)) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
+  // the next slice's slot range is loaded while this slice's gathers are in flight
+  long long b0 = 0, b1 = 0;
+  if (gw < A.nslices) b0 = __ldg(A.sptr + gw), b1 = __ldg(A.sptr + gw + 1);
   for (int s = gw; s < A.nslices; s += nw) {
-    const T sum = amg_row<T, 4, V>(A, x, s, lane);
+    long long n0 = 0, n1 = 0;
+    if (s + nw < A.nslices) n0 = __ldg(A.sptr + s + nw), n1 = __ldg(A.sptr + s + nw + 1);
+    const T sum = amg_row_at<T, 4, V>(A, x, b0, (int)((b1 - b0) >> 5), lane);
+    b0 = n0;
+    b1 = n1;
     const int i = s * 32 + lane;
     if (i < A.nrows) {
-      if (MODE == kResid) y[i] = (w == T(1)) ? b[i] - sum : fmat(-w, sum, b[i]);
+      // kResid: level 0 may write its residual in aggregate order (yperm)
+      if (MODE == kResid) y[yperm ? yperm[i] : i] = (w == T(1)) ? b[i] - sum : fmat(-w, sum, b[i]);
       else if (MODE == kPlain) y[i] = sum;
       else if (MODE == kAdd) y[i] += sum;
       else if (MODE == kScaleAdd) y[i] = fmat(w, b[i], sum);
@@ -488,25 +518,53 @@ __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __r
 // The same products from the CSR form: LANES threads per row, each summing a strided part
 // of the row, combined by a fixed shuffle tree (deterministic).  The row loop is uniform
 // across the warp (32 / LANES rows per warp per pass), so every lane takes part in the
-// shuffles.
-template <typename T, int MODE, int LANES, typename V = T>
+// shuffles.  Software-pipelined: the next pass's row bounds are loaded while this pass's
+// gathers are in flight, and each lane loads up to U of its entries before gathering
+// them, so a pass costs two dependent memory round trips instead of two per entry plus
+// one for the bounds.  Each lane still adds its entries in increasing order.
+template <typename T, int MODE, int LANES, typename V = T, typename CI = int>
 __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restrict__ rp,
-                                                 const int* __restrict__ col,
+                                                 const CI* __restrict__ col,
                                                  const V* __restrict__ val, const T* __restrict__ x,
                                                  const T* __restrict__ b,
                                                  const T* __restrict__ dinv, T* __restrict__ y,
                                                  PcgScalars* S, T w) {
   if (amg_enter(S)) return;
   constexpr int RPW = 32 / LANES;  // rows per warp per pass
+  constexpr int U = 4;             // entries a lane loads before their gathers
   const int lane = threadIdx.x & 31, sub = lane % LANES;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int r0 = gw * RPW; r0 < nrows; r0 += nw * RPW) {
+  int r0 = gw * RPW;
+  int kb = 0, ke = 0;
+  {
     const int i = r0 + lane / LANES;
+    if (i < nrows) kb = __ldg(rp + i), ke = __ldg(rp + i + 1);
+  }
+  for (; r0 < nrows; r0 += nw * RPW) {
+    const int i = r0 + lane / LANES;
+    int kbn = 0, ken = 0;  // the next pass's row, loaded ahead
+    const int in = i + nw * RPW;
+    if (in < nrows) kbn = __ldg(rp + in), ken = __ldg(rp + in + 1);
     T sum = T(0);
-    if (i < nrows)
-      for (int k = rp[i] + sub; k < rp[i + 1]; k += LANES)
-        sum = fmat((T)to_arith(ld_stream(val + k)), __ldg(x + ld_stream(col + k)), sum);
+    for (int k0 = kb + sub; k0 < ke; k0 += U * LANES) {
+      int c[U];
+      V v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u * LANES;
+        // 16-bit columns are offsets from the row
+        c[u] = (k < ke) ? (sizeof(CI) == 2 ? i + (int)ld_stream(col + k) : (int)ld_stream(col + k))
+                        : -1;
+        v[u] = (k < ke) ? ld_stream(val + k) : V(0);
+      }
+      T xv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) xv[u] = (c[u] >= 0) ? __ldg(x + c[u]) : T(0);
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (c[u] >= 0) sum = fmat((T)to_arith(v[u]), xv[u], sum);
+    }
 #pragma unroll
     for (int o = LANES / 2; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o, LANES);
     if (i < nrows && sub == 0) {
@@ -516,6 +574,8 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
       else if (MODE == kScaleAdd) y[i] = fmat(w, b[i], sum);
       else y[i] = fmat(dinv[i], b[i] - sum, x[i]);
     }
+    kb = kbn;
+    ke = ken;
   }
 }
 
@@ -531,6 +591,16 @@ void amg_mv_v(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const
   }
   const int nb = vec_blocks((int)std::min<long long>((long long)M.nrows * M.lanes, 1LL << 30));
   const int* rp = M.rp.p;
+  if (M.short_cols) {
+    const short* ci = M.dcol.p;
+    if (M.lanes == 32)
+      k_amg_csr<T, MODE, 32, V, short><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
+    else if (M.lanes == 16)
+      k_amg_csr<T, MODE, 16, V, short><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
+    else
+      k_amg_csr<T, MODE, 8, V, short><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
+    return;
+  }
   const int* ci = M.col.p;
   if (M.lanes == 32)
     k_amg_csr<T, MODE, 32, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
@@ -602,7 +672,8 @@ __global__ void __launch_bounds__(256, 8) k_amgp_spmv(SellView<float> A, PackedV
                                                       const float* __restrict__ b,
                                                       const float* __restrict__ dinv,
                                                       float* __restrict__ y, PcgScalars* S,
-                                                      ReduceScratch rs, int first, float w) {
+                                                      ReduceScratch rs, int first, float w,
+                                                      const int* __restrict__ yperm) {
   if (amg_enter(S)) return;
   constexpr int NT = 1 << NIB;
   __shared__ float tab[NT];
@@ -612,42 +683,28 @@ __global__ void __launch_bounds__(256, 8) k_amgp_spmv(SellView<float> A, PackedV
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   double acc[1] = {0.0};
+  PackedWords cur, nxt;
+  if (gw < A.nslices) packed_words<NIB>(pk.delta, pk.idx, pk.plain, gw, lane, cur);
+  nxt = cur;
   for (int s = gw; s < A.nslices; s += nw) {
+    if (s + nw < A.nslices) packed_words<NIB>(pk.delta, pk.idx, pk.plain, s + nw, lane, nxt);
     const int i = s * 32 + lane;
     float sum;
-    if (__ldg(pk.plain + s)) {
+    if (cur.plain) {
       sum = amg_row<float, 2>(A, x, s, lane);
     } else {
-      const uint4 d = ld_stream(pk.delta + i);
-      unsigned w0, w1;
-      if (NIB == 4) {
-        w0 = ld_stream(static_cast<const unsigned*>(pk.idx) + i);
-        w1 = 0u;
-      } else {
-        const uint2 w = ld_stream(static_cast<const uint2*>(pk.idx) + i);
-        w0 = w.x;
-        w1 = w.y;
-      }
-      const int4 b0 = __ldg(reinterpret_cast<const int4*>(pk.base) + 2 * s);
-      const int4 b1 = __ldg(reinterpret_cast<const int4*>(pk.base) + 2 * s + 1);
-      const int c[8] = {b0.x + (int)(d.x & 0xffffu), b0.y + (int)(d.x >> 16),
-                        b0.z + (int)(d.y & 0xffffu), b0.w + (int)(d.y >> 16),
-                        b1.x + (int)(d.z & 0xffffu), b1.y + (int)(d.z >> 16),
-                        b1.z + (int)(d.w & 0xffffu), b1.w + (int)(d.w >> 16)};
+      int c[8];
+      packed_cols(pk.base, s, cur.d, c);
       float xv[K];
 #pragma unroll
       for (int j = 0; j < K; ++j) xv[j] = __ldg(x + c[j]);
       sum = 0.f;
 #pragma unroll
-      for (int j = 0; j < K; ++j) {
-        const unsigned id =
-            (NIB == 4) ? (w0 >> (4 * j)) & 15u : ((j < 4 ? w0 : w1) >> (8 * (j & 3))) & 255u;
-        sum = fmaf(xv[j], tab[id], sum);
-      }
+      for (int j = 0; j < K; ++j) sum = fmaf(xv[j], tab[packed_index<NIB>(cur, j)], sum);
     }
     if (i < A.nrows) {
-      if (MODE == kResid) {
-        y[i] = (w == 1.0f) ? b[i] - sum : fmaf(-w, sum, b[i]);
+      if (MODE == kResid) {  // in aggregate order when yperm is given
+        y[yperm ? yperm[i] : i] = (w == 1.0f) ? b[i] - sum : fmaf(-w, sum, b[i]);
       } else {
         const float ri = b[i];
         const float zi = fmaf(dinv ? dinv[i] : w, ri - sum, x[i]);
@@ -655,6 +712,7 @@ __global__ void __launch_bounds__(256, 8) k_amgp_spmv(SellView<float> A, PackedV
         acc[0] += (double)ri * (double)zi;
       }
     }
+    cur = nxt;
   }
   if (MODE == kSmooth) grid_reduce<SumOp, 1>(acc, rs, CycleFinish{S, first});
 }
@@ -662,15 +720,15 @@ __global__ void __launch_bounds__(256, 8) k_amgp_spmv(SellView<float> A, PackedV
 template <int MODE>
 void launch_amgp(const PackedView& pk, SellView<float> A, int nb, const float* x, const float* b,
                  const float* dinv, float* y, PcgScalars* S, ReduceScratch rs, int first,
-                 cudaStream_t s, float w) {
+                 cudaStream_t s, float w, const int* yperm) {
   if (pk.nib == 4 && pk.slots == 7)
-    k_amgp_spmv<4, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w);
+    k_amgp_spmv<4, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w, yperm);
   else if (pk.nib == 4)
-    k_amgp_spmv<4, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w);
+    k_amgp_spmv<4, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w, yperm);
   else if (pk.slots == 7)
-    k_amgp_spmv<8, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w);
+    k_amgp_spmv<8, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w, yperm);
   else
-    k_amgp_spmv<8, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w);
+    k_amgp_spmv<8, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w, yperm);
 }
 
 // Coarsest level: x = C b, one warp per row of the dense inverse.
@@ -703,9 +761,9 @@ int vec_blocks(int n) {
 template <int MODE, typename T>
 void launch_packed0(const PackedView& pk, SellView<T> A, int nb, const T* x, const T* b,
                     const T* dinv, T* y, PcgScalars* S, ReduceScratch rs, int first,
-                    cudaStream_t s, T w = T(1)) {
+                    cudaStream_t s, T w = T(1), const int* yperm = nullptr) {
   if constexpr (std::is_same<T, float>::value)
-    launch_amgp<MODE>(pk, A, nb, x, b, dinv, y, S, rs, first, s, w);
+    launch_amgp<MODE>(pk, A, nb, x, b, dinv, y, S, rs, first, s, w, yperm);
 }
 
 namespace {
@@ -719,6 +777,7 @@ struct HostLevel {
   double w = 0.0;                          // Jacobi weight 4 / (3 rho)
   const HCsr* P = nullptr;                 // prolongation / restriction (not on the coarsest)
   const HCsr* R = nullptr;
+  const std::vector<int>* agg = nullptr;   // aggregate of every row (not on the coarsest)
   const std::vector<double>* cinv = nullptr;  // coarsest only: dense (pseudo-)inverse
 };
 
@@ -778,6 +837,7 @@ int host_hierarchy(int n, const int* rp, const int* ci, const double* v, const d
     if (drop > 0.0) sparsify(Ac, nrm, drop);
     H.P = &P;
     H.R = &R;
+    H.agg = &agg;
     GIPB_TRY(emit(H));
     A = std::move(Ac);
     z = std::move(nrm);
@@ -821,7 +881,8 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
     GIPB_TRY(L.t.alloc((size_t)A.nr));
     if (H.l > 0) {  // level 0 runs on the solver's own operator
       GIPB_TRY(L.b.alloc((size_t)A.nr));
-      GIPB_TRY(upload(A, &L.A, s));
+      // the FP32 cycle stores its long-row coarse operators compactly where they fit
+      GIPB_TRY(upload(A, &L.A, s, false, !getenv("GIPB200_AMG_WIDE")));
     }
     nnz_all += (double)A.nnz();
     if (H.cinv) {
@@ -833,7 +894,32 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
       // both round the same values), halving their value stream
       const bool half = std::is_same<T, float>::value;
       GIPB_TRY(upload(*H.P, &L.P, s, half));
-      GIPB_TRY(upload(*H.R, &L.R, s, half));
+      if (H.l == 0 && !getenv("GIPB200_AMG_NO_AGG_ORDER")) {
+        // Level 0's residual is written in aggregate order (the rows of aggregate 0, then
+        // of aggregate 1, ..., each in row order), and the restriction reads it there: a
+        // coarse row's columns (its aggregate and the neighbours' cells) then lie close
+        // together instead of across three breadth-first levels of the fine numbering.
+        const std::vector<int>& agg = *H.agg;
+        std::vector<int> start((size_t)H.R->nr + 1, 0);
+        for (int a : agg) start[(size_t)a + 1]++;
+        for (int j = 0; j < H.R->nr; ++j) start[j + 1] += start[j];
+        std::vector<int> perm((size_t)A.nr);
+        for (int i = 0; i < A.nr; ++i) perm[i] = start[agg[i]]++;
+        HCsr Rp = *H.R;  // columns renumbered, each row's entries sorted by the new column
+        for (int j = 0; j < Rp.nr; ++j) {
+          std::vector<std::pair<int, double>> e;
+          for (int k = Rp.rp[j]; k < Rp.rp[j + 1]; ++k) e.push_back({perm[Rp.ci[k]], Rp.v[k]});
+          std::sort(e.begin(), e.end());
+          for (int k = Rp.rp[j]; k < Rp.rp[j + 1]; ++k) {
+            Rp.ci[k] = e[k - Rp.rp[j]].first;
+            Rp.v[k] = e[k - Rp.rp[j]].second;
+          }
+        }
+        GIPB_TRY(upload(Rp, &L.R, s, half));
+        GIPB_TRY(perm0.upload(perm.data(), perm.size(), s));
+      } else {
+        GIPB_TRY(upload(*H.R, &L.R, s, half));
+      }
     }
     lv.push_back(std::move(Lp));
     return GIPB200_OK;
@@ -845,10 +931,7 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
 }
 
 int CycleTrace::mark(cudaStream_t s, int lvl, int knd, double by) {
-  cudaEvent_t e;
-  GIPB_CUDA(cudaEventCreate(&e));
-  ev.push_back(e);
-  GIPB_CUDA(cudaEventRecord(e, s));
+  GIPB_TRY(close(s));
   level.push_back(lvl);
   kind.push_back(knd);
   bytes.push_back(by);
@@ -859,7 +942,7 @@ int CycleTrace::close(cudaStream_t s) {
   cudaEvent_t e;
   GIPB_CUDA(cudaEventCreate(&e));
   ev.push_back(e);
-  GIPB_CUDA(cudaEventRecord(e, s));
+  GIPB_CUDA(cudaEventRecordWithFlags(e, s, captured ? cudaEventRecordExternal : 0));
   return GIPB200_OK;
 }
 
@@ -890,15 +973,16 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
       GIPB_TRY(mark(l, GIPB200_CYCLE_JACOBI0, 3.0 * n * w));
       k_amg_jacobi0<T><<<vec_blocks(V.n), 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
     }
-    GIPB_TRY(mark(l, GIPB200_CYCLE_RESIDUAL, a_bytes(l) + (skip ? 2.0 : 3.0) * n * w));
+    GIPB_TRY(mark(l, GIPB200_CYCLE_RESIDUAL, a_bytes(l) + (skip ? 2.0 : 3.0) * n * w +
+                                                 (l == 0 && perm0.p ? 4.0 * n : 0.0)));
     if (l == 0) {
       const int bs = vec_blocks(A0.nslices * 32);
       if (packed)
         launch_packed0<kResid>(*pk, A0, bs, skip ? r : V.x.p, b, (const T*)nullptr, V.t.p, S, rs,
-                               first, s, skip ? (T)omega0 : T(1));
+                               first, s, skip ? (T)omega0 : T(1), perm0.p);
       else
         k_amg_spmv<T, kResid><<<bs, 256, 0, s>>>(A0, skip ? r : V.x.p, b, nullptr, V.t.p, S,
-                                                  skip ? (T)omega0 : T(1));
+                                                  skip ? (T)omega0 : T(1), perm0.p);
     } else {
       amg_mv<T, kResid>(V.A, V.x.p, b, (const T*)nullptr, V.t.p, S, s);
     }
@@ -950,6 +1034,7 @@ double AmgT<T>::cycle_bytes(double a0_stream_bytes) const {
     const bool skip = l == 0 && unit0;                   // x0 = omega0 r not formed
     if (!skip) b += 3.0 * n * w;                         // x = dinv b
     b += a + (skip ? 2.0 : 3.0) * n * w;                 // t = b - A x
+    if (l == 0 && perm0.p) b += 4.0 * n;                 // its aggregate-order positions
     b += stream_bytes(V.R) + (n + nn) * w;               // b_next = R t
     b += stream_bytes(V.P) + (nn + 2.0 * n) * w;         // x += P x_next
     b += a + (skip ? 3.0 : 4.0) * n * w;                 // smoothed x

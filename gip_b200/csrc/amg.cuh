@@ -27,6 +27,9 @@ struct SellT {
   DevBuf<int> rp;
   bool half = false;           // values stored in FP16 (hval) instead of T (val)
   DevBuf<__half> hval;
+  // CSR form with 16-bit columns: column = row + dcol[k] (every offset fits in int16)
+  bool short_cols = false;
+  DevBuf<short> dcol;
   SellView<T> view() const { return {nrows, nslices, sptr.p, col.p, val.p}; }
   SellView<__half> hview() const { return {nrows, nslices, sptr.p, col.p, hval.p}; }
 };
@@ -50,6 +53,7 @@ struct CycleTrace {
   std::vector<cudaEvent_t> ev;
   std::vector<int> level, kind;
   std::vector<double> bytes;
+  bool captured = false;  // record into a graph being captured (external event nodes)
   int mark(cudaStream_t s, int lvl, int knd, double by);  // before a kernel
   int close(cudaStream_t s);                              // after the last one
   ~CycleTrace();
@@ -77,6 +81,9 @@ struct AmgT {
   // like the per-row one, so the cycle stays a symmetric positive definite operator.
   bool unit0 = false;
   double omega0 = 0.0;
+  // Level 0's residual position in aggregate order (empty: written in row order); the
+  // level-0 restriction's columns are numbered in that order.
+  DevBuf<int> perm0;
 
   // Hierarchy of the n x n operator (host CSR, FP64 values; columns < n), near-null
   // vector z.  singular: the operator annihilates z (pinned-Neumann inner system), so the
@@ -101,7 +108,7 @@ struct AmgT {
 template <typename T>
 double stream_bytes(const SellT<T>& M) {
   const double w = M.half ? 2.0 : (double)sizeof(T);
-  if (M.lanes > 0) return (double)M.nnz * (4.0 + w) + (M.nrows + 1.0) * 4.0;
+  if (M.lanes > 0) return (double)M.nnz * ((M.short_cols ? 2.0 : 4.0) + w) + (M.nrows + 1.0) * 4.0;
   return (double)M.nslots * (4.0 + w) + (M.nslices + 1.0) * 8.0;
 }
 

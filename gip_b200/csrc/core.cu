@@ -138,6 +138,26 @@ int sell_build(Sell* S, int nrows, int ncols, int nnz, const int* rp, const int*
   return GIPB200_OK;
 }
 
+int csr_build(Sell* S, int nrows, int ncols, int nnz, const int* rp, const int* col,
+              const double* val, cudaStream_t stream) {
+  GIPB_TRY(validate_csr(nrows, ncols, nnz, rp, col, ncols, "matrix"));
+  S->nrows = nrows;
+  S->ncols = ncols;
+  S->nnz = nnz;
+  S->nslices = 0;
+  S->nslots = 0;
+  GIPB_TRY(S->rowptr.upload(rp, (size_t)nrows + 1, stream));
+  GIPB_TRY(S->csr_col.upload(col, (size_t)std::max(nnz, 1), stream));
+  if (val) {
+    GIPB_TRY(S->csr_val.upload(val, (size_t)std::max(nnz, 1), stream));
+  } else {
+    GIPB_TRY(S->csr_val.alloc((size_t)std::max(nnz, 1)));
+    GIPB_TRY(S->csr_val.zero(stream));
+  }
+  GIPB_CUDA(cudaStreamSynchronize(stream));
+  return GIPB200_OK;
+}
+
 __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)

@@ -99,6 +99,62 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[K], ReduceScratch 
   return true;
 }
 
+// ------------------------------------------------------------------ packed FP32 rows
+// The mixed form's compressed operator: per row one 16-byte word of eight 16-bit column
+// deltas from per-(slice, slot) int32 bases, and eight value-table indices (4 or 8 bits).
+// A kernel loads a slice's words one slice ahead of their use (software pipelining): the
+// words' memory latency then overlaps the previous slice's gathers instead of adding a
+// second dependent round trip to every row.
+struct PackedWords {
+  uint4 d;          // column deltas
+  unsigned w0, w1;  // value-table indices
+  int plain;        // the slice is stored in the plain sliced layout instead
+};
+
+template <int NIB>
+__device__ __forceinline__ void packed_words(const uint4* __restrict__ delta,
+                                             const void* __restrict__ idx,
+                                             const unsigned char* __restrict__ plain, int s,
+                                             int lane, PackedWords& o) {
+  const int i = s * 32 + lane;
+  o.plain = __ldg(plain + s);
+  if (o.plain) {
+    o.d = make_uint4(0u, 0u, 0u, 0u);
+    o.w0 = o.w1 = 0u;
+    return;
+  }
+  o.d = ld_stream(delta + i);
+  if (NIB == 4) {
+    o.w0 = ld_stream(static_cast<const unsigned*>(idx) + i);
+    o.w1 = 0u;
+  } else {
+    const uint2 w = ld_stream(static_cast<const uint2*>(idx) + i);
+    o.w0 = w.x;
+    o.w1 = w.y;
+  }
+}
+
+// The row's eight columns: the slice's slot bases plus the row's deltas.
+__device__ __forceinline__ void packed_cols(const int* __restrict__ base, int s, const uint4& d,
+                                            int (&c)[8]) {
+  const int4 b0 = __ldg(reinterpret_cast<const int4*>(base) + 2 * s);
+  const int4 b1 = __ldg(reinterpret_cast<const int4*>(base) + 2 * s + 1);
+  c[0] = b0.x + (int)(d.x & 0xffffu);
+  c[1] = b0.y + (int)(d.x >> 16);
+  c[2] = b0.z + (int)(d.y & 0xffffu);
+  c[3] = b0.w + (int)(d.y >> 16);
+  c[4] = b1.x + (int)(d.z & 0xffffu);
+  c[5] = b1.y + (int)(d.z >> 16);
+  c[6] = b1.z + (int)(d.w & 0xffffu);
+  c[7] = b1.w + (int)(d.w >> 16);
+}
+
+// Value-table index of slot j.
+template <int NIB>
+__device__ __forceinline__ unsigned packed_index(const PackedWords& w, int j) {
+  return (NIB == 4) ? (w.w0 >> (4 * j)) & 15u : ((j < 4 ? w.w0 : w.w1) >> (8 * (j & 3))) & 255u;
+}
+
 // One row of a SELL-32 matrix, summed slot by slot in CSR order with GIP's rounding.
 // `any` reports whether the row has at least one stored nonzero.
 template <typename V, typename X, int CH = 8>

@@ -173,6 +173,86 @@ __global__ void __launch_bounds__(256) k_dns_gradcorr(SellView<double> Gx, SellV
 }
 
 // ------------------------------------------------------------------ MassFluxes
+// The same seven ordered updates with SFx, SFy, SFz merged per face (FaceOps3): slot j of
+// a face belongs to SFx for j < cx, to SFy for j < cx + cy, else to SFz; every operator's
+// sums run over its own entries in stored order, as in k_dns_massflux.
+__global__ void __launch_bounds__(256) k_dns_massflux3(
+    SellView<double> SO, SellView<double> SF, const unsigned short* __restrict__ cnt,
+    const double* __restrict__ p, const double* __restrict__ gpx, const double* __restrict__ gpy,
+    const double* __restrict__ gpz, const double* __restrict__ u, const double* __restrict__ v,
+    const double* __restrict__ w, double* __restrict__ mf, double rho, const DnsScalars* S) {
+  const double sigma = S->sigma;
+  const double fact1 = ddiv(-1.0, sigma);
+  const double fact2 = ddiv(1.0, sigma);
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int ns = max(SO.nslices, SF.nslices);
+  for (int s = gw; s < ns; s += nw) {
+    const int f = s * 32 + lane;
+    double so = 0;
+    bool a0 = false;
+    if (s < SO.nslices) sell_row_f64(SO, p, s, lane, so, a0);
+    double gx = 0, gy = 0, gz = 0, ux = 0, uy = 0, uz = 0;
+    int cx = 0, cy = 0, cz = 0;
+    if (s < SF.nslices) {
+      const unsigned c = (f < SF.nrows) ? cnt[f] : 0u;
+      cx = c & 15u;
+      cy = (c >> 4) & 15u;
+      cz = (c >> 8) & 15u;
+      const long long base = SF.sptr[s];
+      const int len = (int)((SF.sptr[s + 1] - base) >> 5);
+      for (int j0 = 0; j0 < len; j0 += 2) {
+        int col[2];
+        double val[2];
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const long long k = base + 32LL * (j0 + t) + lane;
+          col[t] = (j0 + t < len) ? ld_stream(SF.col + k) : -1;
+          val[t] = (j0 + t < len) ? ld_stream(SF.val + k) : 0.0;
+        }
+        double a[2], b[2];
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          const int j = j0 + t;
+          const double* g = (j < cx) ? gpx : (j < cx + cy) ? gpy : gpz;
+          const double* q = (j < cx) ? u : (j < cx + cy) ? v : w;
+          a[t] = (col[t] >= 0) ? __ldg(g + col[t]) : 0.0;
+          b[t] = (col[t] >= 0) ? __ldg(q + col[t]) : 0.0;
+        }
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          if (col[t] < 0) continue;
+          const int j = j0 + t;
+          if (j < cx) {
+            gx = dadd(gx, dmul(a[t], val[t]));
+            ux = dadd(ux, dmul(b[t], val[t]));
+          } else if (j < cx + cy) {
+            gy = dadd(gy, dmul(a[t], val[t]));
+            uy = dadd(uy, dmul(b[t], val[t]));
+          } else {
+            gz = dadd(gz, dmul(a[t], val[t]));
+            uz = dadd(uz, dmul(b[t], val[t]));
+          }
+        }
+      }
+    }
+    a0 = a0 && f < SO.nrows;
+    const bool ax = cx > 0, ay = cy > 0, az = cz > 0;
+    if (a0 || ax || ay || az) {
+      double m = mf[f];
+      if (a0) m = axpby_row(fact1, so, 0.0, m);
+      if (ax) m = axpby_row(fact2, gx, 1.0, m);
+      if (ay) m = axpby_row(fact2, gy, 1.0, m);
+      if (az) m = axpby_row(fact2, gz, 1.0, m);
+      if (ax) m = axpby_row(rho, ux, 1.0, m);
+      if (ay) m = axpby_row(rho, uy, 1.0, m);
+      if (az) m = axpby_row(rho, uz, 1.0, m);
+      mf[f] = m;
+    }
+  }
+}
+
 // mf = -dt SO p + dt SF gp + rho SF u, as seven ordered SpMV updates -- GIP_DNS.h:381-390
 __global__ void __launch_bounds__(256) k_dns_massflux(
     SellView<double> SO, SellView<double> SFx, SellView<double> SFy, SellView<double> SFz,
@@ -390,8 +470,12 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync) {
   };
   mark(0);
   // PredictorVelocity: C's values from the face fluxes, then D/C products and AB2
-  GIPB_TRY(launch_csr_spmv(Ec.nrows, Ec.rowptr.p, Ec.csr_col.p, Ec.csr_val.p, mf.p, cval.p, D.pos.p,
-                           0.0, 0.0, 0, s));
+  if (ec_slot)
+    GIPB_TRY(launch_csr_spmv(ec_rows, ec_rp.p, ec_col.p, ec_val.p, mf.p, cval.p, nullptr, 0.0, 0.0,
+                             0, s));
+  else
+    GIPB_TRY(launch_csr_spmv(Ec.nrows, Ec.rowptr.p, Ec.csr_col.p, Ec.csr_val.p, mf.p, cval.p,
+                             D.pos.p, 0.0, 0.0, 0, s));
   k_dns_convdiff<<<grid.convdiff, 256, 0, s>>>(D.view(), cval.p, u.p, v.p, w.p, ax.p, ay.p, az.p);
   k_dns_ab2<<<grid.ab2, 256, 0, s>>>(N, u.p, v.p, w.p, ax.p, ay.p, az.p, ax0.p, ay0.p, az0.p, sc.p);
   mark(1);
@@ -410,9 +494,14 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync) {
                                                gpz.p, u.p, v.p, w.p, N, prm.rho, sc.p);
   mark(5);
   // MassFluxes
-  k_dns_massflux<<<grid.massflux, 256, 0, s>>>(SO.view(), SFx.view(), SFy.view(), SFz.view(), p.p,
-                                               gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p, prm.rho,
-                                               sc.p);
+  if (SF3.on)
+    k_dns_massflux3<<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p, p.p, gpx.p,
+                                                  gpy.p, gpz.p, u.p, v.p, w.p, mf.p, prm.rho,
+                                                  sc.p);
+  else
+    k_dns_massflux<<<grid.massflux, 256, 0, s>>>(SO.view(), SFx.view(), SFy.view(), SFz.view(),
+                                                 p.p, gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p,
+                                                 prm.rho, sc.p);
   mark(6);
   // CFLCondition
   k_dns_massr<<<grid.massr, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
@@ -432,15 +521,17 @@ void Dns::phase_bytes(double out[7]) const {
   auto op = [](const Sell& M) { return 12.0 * M.nnz + 8.0 * (M.nslices + 1.0); };
   const double n = N, no = NO, nf = NF;
   // predictor: C's values = Ec mf (CSR, rows scattered into C's slots), D/C products, AB2
-  const double ec = 12.0 * Ec.nnz + 4.0 * (Ec.nrows + 1.0) + 4.0 * Ec.nrows + 8.0 * nf +
-                    8.0 * Ec.nrows;
+  const double ec = ec_slot ? 12.0 * Ec.nnz + 4.0 * (ec_rows + 1.0) + 8.0 * nf + 8.0 * Ec.nrows
+                            : 12.0 * Ec.nnz + 4.0 * (Ec.nrows + 1.0) + 4.0 * Ec.nrows + 8.0 * nf +
+                                  8.0 * Ec.nrows;
   const double cd = op(D) + 8.0 * D.nnz + 24.0 * no + 24.0 * n;
   out[0] = ec + cd + 120.0 * n;
   out[1] = op(Mx) + op(My) + op(Mz) + 24.0 * no + 8.0 * n;          // rhs
   out[2] = 0.0;                                                      // PCG
   out[3] = 16.0 * no + op(Lb) + 24.0 * Lb.nnz;                       // p0/p copies, ghosts
   out[4] = op(Gx) + op(Gy) + op(Gz) + 8.0 * no + 24.0 * no + 48.0 * n;  // gp, u -= gp
-  out[5] = op(SO) + op(SFx) + op(SFy) + op(SFz) + 56.0 * no + 16.0 * nf;  // mf
+  out[5] = op(SO) + op(SFx) + op(SFy) + op(SFz) + 56.0 * no + 16.0 * nf +  // mf
+           (SF3.on ? 2.0 * nf : 0.0);                                        // face counts
   out[6] = op(Mres) + 8.0 * nf + 8.0 * n + 32.0 * n;                 // massr, CFL
 }
 
@@ -551,6 +642,77 @@ static int check_op(const gipb200_host_csr& m, const char* name, int rows_max, i
 
 static int build_op(Sell* S, const gipb200_host_csr& m) {
   return sell_build(S, m.nrows, m.ncols, m.nnz, m.rowptr, m.col, m.val, 0);
+}
+
+// Ec in D's slot order (Dns::ec_slot): slot t of D's sliced layout holds the nonzero k of
+// row i at position k - rowptr[i] of slice i / 32, lane i % 32.
+static int build_ec_slot(Dns& E, const gipb200_host_csr& D, const gipb200_host_csr& Ec) {
+  if (getenv("GIPB200_NO_EC_SLOT") || Ec.nrows != D.nnz) return GIPB200_OK;
+  const int ns = (D.nrows + 31) / 32;
+  std::vector<long long> sptr((size_t)ns + 1, 0);
+  for (int sl = 0; sl < ns; ++sl) {
+    int len = 0;
+    for (int r = sl * 32; r < std::min(D.nrows, sl * 32 + 32); ++r)
+      len = std::max(len, D.rowptr[r + 1] - D.rowptr[r]);
+    sptr[sl + 1] = sptr[sl] + 32LL * len;
+  }
+  const long long nslots = sptr[ns];
+  if (nslots > 0x7ffffffeLL) return GIPB200_OK;
+  std::vector<int> src((size_t)nslots, -1);  // slot -> Ec row (the CSR nonzero of D)
+  for (int r = 0; r < D.nrows; ++r)
+    for (int k = D.rowptr[r]; k < D.rowptr[r + 1]; ++k)
+      src[(size_t)(sptr[r >> 5] + 32LL * (k - D.rowptr[r]) + (r & 31))] = k;
+  std::vector<int> rp((size_t)nslots + 1, 0), col;
+  std::vector<double> val;
+  col.reserve((size_t)Ec.nnz);
+  val.reserve((size_t)Ec.nnz);
+  for (long long t = 0; t < nslots; ++t) {
+    const int k = src[(size_t)t];
+    if (k >= 0)
+      for (int e = Ec.rowptr[k]; e < Ec.rowptr[k + 1]; ++e) {
+        col.push_back(Ec.col[e]);
+        val.push_back(Ec.val[e]);
+      }
+    rp[(size_t)t + 1] = (int)col.size();
+  }
+  GIPB_TRY(E.ec_rp.upload(rp.data(), rp.size(), 0));
+  GIPB_TRY(E.ec_col.upload(col.data(), std::max<size_t>(col.size(), 1), 0));
+  GIPB_TRY(E.ec_val.upload(val.data(), std::max<size_t>(val.size(), 1), 0));
+  GIPB_CUDA(cudaStreamSynchronize(0));
+  E.ec_rows = (int)nslots;
+  E.ec_slot = true;
+  return GIPB200_OK;
+}
+
+// FaceOps3 from the three face operators (host CSR, NF rows or none).  Left off when a
+// face row of one operator has more than 15 entries.
+static int build_face3(FaceOps3* F, const gipb200_host_csr* const op[3], int NF, int NO) {
+  F->on = false;
+  if (NF <= 0 || getenv("GIPB200_NO_FACE3")) return GIPB200_OK;
+  std::vector<int> rp((size_t)NF + 1, 0), col;
+  std::vector<double> val;
+  std::vector<unsigned short> cnt((size_t)NF, 0);
+  for (int f = 0; f < NF; ++f) {
+    unsigned packed = 0;
+    for (int o = 0; o < 3; ++o) {
+      const gipb200_host_csr& m = *op[o];
+      if (f >= m.nrows) continue;
+      const int c = m.rowptr[f + 1] - m.rowptr[f];
+      if (c > 15) return GIPB200_OK;
+      packed |= (unsigned)c << (4 * o);
+      for (int k = m.rowptr[f]; k < m.rowptr[f + 1]; ++k) {
+        col.push_back(m.col[k]);
+        val.push_back(m.val[k]);
+      }
+    }
+    cnt[f] = (unsigned short)packed;
+    rp[f + 1] = (int)col.size();
+  }
+  GIPB_TRY(sell_build(&F->S, NF, NO, (int)col.size(), rp.data(), col.data(), val.data(), 0));
+  GIPB_TRY(F->cnt.upload(cnt.data(), cnt.size(), 0));
+  GIPB_CUDA(cudaStreamSynchronize(0));
+  F->on = true;
+  return GIPB200_OK;
 }
 
 int check_dns_ops(const gipb200_dns_ops* ops) {
@@ -684,7 +846,10 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     }
     const gipb200_dns_ops* bops = &rops;
     GIPB_TRY(build_op(&E.D, bops->D));
-    GIPB_TRY(build_op(&E.Ec, bops->Ec));
+    // Ec is only ever read row by row in CSR form (C's values, the adjoint's convective
+    // term): no sliced copy
+    GIPB_TRY(csr_build(&E.Ec, bops->Ec.nrows, bops->Ec.ncols, bops->Ec.nnz, bops->Ec.rowptr,
+                       bops->Ec.col, bops->Ec.val, 0));
     GIPB_TRY(build_op(&E.L, bops->L));
     GIPB_TRY(build_op(&E.Lb, bops->Lb));
     GIPB_TRY(build_op(&E.Mx, bops->Mx));
@@ -698,6 +863,19 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     GIPB_TRY(build_op(&E.SFy, bops->SFy));
     GIPB_TRY(build_op(&E.SFz, bops->SFz));
     GIPB_TRY(build_op(&E.SO, bops->SO));
+    GIPB_TRY(build_ec_slot(E, bops->D, bops->Ec));
+    {
+      const gipb200_host_csr* sf[3] = {&bops->SFx, &bops->SFy, &bops->SFz};
+      GIPB_TRY(build_face3(&E.SF3, sf, NF, NO));
+      if (E.SF3.on)  // the separate sliced copies are no longer read on the device
+        for (Sell* S : {&E.SFx, &E.SFy, &E.SFz}) {
+          S->col.release();
+          S->val.release();
+          S->pos.release();
+          S->csr_col.release();
+          S->csr_val.release();
+        }
+    }
     // C starts with D's values (C.postConstruct reads the D file, GIP_DNS.h:151)
     GIPB_TRY(E.cval.alloc((size_t)std::max<long long>(E.D.nslots, 1)));
     GIPB_CUDA(cudaMemcpy(E.cval.p, E.D.val.p, E.cval.n * 8, cudaMemcpyDeviceToDevice));

@@ -30,10 +30,29 @@ struct DnsHistory {
 // Device timestamps at the step's 8 phase boundaries (kPhaseMarks per step, ns).
 constexpr int kPhaseMarks = 8;
 
+// SFx, SFy and SFz merged row by row for the mass-flux kernel: a face row holds its SFx
+// entries, then its SFy entries, then its SFz entries (each in stored order), with the
+// three counts per face.  A face of a structured grid has entries in one of the three
+// only, so the merged slices have no padding where three separate ones are two-thirds
+// padding.  Each operator's row sum keeps its own order, so results are unchanged.
+struct FaceOps3 {
+  bool on = false;
+  Sell S;                            // merged rows (NF rows)
+  DevBuf<unsigned short> cnt;        // per face: cx | cy << 4 | cz << 8
+};
+
 struct Dns {
   int N = 0, NO = 0, NF = 0;
   gipb200_dns_params prm{};
   Sell D, Ec, L, Lb, Mx, My, Mz, Mres, Gx, Gy, Gz, SFx, SFy, SFz, SO;
+  FaceOps3 SF3;
+  // Ec with its rows in C's slot order (row t = the Ec row of the nonzero stored in slot t
+  // of D's sliced layout; padding slots are empty rows), so C's values are written
+  // contiguously instead of through D's position map.
+  bool ec_slot = false;
+  int ec_rows = 0;
+  DevBuf<int> ec_rp, ec_col;
+  DevBuf<double> ec_val;
   DevBuf<double> cval;
   DevBuf<double> u, v, w, dxs, ax, ay, az, ax0, ay0, az0, rhs, p, p0, gpx, gpy, gpz, temp, mf;
   Pcg pcg;

@@ -145,6 +145,9 @@ struct Sell {
 // Builds SELL-32 (and keeps a device CSR copy) from host CSR arrays.
 int sell_build(Sell* S, int nrows, int ncols, int nnz, const int* h_rowptr, const int* h_col,
                const double* h_val, cudaStream_t stream);
+// Only the device CSR copy (operators read row by row, never sliced).
+int csr_build(Sell* S, int nrows, int ncols, int nnz, const int* h_rowptr, const int* h_col,
+              const double* h_val, cudaStream_t stream);
 // Adds an FP32 value copy.
 int sell_add_fp32(Sell* S, cudaStream_t stream);
 int validate_csr(int nrows, int ncols, int nnz, const int* rowptr, const int* col,

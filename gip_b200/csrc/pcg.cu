@@ -520,38 +520,24 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   double acc[1] = {0.0};
+  PackedWords cur, nxt;
+  if (gw < A.nslices) packed_words<NIB>(delta, idx, plain, gw, lane, cur);
+  nxt = cur;
   for (int s = gw; s < A.nslices; s += nw) {
+    if (s + nw < A.nslices) packed_words<NIB>(delta, idx, plain, s + nw, lane, nxt);
     const int i = s * 32 + lane;
     float sum;
-    if (__ldg(plain + s)) {
+    if (cur.plain) {
       sum = sell_row_dir<2>(A, r, pin, beta, s, lane);  // rare fallback: few registers
     } else {
-      const uint4 d = ld_stream(delta + i);
-      unsigned w0, w1;
-      if (NIB == 4) {
-        w0 = ld_stream(static_cast<const unsigned*>(idx) + i);
-        w1 = 0u;
-      } else {
-        const uint2 w = ld_stream(static_cast<const uint2*>(idx) + i);
-        w0 = w.x;
-        w1 = w.y;
-      }
-      const int4 b0 = __ldg(reinterpret_cast<const int4*>(base) + 2 * s);
-      const int4 b1 = __ldg(reinterpret_cast<const int4*>(base) + 2 * s + 1);
-      const int c[8] = {b0.x + (int)(d.x & 0xffffu), b0.y + (int)(d.x >> 16),
-                        b0.z + (int)(d.y & 0xffffu), b0.w + (int)(d.y >> 16),
-                        b1.x + (int)(d.z & 0xffffu), b1.y + (int)(d.z >> 16),
-                        b1.z + (int)(d.w & 0xffffu), b1.w + (int)(d.w >> 16)};
+      int c[8];
+      packed_cols(base, s, cur.d, c);
       float xv[K];
 #pragma unroll
       for (int j = 0; j < K; ++j) xv[j] = fmaf(beta, __ldg(pin + c[j]), __ldg(r + c[j]));
       sum = 0.f;
 #pragma unroll
-      for (int j = 0; j < K; ++j) {
-        const unsigned id =
-            (NIB == 4) ? (w0 >> (4 * j)) & 15u : ((j < 4 ? w0 : w1) >> (8 * (j & 3))) & 255u;
-        sum = fmaf(xv[j], tab[id], sum);
-      }
+      for (int j = 0; j < K; ++j) sum = fmaf(xv[j], tab[packed_index<NIB>(cur, j)], sum);
     }
     if (i < A.nrows) {
       const float pi = fmaf(beta, pin[i], r[i]);
@@ -559,6 +545,7 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
       Ap[i] = sum;
       acc[0] += (double)pi * (double)sum;
     }
+    cur = nxt;
   }
   grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
 }
@@ -1633,34 +1620,52 @@ int Pcg::profile_vcycle(int reps, cudaStream_t s, int cap, int* n_kernels, int* 
   const double plain32 = (double)L->nslots * 8.0 + (L->nslices + 1.0) * 8.0;
   const double a0 = amg ? (cop.enabled ? cop.bytes_per_launch - 16.0 * n : plain32)
                         : (double)L->nslots * 12.0 + (L->nslices + 1.0) * 8.0;
-  std::vector<double> sum;
-  int nk = 0;
-  for (int k = 0; k <= reps; ++k) {  // cycle 0 is untimed
-    CycleTrace tr;
-    if (amg)
-      GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, tsc.p, rs, 1, s, &pk0, &tr, a0));
-    else
-      GIPB_TRY(amg64->enqueue(L->view(), r.p, z64.p, tsc.p, rs, 1, s, nullptr, &tr, a0));
-    GIPB_CUDA(cudaEventSynchronize(tr.ev.back()));
-    nk = (int)tr.kind.size();
-    if (k == 0) {
-      sum.assign(nk, 0.0);
-      for (int j = 0; j < std::min(nk, cap); ++j) {
-        if (level) level[j] = tr.level[j];
-        if (kind) kind[j] = tr.kind[j];
-        if (bytes) bytes[j] = tr.bytes[j];
-      }
-      continue;
+  // The cycle is captured into a graph with an event node before every kernel, so each
+  // kernel is timed as a graph launch runs it (no host enqueue gaps between kernels).
+  CycleTrace tr;
+  tr.captured = true;
+  cudaStream_t cs = body_stream[0];
+  GIPB_CUDA(cudaStreamSynchronize(s));
+  GIPB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+  int st = amg ? amg->enqueue(a32(), r32.p, z32.p, tsc.p, rs, 1, cs, &pk0, &tr, a0)
+               : amg64->enqueue(L->view(), r.p, z64.p, tsc.p, rs, 1, cs, nullptr, &tr, a0);
+  cudaGraph_t g = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(cs, &g);
+  if (st != GIPB200_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (ce != cudaSuccess) return fail(GIPB200_ERR_CUDA, "capture failed: %s", cudaGetErrorString(ce));
+  cudaGraphExec_t ex = nullptr;
+  ce = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess)
+    return fail(GIPB200_ERR_CUDA, "instantiate failed: %s", cudaGetErrorString(ce));
+  const int nk = (int)tr.kind.size();
+  std::vector<double> sum((size_t)nk, 0.0);
+  for (int k = 0; k <= reps && st == GIPB200_OK; ++k) {  // launch 0 is untimed
+    if (cudaGraphLaunch(ex, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+      st = fail(GIPB200_ERR_CUDA, "profiled V-cycle failed");
+      break;
     }
-    for (int j = 0; j < nk; ++j) {
+    for (int j = 0; j < nk && k > 0; ++j) {
       float t = 0.f;
-      GIPB_CUDA(cudaEventElapsedTime(&t, tr.ev[j], tr.ev[j + 1]));
+      if (cudaEventElapsedTime(&t, tr.ev[j], tr.ev[j + 1]) != cudaSuccess) {
+        st = fail(GIPB200_ERR_CUDA, "cudaEventElapsedTime failed");
+        break;
+      }
       sum[j] += t;
     }
   }
+  cudaGraphExecDestroy(ex);
+  GIPB_TRY(st);
   *n_kernels = nk;
-  if (ms)
-    for (int j = 0; j < std::min(nk, cap); ++j) ms[j] = sum[j] / reps;
+  for (int j = 0; j < std::min(nk, cap); ++j) {
+    if (level) level[j] = tr.level[j];
+    if (kind) kind[j] = tr.kind[j];
+    if (bytes) bytes[j] = tr.bytes[j];
+    if (ms) ms[j] = sum[j] / reps;
+  }
   return GIPB200_OK;
 }
 

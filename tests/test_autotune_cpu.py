@@ -5,40 +5,47 @@ from gip_b200 import autotune
 
 
 class FakeEngine:
-    """Times each grid size from a table, records the launches it was given."""
+    """Times each kernel's grid size from a table, records the launches it was given."""
 
-    def __init__(self, ms_by_blocks):
+    def __init__(self, ms_by_blocks, ms_update=None):
         self.ms = ms_by_blocks
-        self.blocks = None
+        self.ms_update = ms_update or {}
+        self.blocks = self.vec = None
         self.timed = []
 
-    def set_launch(self, blocks, threads):
-        self.blocks = blocks
+    def set_launch(self, blocks, vec):
+        self.blocks, self.vec = blocks, vec
 
     def kernel_time(self, kernel, reps=15):
-        self.timed.append(self.blocks)
+        if kernel == "mixed_update":
+            self.timed.append(("update", self.vec))
+            return self.ms_update[self.vec], 0.0
+        self.timed.append(("spmv", self.blocks))
         return self.ms[self.blocks], 0.0
 
 
-def test_picks_fastest_grid_and_caches(tmp_path, monkeypatch):
+def test_picks_fastest_grids_and_caches(tmp_path, monkeypatch):
     monkeypatch.setattr(autotune, "_sm_count", lambda: 148)
     monkeypatch.setattr(autotune, "_CACHE", {})
     ms = {148: 1.0, 296: 0.7, 592: 0.5, 888: 0.6, 1184: 0.9}
-    E = FakeEngine(ms)
+    mu = {148: 0.4, 296: 0.3, 592: 0.35, 888: 0.2, 1184: 0.25}
+    E = FakeEngine(ms, mu)
     path = str(tmp_path / "tune.json")
     r = autotune.tune(E, "mixed", rows=1000, nnz=7000, path=path)
-    assert r["blocks"] == 592 and not r["cached"] and E.blocks == 592
-    assert sorted(E.timed) == sorted(ms)
-    assert json.load(open(path)) == {"mixed:1000:7000": 592}
-    # the same operator class again: no timing, the cached grid applied
-    F = FakeEngine(ms)
+    assert (r["blocks"], r["vec_blocks"]) == (592, 888) and not r["cached"]
+    assert (E.blocks, E.vec) == (592, 888)
+    assert sorted(b for k, b in E.timed if k == "spmv") == sorted(ms)
+    assert sorted(b for k, b in E.timed if k == "update") == sorted(mu)
+    assert json.load(open(path)) == {"mixed:1000:7000": {"blocks": 592, "vec_blocks": 888}}
+    # the same operator class again: no timing, the cached grids applied
+    F = FakeEngine(ms, mu)
     r = autotune.tune(F, "mixed", rows=1000, nnz=7000, path=path)
-    assert r == {"blocks": 592, "cached": True} and F.timed == [] and F.blocks == 592
+    assert r["cached"] and F.timed == [] and (F.blocks, F.vec) == (592, 888)
     # a fresh process reads the file
     monkeypatch.setattr(autotune, "_CACHE", {})
-    G = FakeEngine(ms)
+    G = FakeEngine(ms, mu)
     assert autotune.tune(G, "mixed", rows=1000, nnz=7000, path=path)["cached"]
-    assert G.timed == [] and G.blocks == 592
+    assert G.timed == [] and (G.blocks, G.vec) == (592, 888)
 
 
 def test_grid_capped_and_classes_separate(monkeypatch):
@@ -46,6 +53,7 @@ def test_grid_capped_and_classes_separate(monkeypatch):
     monkeypatch.setattr(autotune, "_CACHE", {})
     E = FakeEngine({2000: 0.3, 4000: 0.2, 8192: 0.25})
     r = autotune.tune(E, "fp64", rows=5, nnz=9, multiples=(1, 2, 8, 16))
-    assert max(E.timed) == 8192 and r["blocks"] == 4000
+    assert max(b for _, b in E.timed) == 8192 and r["blocks"] == 4000
+    assert "vec_blocks" not in r                 # the FP64 forms tune the SpMV grid only
     E2 = FakeEngine({2000: 0.1, 4000: 0.2, 8192: 0.25})
     assert autotune.tune(E2, "fp64", rows=6, nnz=9, multiples=(1, 2, 8))["blocks"] == 2000

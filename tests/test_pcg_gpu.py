@@ -231,3 +231,26 @@ def test_fp64_amg_preconditioner_and_fixed_mode_refusal(gpu, oracle_mod):
     xs = x.cpu().numpy()
     assert np.linalg.norm(b - L.to_scipy() @ xs) <= 1.5e-10 * np.linalg.norm(b)
     assert np.abs(xs - xr).max() / np.abs(xr).max() < 1e-6
+
+
+def test_amg_compact_coarse_operators(gpu, monkeypatch):
+    # the FP32 cycle's long-row coarse operators stored with 16-bit column offsets and FP16
+    # values (a slightly different, still symmetric preconditioner): the solve meets the
+    # same tolerance on the FP64 true residual in about the same number of iterations as
+    # with FP32 values and 32-bit columns
+    from gip_b200 import device as dv
+    L, b = cavity.poisson_problem(48, seed=9)
+    A = dv.DeviceMatrix(L)
+    its = {}
+    for wide in ("0", "1"):
+        if wide == "1":
+            monkeypatch.setenv("GIPB200_AMG_WIDE", "1")
+        S = dv.PcgSolver(A, mode="mixed", maxit=2000, tol=1e-8, inner_tol=1e-2, max_outer=100,
+                         precond="amg")
+        x = _t(np.zeros(L.nrows))
+        res = S.solve(_t(b), x, _t(np.zeros(L.nrows)))
+        assert res["status"] == 0, (wide, res)
+        xs = x.cpu().numpy()
+        assert np.linalg.norm(b - L.to_scipy() @ xs) <= 1.0001e-8 * np.linalg.norm(b), wide
+        its[wide] = res["iterations"]
+    assert abs(its["0"] - its["1"]) <= max(2, its["1"] // 10), its
