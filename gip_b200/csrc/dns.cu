@@ -9,6 +9,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstddef>
 #include <string>
@@ -742,6 +743,10 @@ int check_dns_ops(const gipb200_dns_ops* ops) {
 
 int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double* h_v,
              const double* h_w, const double* h_dxs, const gipb200_dns_params* prm) {
+  const auto t_begin = std::chrono::steady_clock::now();
+  auto since = [](std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+  };
   GIPB_TRY(check_dns_ops(ops));
   if (prm->pcg.mode < 0 || prm->pcg.mode > 2) return fail(GIPB200_ERR_ARG, "bad PCG mode");
   const int N = ops->n_inner, NO = ops->n_owned, NF = ops->n_faces;
@@ -844,6 +849,8 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
       GIPB_TRY(E.staging.alloc(std::max(NO, NF)));
       E.reordered = true;
     }
+    E.setup_s[0] = since(t_begin);  // checks and renumbering
+    const auto t_ops = std::chrono::steady_clock::now();
     const gipb200_dns_ops* bops = &rops;
     GIPB_TRY(build_op(&E.D, bops->D));
     // Ec is only ever read row by row in CSR form (C's values, the adjoint's convective
@@ -891,7 +898,10 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     GIPB_CUDA(cudaMemcpy(E.v.p, pv, (size_t)NO * 8, cudaMemcpyHostToDevice));
     GIPB_CUDA(cudaMemcpy(E.w.p, pw, (size_t)NO * 8, cudaMemcpyHostToDevice));
     GIPB_CUDA(cudaMemcpy(E.dxs.p, pdx, (size_t)NO * 8, cudaMemcpyHostToDevice));
+    E.setup_s[1] = since(t_ops);  // device layouts of the operators, fields
+    const auto t_pcg = std::chrono::steady_clock::now();
     GIPB_TRY(E.pcg.init(&E.L, NO, prm->pcg, 0));
+    E.setup_s[2] = since(t_pcg);  // the pressure solver (FP32 operator, packing, AMG)
     GIPB_TRY(E.sc.alloc(1));
     GIPB_TRY(E.sc.zero());
     GIPB_TRY(reduce_scratch_alloc(&E.partials, &E.ticket, &E.rs));
@@ -909,6 +919,7 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     GIPB_TRY(one_wave(k_dns_cfl, E.blocks_vec, &E.grid.cfl));
     GIPB_CUDA(cudaStreamCreateWithFlags(&E.cap_stream, cudaStreamNonBlocking));
     GIPB_CUDA(cudaDeviceSynchronize());
+    E.setup_s[3] = since(t_begin);
     return GIPB200_OK;
 }
 
@@ -1229,6 +1240,12 @@ int gipb200_dns_kernel_time(gipb200_dns Dh, int kernel, int reps, void* stream, 
     return fail(GIPB200_ERR_ARG, "unknown kernel id %d", kernel);
   return Dh->E.pcg.time_spmv(kernel == GIPB200_KERNEL_MIXED_SPMV_DOT, reps, as_stream(stream),
                              avg_ms, bytes);
+}
+
+int gipb200_dns_setup_profile(gipb200_dns Dh, double* h_seconds) {
+  if (!Dh || !h_seconds) return fail(GIPB200_ERR_ARG, "null argument");
+  for (int k = 0; k < 4; ++k) h_seconds[k] = Dh->E.setup_s[k];
+  return GIPB200_OK;
 }
 
 int gipb200_dns_phase_bytes(gipb200_dns Dh, double* h_bytes) {

@@ -46,6 +46,7 @@ struct Dns {
   gipb200_dns_params prm{};
   Sell D, Ec, L, Lb, Mx, My, Mz, Mres, Gx, Gy, Gz, SFx, SFy, SFz, SO;
   FaceOps3 SF3;
+  double setup_s[4] = {0, 0, 0, 0};  // create time: renumbering, operators, solver, total
   // Ec with its rows in C's slot order (row t = the Ec row of the nonzero stored in slot t
   // of D's sliced layout; padding slots are empty rows), so C's values are written
   // contiguously instead of through D's position map.

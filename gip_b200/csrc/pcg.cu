@@ -454,12 +454,19 @@ __device__ __forceinline__ float sell_row_dir(const SellView<float>& A, const fl
 
 // Ap = Â p and p.Ap with p = r + beta p_in (the direction update of GIP_LinearSolver.h:
 // 113-115 folded into the product): rows write p_out, gathers form p from r and p_in.
+// REC (the AMG path, where beta is small): the product of the new direction comes from the
+// recurrence A p = A z + beta A p_in, so the rows gather z alone (one gather per nonzero
+// instead of two) and read their own previous product Apin; rounding errors of the
+// recurrence are damped by beta every iteration.  beta = 0 (the first iteration of a
+// solve, or a restart) takes A z alone and reads no previous product.
+template <bool REC>
 __global__ void __launch_bounds__(256, 8) k_mx_spmv_dot(SellView<float> A, const float* __restrict__ r,
                                                      const float* __restrict__ pin,
                                                      float* __restrict__ pout,
                                                      float* __restrict__ Ap, PcgScalars* S,
                                                      ReduceScratch rs, int use_cond,
-                                                     cudaGraphConditionalHandle loop_cond) {
+                                                     cudaGraphConditionalHandle loop_cond,
+                                                     const float* __restrict__ Apin) {
   mx_enter(S, use_cond, loop_cond);
   if (S->done) return;
   const float beta = (float)S->beta;
@@ -478,13 +485,14 @@ __global__ void __launch_bounds__(256, 8) k_mx_spmv_dot(SellView<float> A, const
     const int s2 = s + 2 * nw;
     n0 = -1;
     if (s2 < A.nslices) n0 = __ldg(A.sptr + s2), n1 = __ldg(A.sptr + s2 + 1);
-    const float sum = sell_row_dir<4>(A, r, pin, beta, s, lane);
+    const float sum = REC ? sell_row_f32<2>(A, r, s, lane) : sell_row_dir<4>(A, r, pin, beta, s, lane);
     const int i = s * 32 + lane;
     if (i < A.nrows) {
       const float pi = fmaf(beta, pin[i], r[i]);
+      const float api = (REC && beta != 0.f) ? fmaf(beta, Apin[i], sum) : sum;
       pout[i] = pi;
-      Ap[i] = sum;
-      acc[0] += (double)pi * (double)sum;
+      Ap[i] = api;
+      acc[0] += (double)pi * (double)api;
     }
   }
   grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
@@ -496,7 +504,7 @@ __global__ void __launch_bounds__(256, 8) k_mx_spmv_dot(SellView<float> A, const
 // the loop has no branches.  A warp owns a slice; in a packed slice each lane loads its
 // row's 16-byte delta word and its index word, then issues K independent pairs of
 // gathers (r and p_in).  K = 7 when no packed row has an eighth slot.
-template <int NIB, int K>
+template <int NIB, int K, bool REC>
 __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
                                                          const uint4* __restrict__ delta,
                                                          const void* __restrict__ idx,
@@ -508,7 +516,8 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
                                                          float* __restrict__ pout,
                                                          float* __restrict__ Ap, PcgScalars* S,
                                                          ReduceScratch rs, int use_cond,
-                                                         cudaGraphConditionalHandle loop_cond) {
+                                                         cudaGraphConditionalHandle loop_cond,
+                                                         const float* __restrict__ Apin) {
   mx_enter(S, use_cond, loop_cond);
   if (S->done) return;
   constexpr int NT = 1 << NIB;
@@ -527,57 +536,46 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
     if (s + nw < A.nslices) packed_words<NIB>(delta, idx, plain, s + nw, lane, nxt);
     const int i = s * 32 + lane;
     float sum;
-    if (cur.plain) {
-      sum = sell_row_dir<2>(A, r, pin, beta, s, lane);  // rare fallback: few registers
+    if (cur.plain) {  // rare fallback: few registers
+      sum = REC ? sell_row_f32<2>(A, r, s, lane) : sell_row_dir<2>(A, r, pin, beta, s, lane);
     } else {
       int c[8];
       packed_cols(base, s, cur.d, c);
       float xv[K];
 #pragma unroll
-      for (int j = 0; j < K; ++j) xv[j] = fmaf(beta, __ldg(pin + c[j]), __ldg(r + c[j]));
+      for (int j = 0; j < K; ++j)
+        xv[j] = REC ? __ldg(r + c[j]) : fmaf(beta, __ldg(pin + c[j]), __ldg(r + c[j]));
       sum = 0.f;
 #pragma unroll
       for (int j = 0; j < K; ++j) sum = fmaf(xv[j], tab[packed_index<NIB>(cur, j)], sum);
     }
     if (i < A.nrows) {
       const float pi = fmaf(beta, pin[i], r[i]);
+      const float api = (REC && beta != 0.f) ? fmaf(beta, Apin[i], sum) : sum;
       pout[i] = pi;
-      Ap[i] = sum;
-      acc[0] += (double)pi * (double)sum;
+      Ap[i] = api;
+      acc[0] += (double)pi * (double)api;
     }
     cur = nxt;
   }
   grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
 }
 
-// ------------------------------------------------------------------ TMA-staged packed SpMV
-// Bulk copies (cp.async.bulk, no tensor map, no multicast) and mbarriers, hand-written.
-namespace tma {
+// ------------------------------------------------------------------ bounded barrier waits
+// Shared-memory mbarrier waits with an iteration bound: a wait that would never complete
+// gives up after about one second of SM clock and reports instead of hanging the GPU.
+namespace mbar {
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
   return (unsigned)__cvta_generic_to_shared(p);
 }
-__device__ __forceinline__ void bar_init(unsigned long long* bar, unsigned count) {
+__device__ __forceinline__ void init(unsigned long long* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
                : "memory");
 }
-__device__ __forceinline__ void bar_init_fence() {
+__device__ __forceinline__ void init_fence() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-__device__ __forceinline__ void bar_expect(unsigned long long* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
-               "r"(bytes)
-               : "memory");
-}
-// global -> this CTA's shared memory; completion counted on `bar` in bytes
-__device__ __forceinline__ void copy_g2s(void* dst, const void* src, unsigned bytes,
-                                         unsigned long long* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
-      : "memory");
-}
-__device__ __forceinline__ bool bar_try(unsigned long long* bar, unsigned parity) {
+__device__ __forceinline__ bool try_wait(unsigned long long* bar, unsigned parity) {
   unsigned ok;
   asm volatile(
       "{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
@@ -588,136 +586,22 @@ __device__ __forceinline__ bool bar_try(unsigned long long* bar, unsigned parity
   return ok != 0;
 }
 // Waits for the phase with the given parity; gives up after ~1 s of SM clock.
-__device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parity) {
+__device__ __forceinline__ bool wait(unsigned long long* bar, unsigned parity) {
   const long long t0 = clock64();
-  while (!bar_try(bar, parity))
+  while (!try_wait(bar, parity))
     if (clock64() - t0 > 2000000000LL) return false;
   return true;
 }
-}  // namespace tma
+}  // namespace mbar
 
-// A wait that can never complete (no copy, no arrival): the bounded wait must give up.
+// A wait that can never complete (no arrival): the bounded wait must give up.
 __global__ void k_bounded_wait_check(int* status) {
   __shared__ __align__(8) unsigned long long bar;
   if (threadIdx.x == 0) {
-    tma::bar_init(&bar, 1);
-    tma::bar_init_fence();
-    *status = tma::bar_wait(&bar, 0) ? GIPB200_OK : GIPB200_ERR_TIMEOUT;
+    mbar::init(&bar, 1);
+    mbar::init_fence();
+    *status = mbar::wait(&bar, 0) ? GIPB200_OK : GIPB200_ERR_TIMEOUT;
   }
-}
-
-// k_mxp_spmv_dot with the packed stream staged through shared memory by bulk copies.
-// Each warp runs its own pipeline over its own slices (gw, gw + nw, ...): lane 0 keeps
-// kStages slices of delta words, index words and slot bases in flight, each stage with
-// its own mbarrier, so a warp waits only for its own data and never for other warps.
-// Plain slices (slot base -1) read the plain layout from global memory.  The same FMA
-// order as k_mxp_spmv_dot and k_mx_spmv_dot, so the same results.
-constexpr int kStages = 4;
-template <int NIB, int K>
-__global__ void __launch_bounds__(256, 8) k_mxt_spmv_dot(SellView<float> A,
-                                                         const uint4* __restrict__ delta,
-                                                         const void* __restrict__ idx,
-                                                         const int* __restrict__ base,
-                                                         const float* __restrict__ table,
-                                                         const float* __restrict__ r,
-                                                         const float* __restrict__ pin,
-                                                         float* __restrict__ pout,
-                                                         float* __restrict__ Ap, PcgScalars* S,
-                                                         ReduceScratch rs, int use_cond,
-                                                         cudaGraphConditionalHandle loop_cond) {
-  mx_enter(S, use_cond, loop_cond);
-  if (S->done) return;
-  constexpr int NT = 1 << NIB;
-  constexpr int IW = NIB / 4;  // 32-bit index words per row
-  __shared__ __align__(128) uint4 s_delta[8][kStages][32];
-  __shared__ __align__(128) unsigned s_idx[8][kStages][32 * IW];
-  __shared__ __align__(128) int s_base[8][kStages][8];
-  __shared__ __align__(8) unsigned long long s_bar[8][kStages];
-  __shared__ float tab[NT];
-  for (int t = threadIdx.x; t < NT; t += blockDim.x) tab[t] = table[t];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  uint4(*sd)[32] = s_delta[warp];
-  unsigned(*si)[32 * IW] = s_idx[warp];
-  int(*sb)[8] = s_base[warp];
-  unsigned long long* bar = s_bar[warp];
-  // slice sl into stage st (lane 0)
-  auto fill = [&](int sl, int st) {
-    tma::bar_expect(&bar[st], 512u + 128u * IW + 32u);
-    tma::copy_g2s(&sd[st][0], delta + (size_t)sl * 32, 512u, &bar[st]);
-    tma::copy_g2s(&si[st][0], static_cast<const unsigned*>(idx) + (size_t)sl * 32 * IW,
-                  128u * IW, &bar[st]);
-    tma::copy_g2s(&sb[st][0], base + (size_t)sl * 8, 32u, &bar[st]);
-  };
-  if (lane == 0) {
-    for (int st = 0; st < kStages; ++st) tma::bar_init(&bar[st], 1);
-    tma::bar_init_fence();
-  }
-  __syncthreads();  // table and barriers ready
-  if (lane == 0)
-    for (int st = 0; st < kStages; ++st) {
-      const int sl = gw + st * nw;
-      if (sl < A.nslices) fill(sl, st);
-    }
-  const float beta = (float)S->beta;
-  double acc[1] = {0.0};
-  bool failed = false;
-  int it = 0;
-  for (int s = gw; s < A.nslices; s += nw, ++it) {
-    const int st = it % kStages;
-    const unsigned par = (unsigned)(it / kStages) & 1u;
-    const bool ok = tma::bar_wait(&bar[st], par);
-    if (!__all_sync(0xffffffffu, ok)) {  // a copy never landed: stop, report, drain
-      failed = true;
-      break;
-    }
-    const int i = s * 32 + lane;
-    float sum;
-    if (sb[st][0] < 0) {
-      sum = sell_row_dir<2>(A, r, pin, beta, s, lane);
-    } else {
-      const uint4 d = sd[st][lane];
-      const unsigned w0 = si[st][lane * IW];
-      const unsigned w1 = (IW == 2) ? si[st][lane * IW + 1] : 0u;
-      const int* b8 = sb[st];
-      const int c8[8] = {b8[0] + (int)(d.x & 0xffffu), b8[1] + (int)(d.x >> 16),
-                         b8[2] + (int)(d.y & 0xffffu), b8[3] + (int)(d.y >> 16),
-                         b8[4] + (int)(d.z & 0xffffu), b8[5] + (int)(d.z >> 16),
-                         b8[6] + (int)(d.w & 0xffffu), b8[7] + (int)(d.w >> 16)};
-      float xv[K];
-#pragma unroll
-      for (int j = 0; j < K; ++j) xv[j] = fmaf(beta, __ldg(pin + c8[j]), __ldg(r + c8[j]));
-      sum = 0.f;
-#pragma unroll
-      for (int j = 0; j < K; ++j) {
-        const unsigned id =
-            (NIB == 4) ? (w0 >> (4 * j)) & 15u : ((j < 4 ? w0 : w1) >> (8 * (j & 3))) & 255u;
-        sum = fmaf(xv[j], tab[id], sum);
-      }
-    }
-    __syncwarp();  // every lane is done with stage st
-    if (lane == 0) {
-      const int ns2 = s + kStages * nw;
-      if (ns2 < A.nslices) fill(ns2, st);
-    }
-    if (i < A.nrows) {
-      const float pi = fmaf(beta, pin[i], r[i]);
-      pout[i] = pi;
-      Ap[i] = sum;
-      acc[0] += (double)pi * (double)sum;
-    }
-  }
-  if (failed && lane == 0) {
-    S->status = GIPB200_ERR_TIMEOUT;
-    S->done = 1;
-    // wait (bounded) for the copies still in flight into this warp's stages
-    for (int k = 0; k < kStages; ++k) {
-      const int j = it + k;
-      if (gw + j * nw < A.nslices) tma::bar_wait(&bar[j % kStages], (unsigned)(j / kStages) & 1u);
-    }
-  }
-  grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
 }
 
 struct BetaFinish32 {
@@ -907,6 +791,13 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
     GIPB_TRY(p32b.alloc(n_all));
     GIPB_TRY(p32b.zero(s));
     GIPB_TRY(Ap32.alloc(n));
+    GIPB_TRY(Ap32.zero(s));
+    // the product recurrence on the AMG path (beta small): its second product buffer
+    rec = prm.precond == GIPB200_PRECOND_AMG && !getenv("GIPB200_NO_AP_RECURRENCE");
+    if (rec) {
+      GIPB_TRY(Ap32b.alloc(n));
+      GIPB_TRY(Ap32b.zero(s));
+    }
     GIPB_TRY(r32.alloc(n));
     GIPB_TRY(y32.alloc(n));
     if (n > 0) {
@@ -1162,27 +1053,6 @@ int Pcg::build_compressed(cudaStream_t s) {
   GIPB_CUDA(cudaStreamSynchronize(s));
   cop.index_bits = nib;
   cop.slots = max_len <= 7 ? 7 : 8;
-  {
-    const char* e = getenv("GIPB200_TMA");  // "1": stage the stream, "0": read it directly
-    if (e) cop.tma = e[0] == '1';
-  }
-  if (cop.tma) {
-    // enough shared memory per SM for 8 resident blocks (the rest stays L1), and the
-    // grid cap that keeps the kernel in one wave
-    const void* kfn = nib == 4 ? (cop.slots == 7 ? (const void*)k_mxt_spmv_dot<4, 7>
-                                                 : (const void*)k_mxt_spmv_dot<4, 8>)
-                               : (cop.slots == 7 ? (const void*)k_mxt_spmv_dot<8, 7>
-                                                 : (const void*)k_mxt_spmv_dot<8, 8>);
-    cudaFuncAttributes fa;
-    GIPB_CUDA(cudaFuncGetAttributes(&fa, kfn));
-    int dev = 0, smem_sm = 0;
-    GIPB_CUDA(cudaGetDevice(&dev));
-    GIPB_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
-    const int pct = (int)std::min<long long>(
-        100, (800LL * ((long long)fa.sharedSizeBytes + 1024) + smem_sm - 1) / smem_sm);
-    GIPB_CUDA(cudaFuncSetAttribute(kfn, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
-    GIPB_TRY(one_wave(kfn, kMaxReduceBlocks, &cop.max_blocks));
-  }
   cop.ntable = (int)keys.size() + 1;
   // streamed bytes: packed rows (delta + index words), their slot bases; plain slices
   // (column + value per slot, slice offsets); the plain flags; per row r and the old
@@ -1200,7 +1070,8 @@ double Pcg::iteration_bytes() const {
   if (prm.mode == GIPB200_PCG_MIXED) {
     // plain FP32 operator stream: column + value per slot, slice offsets
     const double plain = (double)L->nslots * 8.0 + (L->nslices + 1.0) * 8.0;
-    const double spmv = cop.enabled ? cop.bytes_per_launch : plain + 16.0 * nn;
+    const double spmv = (cop.enabled ? cop.bytes_per_launch : plain + 16.0 * nn) +
+                        (rec ? 4.0 * nn : 0.0);  // the previous A p read by the recurrence
     double b = spmv + 24.0 * nn;  // SpMV-dot (direction formed inside), y/r update
     if (amg) b += amg->cycle_bytes(cop.enabled ? cop.bytes_per_launch - 16.0 * nn : plain);
     return b;
@@ -1240,8 +1111,8 @@ int Pcg::read_flag(cudaStream_t s, int which, int* v) {
   return GIPB200_OK;
 }
 
-static void launch_mx_spmv(const Pcg& P, const float* pin, float* pout, float* Ap,
-                           PcgScalars* sc, int use_cond, cudaGraphConditionalHandle h,
+static void launch_mx_spmv(const Pcg& P, const float* pin, float* pout, const float* Apin,
+                           float* Ap, PcgScalars* sc, int use_cond, cudaGraphConditionalHandle h,
                            cudaStream_t s);
 
 // ------------------------------------------------------------------ conditional while-nodes
@@ -1389,10 +1260,13 @@ int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaS
     for (int half = 0; half < 2; ++half) {
       float* pin = half ? p32b.p : p32.p;
       float* pout = half ? p32.p : p32b.p;
+      // with the product recurrence the products alternate like the directions
+      float* apin = (rec && half) ? Ap32b.p : Ap32.p;
+      float* apout = rec ? (half ? Ap32.p : Ap32b.p) : Ap32.p;
       cudaGraphConditionalHandle hu;
       GIPB_TRY(make_handle(os, 0, 0, &hu));
-      launch_mx_spmv(*this, pin, pout, Ap32.p, sc.p, 1, hl, os);
-      k_mx_update<<<blocks_vec, 256, 0, os>>>(n, y32.p, r32.p, pout, Ap32.p, sc.p, rs,
+      launch_mx_spmv(*this, pin, pout, apin, apout, sc.p, 1, hl, os);
+      k_mx_update<<<blocks_vec, 256, 0, os>>>(n, y32.p, r32.p, pout, apout, sc.p, rs,
                                                prm.inner_tol, prm.maxit, pin_row, scale.p, 1, hu,
                                                amg ? 1 : 0);
       GIPB_LAUNCH_CHECK();
@@ -1457,39 +1331,33 @@ int Pcg::enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t
   return GIPB200_OK;
 }
 
-static void launch_mx_spmv(const Pcg& P, const float* pin, float* pout, float* Ap,
-                           PcgScalars* sc, int use_cond, cudaGraphConditionalHandle h,
+static void launch_mx_spmv(const Pcg& P, const float* pin, float* pout, const float* Apin,
+                           float* Ap, PcgScalars* sc, int use_cond, cudaGraphConditionalHandle h,
                            cudaStream_t s) {
   const CompressedOp& c = P.cop;
   const SellView<float> A = P.a32();
-  const int nb = (c.enabled && c.tma) ? std::min(P.blocks_spmv, c.max_blocks) : P.blocks_spmv;
+  const int nb = P.blocks_spmv;
   const float* r = P.amg ? P.z32.p : P.r32.p;  // direction from the preconditioned residual
-  if (!c.enabled)
-    k_mx_spmv_dot<<<nb, 256, 0, s>>>(A, r, pin, pout, Ap, sc, P.rs, use_cond, h);
-  else if (c.tma && c.index_bits == 4 && c.slots == 7)
-    k_mxt_spmv_dot<4, 7><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.table.p, r, pin,
-                                             pout, Ap, sc, P.rs, use_cond, h);
-  else if (c.tma && c.index_bits == 4)
-    k_mxt_spmv_dot<4, 8><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.table.p, r, pin,
-                                             pout, Ap, sc, P.rs, use_cond, h);
-  else if (c.tma && c.slots == 7)
-    k_mxt_spmv_dot<8, 7><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.table.p, r, pin,
-                                             pout, Ap, sc, P.rs, use_cond, h);
-  else if (c.tma)
-    k_mxt_spmv_dot<8, 8><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.table.p, r, pin,
-                                             pout, Ap, sc, P.rs, use_cond, h);
-  else if (c.index_bits == 4 && c.slots == 7)
-    k_mxp_spmv_dot<4, 7><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.plain.p,
-                                             c.table.p, r, pin, pout, Ap, sc, P.rs, use_cond, h);
-  else if (c.index_bits == 4)
-    k_mxp_spmv_dot<4, 8><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx4.p, c.base.p, c.plain.p,
-                                             c.table.p, r, pin, pout, Ap, sc, P.rs, use_cond, h);
-  else if (c.slots == 7)
-    k_mxp_spmv_dot<8, 7><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.plain.p,
-                                             c.table.p, r, pin, pout, Ap, sc, P.rs, use_cond, h);
-  else
-    k_mxp_spmv_dot<8, 8><<<nb, 256, 0, s>>>(A, c.delta.p, c.idx8.p, c.base.p, c.plain.p,
-                                             c.table.p, r, pin, pout, Ap, sc, P.rs, use_cond, h);
+  const void* ix = c.index_bits == 4 ? (const void*)c.idx4.p : (const void*)c.idx8.p;
+#define GIPB_MXP(NIB, K, REC)                                                                 \
+  k_mxp_spmv_dot<NIB, K, REC><<<nb, 256, 0, s>>>(A, c.delta.p, ix, c.base.p, c.plain.p,      \
+                                                 c.table.p, r, pin, pout, Ap, sc, P.rs,       \
+                                                 use_cond, h, Apin)
+  if (!c.enabled) {
+    if (P.rec)
+      k_mx_spmv_dot<true><<<nb, 256, 0, s>>>(A, r, pin, pout, Ap, sc, P.rs, use_cond, h, Apin);
+    else
+      k_mx_spmv_dot<false><<<nb, 256, 0, s>>>(A, r, pin, pout, Ap, sc, P.rs, use_cond, h, Apin);
+  } else if (c.index_bits == 4 && c.slots == 7) {
+    if (P.rec) GIPB_MXP(4, 7, true); else GIPB_MXP(4, 7, false);
+  } else if (c.index_bits == 4) {
+    if (P.rec) GIPB_MXP(4, 8, true); else GIPB_MXP(4, 8, false);
+  } else if (c.slots == 7) {
+    if (P.rec) GIPB_MXP(8, 7, true); else GIPB_MXP(8, 7, false);
+  } else {
+    if (P.rec) GIPB_MXP(8, 8, true); else GIPB_MXP(8, 8, false);
+  }
+#undef GIPB_MXP
 }
 
 int Pcg::launch_mixed_residual(const double* b, const double* x, int first, cudaStream_t s,
@@ -1514,8 +1382,10 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
   for (int k = 0; k < prm.maxit; ++k) {
     float* pin = (k & 1) ? p32b.p : p32.p;
     float* pout = (k & 1) ? p32.p : p32b.p;
-    launch_mx_spmv(*this, pin, pout, Ap32.p, sc.p, 0, 0, s);
-    k_mx_update<<<blocks_vec, 256, 0, s>>>(n, y32.p, r32.p, pout, Ap32.p, sc.p, rs, prm.inner_tol,
+    float* apin = (rec && (k & 1)) ? Ap32b.p : Ap32.p;
+    float* apout = rec ? ((k & 1) ? Ap32.p : Ap32b.p) : Ap32.p;
+    launch_mx_spmv(*this, pin, pout, apin, apout, sc.p, 0, 0, s);
+    k_mx_update<<<blocks_vec, 256, 0, s>>>(n, y32.p, r32.p, pout, apout, sc.p, rs, prm.inner_tol,
                                             prm.maxit, pin_row, scale.p, 0, 0, amg ? 1 : 0);
     k_mx_apply<<<blocks_vec, 256, 0, s>>>(n, x, y32.p, scale.p, sc.p);
     GIPB_LAUNCH_CHECK();
@@ -1569,6 +1439,12 @@ int Pcg::time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* 
   DevBuf<PcgScalars> tsc;
   GIPB_TRY(tsc.alloc(1));
   GIPB_TRY(tsc.zero(s));
+  {  // a nonzero beta, so the timed kernel reads everything an iteration reads
+    PcgScalars h{};
+    h.beta = 0.5;
+    GIPB_CUDA(cudaMemcpyAsync(tsc.p, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    GIPB_CUDA(cudaStreamSynchronize(s));
+  }
   DevBuf<float> tAp32;
   DevBuf<double> tAp;
   cudaEvent_t e0, e1;
@@ -1585,7 +1461,7 @@ int Pcg::time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* 
   for (int k = 0; k <= reps; ++k) {
     if (k == 1) GIPB_CUDA(cudaEventRecord(e0, s));
     if (mixed)
-      launch_mx_spmv(*this, p32.p, p32b.p, tAp32.p, tsc.p, 0, 0, s);
+      launch_mx_spmv(*this, p32.p, p32b.p, Ap32.p, tAp32.p, tsc.p, 0, 0, s);
     else
       k_pcg_spmv_dot<<<blocks_spmv, 256, 0, s>>>(L->view(), p.p, tAp.p, tsc.p, rs,
                                                   GIPB200_PCG_FIXED);
@@ -1604,6 +1480,7 @@ int Pcg::time_spmv(int mixed, int reps, cudaStream_t s, double* avg_ms, double* 
   *bytes = (double)L->nnz * (vbytes + 4.0) + (double)(L->nslices + 1) * 8.0 +
            (double)L->nrows * (mixed ? 4.0 : 2.0) * vbytes;
   if (mixed && cop.enabled) *bytes = cop.bytes_per_launch;
+  if (mixed && rec) *bytes += 4.0 * L->nrows;  // the previous A p, read by the recurrence
   return GIPB200_OK;
 }
 

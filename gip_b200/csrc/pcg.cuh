@@ -45,8 +45,6 @@ struct CompressedOp {
   bool enabled = false;
   int index_bits = 0;            // 4 or 8
   int slots = 8;                 // 7: no packed row uses the eighth slot
-  bool tma = false;              // stage the packed stream through shared memory
-  int max_blocks = 0;            // resident blocks of the staged kernel (one wave)
   DevBuf<uint4> delta;           // per row (nslices * 32)
   DevBuf<unsigned> idx4;         // per row, 8 x 4 bits
   DevBuf<uint2> idx8;            // per row, 8 x 8 bits
@@ -70,6 +68,10 @@ struct Pcg {
   DevBuf<double> scale;      // S = 1/sqrt(L_ii)
   DevBuf<float> p32, Ap32, r32, y32;
   DevBuf<float> p32b;        // second direction buffer: each SpMV reads one, writes the other
+  // AMG path: A p by the recurrence A z + beta A p_in (one gather per nonzero); the two
+  // product buffers alternate like the direction buffers
+  bool rec = false;
+  DevBuf<float> Ap32b;
   CompressedOp cop;
   // AMG preconditioner of the FP32 inner CG (MIXED with GIPB200_PRECOND_AMG)
   std::unique_ptr<Amg> amg;
@@ -89,7 +91,7 @@ struct Pcg {
   SellView<float> a32() const { return {L->nrows, L->nslices, L->sptr.p, col32.p, lhat.p}; }
   PackedView packed() const {
     PackedView v;
-    v.on = cop.enabled && !cop.tma;
+    v.on = cop.enabled;
     v.nib = cop.index_bits;
     v.slots = cop.slots;
     v.delta = cop.delta.p;

@@ -392,6 +392,12 @@ class DnsEngine:
         """Per-kernel profile of the AMG V-cycle: [{level, kind, ms, bytes}] in launch order."""
         return _vcycle_profile("gipb200_dns_vcycle_profile", self.handle, reps, stream)
 
+    def setup_profile(self) -> Dict[str, float]:
+        """Host seconds of the engine's creation by stage."""
+        out = np.zeros(4)
+        L.call("gipb200_dns_setup_profile", self.handle, _hptr(out))
+        return dict(zip(("renumbering", "operators", "solver", "total"), out.tolist()))
+
     def phase_bytes(self) -> Dict[str, float]:
         """Algorithmic bytes of each timestep phase (the PCG's is 0: see info())."""
         out = np.zeros(7)

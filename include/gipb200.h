@@ -192,8 +192,8 @@ int gipb200_pcg_solve(gipb200_pcg S, const double* d_b, double* d_x, const doubl
 
 /* No counterpart in the reference: launches a kernel whose shared-memory barrier wait can
  * never complete and writes the status it reported (GIPB200_ERR_TIMEOUT after about one
- * second of SM clock).  Checks on the device that the bounded wait of the staged SpMV
- * gives up instead of hanging; the context stays usable. */
+ * second of SM clock).  Checks on the device that the library's bounded barrier wait gives
+ * up instead of hanging; the context stays usable. */
 int gipb200_check_bounded_wait(void* stream, int* h_status);
 
 /* No counterpart in the reference: how the solver stores its operator. */
@@ -377,6 +377,10 @@ int gipb200_dns_set_launch(gipb200_dns E, int spmv_blocks, int vec_blocks);
  * vectors once, written vectors once).  The PCG entry is 0: a solve moves iterations x
  * iteration_bytes plus replacements x replacement_bytes (gipb200_dns_get_info). */
 int gipb200_dns_phase_bytes(gipb200_dns E, double* h_bytes);
+/* Host seconds the engine's creation took: h_seconds[0] checks and renumbering, [1] the
+ * operators' device layouts and the fields, [2] the pressure solver (FP32 operator,
+ * packing, AMG hierarchy), [3] the whole of gipb200_dns_create. */
+int gipb200_dns_setup_profile(gipb200_dns E, double* h_seconds);
 /* gipb200_pcg_vcycle_profile for the engine's pressure solver (precond = AMG). */
 int gipb200_dns_vcycle_profile(gipb200_dns E, int reps, void* stream, int cap, int* n_kernels,
                                int* h_level, int* h_kind, double* h_ms, double* h_bytes);
