@@ -434,6 +434,11 @@ __device__ __forceinline__ bool amg_enter(PcgScalars* S) {
 
 __device__ __forceinline__ float fmat(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ double fmat(double a, double b, double c) { return fma(a, b, c); }
+// a * b rounded on its own (the Jacobi start x = D^-1 b, formed where it is gathered)
+__device__ __forceinline__ float mulr(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mulr(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float addr(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double addr(double a, double b) { return __dadd_rn(a, b); }
 
 // Stored operator values to the arithmetic type (FP16-stored transfer operators).
 __device__ __forceinline__ float to_arith(__half v) { return __half2float(v); }
@@ -442,9 +447,12 @@ __device__ __forceinline__ double to_arith(double v) { return v; }
 
 // One row of a sliced operator whose slice starts at slot `base` and has `len` slots,
 // summed slot by slot (padding: column -1, skipped).
+// xs (optional): the gathered vector is xs * x elementwise, each product rounded on its
+// own (the same value a separate x = xs * x pass would store).
 template <typename T, int CH, typename V = T>
 __device__ __forceinline__ T amg_row_at(const SellView<V>& A, const T* __restrict__ x,
-                                        long long base, int len, int lane) {
+                                        long long base, int len, int lane,
+                                        const T* __restrict__ xs = nullptr) {
   const int* cp = A.col + base + lane;
   const V* vp = A.val + base + lane;
   T sum = T(0);
@@ -458,7 +466,8 @@ __device__ __forceinline__ T amg_row_at(const SellView<V>& A, const T* __restric
     }
     T xv[CH];
 #pragma unroll
-    for (int t = 0; t < CH; ++t) xv[t] = (c[t] >= 0) ? __ldg(x + c[t]) : T(0);
+    for (int t = 0; t < CH; ++t)
+      xv[t] = (c[t] >= 0) ? (xs ? mulr(__ldg(xs + c[t]), __ldg(x + c[t])) : __ldg(x + c[t])) : T(0);
 #pragma unroll
     for (int t = 0; t < CH; ++t) sum = fmat(xv[t], v[t], sum);
   }
@@ -481,7 +490,9 @@ __global__ void __launch_bounds__(256) k_amg_jacobi0(int n, const T* __restrict_
     x[i] = dinv[i] * b[i];
 }
 
-enum { kResid = 0, kPlain = 1, kAdd = 2, kSmooth = 3, kScaleAdd = 4 };
+enum { kResid = 0, kPlain = 1, kAdd = 2, kSmooth = 3, kScaleAdd = 4, kDiagAdd = 5 };
+// kDiagAdd: y = D^-1 b + A x (a coarse level's prolongation onto its Jacobi start, which
+// the cycle no longer forms: rounded as the two separate steps round it)
 // kResid: y = b - A x;  kPlain: y = A x;  kAdd: y += A x;  kSmooth: y = x + dinv (b - A x);
 // kScaleAdd: y = w b + A x (the level-0 prolongation onto x0 = w r, never formed)
 template <typename T, int MODE, typename V = T>
@@ -489,7 +500,8 @@ __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __r
                                                      const T* __restrict__ b,
                                                      const T* __restrict__ dinv,
                                                      T* __restrict__ y, PcgScalars* S, T w,
-                                                     const int* __restrict__ yperm = nullptr) {
+                                                     const int* __restrict__ yperm = nullptr,
+                                                     const T* __restrict__ xs = nullptr) {
   if (amg_enter(S)) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -500,7 +512,7 @@ __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __r
   for (int s = gw; s < A.nslices; s += nw) {
     long long n0 = 0, n1 = 0;
     if (s + nw < A.nslices) n0 = __ldg(A.sptr + s + nw), n1 = __ldg(A.sptr + s + nw + 1);
-    const T sum = amg_row_at<T, 4, V>(A, x, b0, (int)((b1 - b0) >> 5), lane);
+    const T sum = amg_row_at<T, 4, V>(A, x, b0, (int)((b1 - b0) >> 5), lane, xs);
     b0 = n0;
     b1 = n1;
     const int i = s * 32 + lane;
@@ -510,6 +522,7 @@ __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __r
       else if (MODE == kPlain) y[i] = sum;
       else if (MODE == kAdd) y[i] += sum;
       else if (MODE == kScaleAdd) y[i] = fmat(w, b[i], sum);
+      else if (MODE == kDiagAdd) y[i] = addr(mulr(dinv[i], b[i]), sum);
       else y[i] = fmat(dinv[i], b[i] - sum, x[i]);
     }
   }
@@ -528,7 +541,7 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
                                                  const V* __restrict__ val, const T* __restrict__ x,
                                                  const T* __restrict__ b,
                                                  const T* __restrict__ dinv, T* __restrict__ y,
-                                                 PcgScalars* S, T w) {
+                                                 PcgScalars* S, T w, const T* __restrict__ xs) {
   if (amg_enter(S)) return;
   constexpr int RPW = 32 / LANES;  // rows per warp per pass
   constexpr int U = 4;             // entries a lane loads before their gathers
@@ -560,7 +573,9 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
       }
       T xv[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) xv[u] = (c[u] >= 0) ? __ldg(x + c[u]) : T(0);
+      for (int u = 0; u < U; ++u)
+        xv[u] = (c[u] >= 0) ? (xs ? mulr(__ldg(xs + c[u]), __ldg(x + c[u])) : __ldg(x + c[u]))
+                            : T(0);
 #pragma unroll
       for (int u = 0; u < U; ++u)
         if (c[u] >= 0) sum = fmat((T)to_arith(v[u]), xv[u], sum);
@@ -572,6 +587,7 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
       else if (MODE == kPlain) y[i] = sum;
       else if (MODE == kAdd) y[i] += sum;
       else if (MODE == kScaleAdd) y[i] = fmat(w, b[i], sum);
+      else if (MODE == kDiagAdd) y[i] = addr(mulr(dinv[i], b[i]), sum);
       else y[i] = fmat(dinv[i], b[i] - sum, x[i]);
     }
     kb = kbn;
@@ -584,42 +600,39 @@ int vec_blocks(int n);
 // y (mode) A x for an AMG operator in either form.
 template <typename T, int MODE, typename V>
 void amg_mv_v(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const T* b,
-              const T* dinv, T* y, PcgScalars* S, cudaStream_t s, T w) {
+              const T* dinv, T* y, PcgScalars* S, cudaStream_t s, T w, const T* xs) {
   if (M.lanes == 0) {
-    k_amg_spmv<T, MODE, V><<<vec_blocks(M.nslices * 32), 256, 0, s>>>(view, x, b, dinv, y, S, w);
+    k_amg_spmv<T, MODE, V><<<vec_blocks(M.nslices * 32), 256, 0, s>>>(view, x, b, dinv, y, S, w,
+                                                                      nullptr, xs);
     return;
   }
   const int nb = vec_blocks((int)std::min<long long>((long long)M.nrows * M.lanes, 1LL << 30));
   const int* rp = M.rp.p;
+#define GIPB_CSR(L, CI, COLS) \
+  k_amg_csr<T, MODE, L, V, CI><<<nb, 256, 0, s>>>(M.nrows, rp, COLS, v, x, b, dinv, y, S, w, xs)
   if (M.short_cols) {
-    const short* ci = M.dcol.p;
-    if (M.lanes == 32)
-      k_amg_csr<T, MODE, 32, V, short><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
-    else if (M.lanes == 16)
-      k_amg_csr<T, MODE, 16, V, short><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
-    else
-      k_amg_csr<T, MODE, 8, V, short><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
-    return;
+    if (M.lanes == 32) GIPB_CSR(32, short, M.dcol.p);
+    else if (M.lanes == 16) GIPB_CSR(16, short, M.dcol.p);
+    else GIPB_CSR(8, short, M.dcol.p);
+  } else {
+    if (M.lanes == 32) GIPB_CSR(32, int, M.col.p);
+    else if (M.lanes == 16) GIPB_CSR(16, int, M.col.p);
+    else GIPB_CSR(8, int, M.col.p);
   }
-  const int* ci = M.col.p;
-  if (M.lanes == 32)
-    k_amg_csr<T, MODE, 32, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
-  else if (M.lanes == 16)
-    k_amg_csr<T, MODE, 16, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
-  else
-    k_amg_csr<T, MODE, 8, V><<<nb, 256, 0, s>>>(M.nrows, rp, ci, v, x, b, dinv, y, S, w);
+#undef GIPB_CSR
 }
 
+// y (mode) A x; xs (optional) scales the gathered x elementwise.
 template <typename T, int MODE>
 void amg_mv(const SellT<T>& M, const T* x, const T* b, const T* dinv, T* y, PcgScalars* S,
-            cudaStream_t s, T w = T(1)) {
+            cudaStream_t s, T w = T(1), const T* xs = nullptr) {
   if constexpr (std::is_same<T, float>::value) {
     if (M.half) {
-      amg_mv_v<T, MODE, __half>(M, M.hview(), M.hval.p, x, b, dinv, y, S, s, w);
+      amg_mv_v<T, MODE, __half>(M, M.hview(), M.hval.p, x, b, dinv, y, S, s, w, xs);
       return;
     }
   }
-  amg_mv_v<T, MODE, T>(M, M.view(), M.val.p, x, b, dinv, y, S, s, w);
+  amg_mv_v<T, MODE, T>(M, M.view(), M.val.p, x, b, dinv, y, S, s, w, xs);
 }
 
 struct CycleFinish {
@@ -969,7 +982,9 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     const T* b = l == 0 ? r : V.b.p;
     const double n = V.n, nn = lv[l + 1]->n;
     const bool skip = l == 0 && u0;
-    if (!skip) {
+    // levels >= 1 gather D^-1 b where they would gather the Jacobi start x = D^-1 b
+    const bool fold = l > 0;
+    if (!skip && !fold) {
       GIPB_TRY(mark(l, GIPB200_CYCLE_JACOBI0, 3.0 * n * w));
       k_amg_jacobi0<T><<<vec_blocks(V.n), 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
     }
@@ -983,8 +998,8 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
       else
         k_amg_spmv<T, kResid><<<bs, 256, 0, s>>>(A0, skip ? r : V.x.p, b, nullptr, V.t.p, S,
                                                   skip ? (T)omega0 : T(1), perm0.p);
-    } else {
-      amg_mv<T, kResid>(V.A, V.x.p, b, (const T*)nullptr, V.t.p, S, s);
+    } else {  // t = b - A (D^-1 b)
+      amg_mv<T, kResid>(V.A, b, b, (const T*)nullptr, V.t.p, S, s, T(1), V.dinv.p);
     }
     GIPB_TRY(mark(l, GIPB200_CYCLE_RESTRICT, stream_bytes(V.R) + (n + nn) * w));
     amg_mv<T, kPlain>(V.R, V.t.p, (const T*)nullptr, (const T*)nullptr, lv[l + 1]->b.p, S, s);
@@ -999,9 +1014,13 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     const T* xc = (l + 1 == L - 1) ? lv[l + 1]->x.p : lv[l + 1]->t.p;
     const double n = V.n, nn = lv[l + 1]->n;
     const bool skip = l == 0 && u0;
-    GIPB_TRY(mark(l, GIPB200_CYCLE_PROLONG, stream_bytes(V.P) + (nn + 2.0 * n) * w));
+    const bool fold = l > 0;
+    GIPB_TRY(mark(l, GIPB200_CYCLE_PROLONG,
+                  stream_bytes(V.P) + (nn + (fold ? 3.0 : 2.0) * n) * w));
     if (skip)  // x0 = omega0 r + P x1
       amg_mv<T, kScaleAdd>(V.P, xc, r, (const T*)nullptr, V.x.p, S, s, (T)omega0);
+    else if (fold)  // x = D^-1 b + P x_coarse
+      amg_mv<T, kDiagAdd>(V.P, xc, V.b.p, V.dinv.p, V.x.p, S, s);
     else
       amg_mv<T, kAdd>(V.P, xc, (const T*)nullptr, (const T*)nullptr, V.x.p, S, s);
     GIPB_TRY(mark(l, GIPB200_CYCLE_SMOOTH, a_bytes(l) + (skip ? 3.0 : 4.0) * n * w));
@@ -1032,11 +1051,12 @@ double AmgT<T>::cycle_bytes(double a0_stream_bytes) const {
     const double n = V.n, nn = lv[l + 1]->n;
     const double a = l == 0 ? a0_stream_bytes : stream_bytes(V.A);
     const bool skip = l == 0 && unit0;                   // x0 = omega0 r not formed
-    if (!skip) b += 3.0 * n * w;                         // x = dinv b
+    const bool fold = l > 0;                             // x = D^-1 b formed where gathered
+    if (!skip && !fold) b += 3.0 * n * w;                // x = dinv b
     b += a + (skip ? 2.0 : 3.0) * n * w;                 // t = b - A x
     if (l == 0 && perm0.p) b += 4.0 * n;                 // its aggregate-order positions
     b += stream_bytes(V.R) + (n + nn) * w;               // b_next = R t
-    b += stream_bytes(V.P) + (nn + 2.0 * n) * w;         // x += P x_next
+    b += stream_bytes(V.P) + (nn + (fold ? 3.0 : 2.0) * n) * w;  // x (+)= P x_next
     b += a + (skip ? 3.0 : 4.0) * n * w;                 // smoothed x
   }
   b += ((double)nc * nc + 2.0 * nc) * w;                 // dense coarsest

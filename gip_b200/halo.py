@@ -116,9 +116,17 @@ class DeviceOps:
                self.dv._dptr(x), self.dv._stream(None))
 
 
+def _stage_on_host(dist, t: torch.Tensor) -> bool:
+    """gloo moves host tensors only: device buffers are staged through host memory."""
+    return t.is_cuda and dist is not None and dist.get_backend() == "gloo"
+
+
 class HaloExchange:
     """GIP_Topo::update for one rank (GIP_Topo.cpp:176-181): pack the interface cells each
-    neighbour reads, exchange them point to point, unpack the halo cells received."""
+    neighbour reads, exchange them point to point, unpack the halo cells received.  With
+    NCCL the device buffers go straight over NVLink; with gloo (tests of several ranks
+    sharing a GPU, or CPU ranks) device buffers are staged through host memory, as GIP's
+    own Cuda Specification stages every exchange (GIP_VectorCuda.cpp:224-247)."""
 
     def __init__(self, part: GipCase, rank: int, world: int, dist, ops):
         t = part.topo_cols
@@ -139,13 +147,19 @@ class HaloExchange:
             return
         for q, idx, buf in self.sends:
             self.ops.gather(idx, x, buf)
+        host = _stage_on_host(self.dist, x)
+        sb = [(q, buf.cpu() if host else buf) for q, _, buf in self.sends]
+        rb = [(q, torch.empty(buf.shape, dtype=buf.dtype) if host else buf)
+              for q, _, buf in self.recvs]
         P2P = self.dist.P2POp
-        reqs = [P2P(self.dist.isend, buf, q) for q, _, buf in self.sends]
-        reqs += [P2P(self.dist.irecv, buf, q) for q, _, buf in self.recvs]
+        reqs = [P2P(self.dist.isend, b, q) for q, b in sb]
+        reqs += [P2P(self.dist.irecv, b, q) for q, b in rb]
         if reqs:
             for w in self.dist.batch_isend_irecv(reqs):
                 w.wait()
-        for q, idx, buf in self.recvs:
+        for (q, idx, buf), (_, b) in zip(self.recvs, rb):
+            if host:
+                buf.copy_(b)
             self.ops.scatter(idx, buf, x)
 
 
@@ -164,9 +178,9 @@ class SlabPcg:
 
     def _allreduce(self, sc: torch.Tensor, k: int) -> None:
         if self.world > 1:
-            v = sc[k:k + 1].clone()
+            v = sc[k:k + 1].cpu() if _stage_on_host(self.dist, sc) else sc[k:k + 1].clone()
             self.dist.all_reduce(v)
-            sc[k:k + 1] = v
+            sc[k:k + 1] = v.to(sc.device)
 
     def solve(self, b: torch.Tensor, x0: torch.Tensor, maxit: int) -> tuple:
         """x (n_all, halos as exchanged) and the scalars (rz, pAp, alpha, beta, rr)."""

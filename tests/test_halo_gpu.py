@@ -46,3 +46,61 @@ def test_slab_pcg_one_rank_on_device_matches_oracle(gpu, oracle_mod, n, maxit):
     got[ids] = x.cpu().numpy()
     assert np.abs(got[:k] - xr[:k]).max() / np.abs(xr[:k]).max() < 1e-10
     assert np.array_equal(got[k:], x0[k:])
+
+
+def _device_rank(rank, world, port, q, maxit):
+    # one rank of the slab-split solve on the device (ranks share the GPU here: gloo moves
+    # the halos and the dot partials through host memory, no kernel waits on another rank)
+    import datetime
+    import os
+
+    import torch.distributed as dist
+
+    from gip_b200 import formats, halo
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        case, meta = cavity.generate(10, re=400.0, permute_seed=5)
+        rng = np.random.default_rng(5)
+        b = rng.standard_normal(case.n_inner)
+        x0 = rng.standard_normal(case.n_owned) * 0.1
+        part = formats.split_ranks(case, cavity.slab_partition(meta, world), world)[rank]
+        ids, k = part.cell_ids, part.n_inner
+        S = halo.SlabPcg(part, rank, world, dist=dist, device=torch.device("cuda"))
+        x, sc = S.solve(S.ops.tensor(b[ids[:k]]), S.ops.tensor(x0[ids]), maxit)
+        q.put((rank, ids[:k].tolist(), x[:k].cpu().numpy().tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_slab_pcg_two_ranks_on_device_matches_oracle(gpu, oracle_mod):
+    import socket
+
+    import torch.multiprocessing as mp
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    world, maxit = 2, 60
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_device_rank, args=(r, world, port, q, maxit)) for r in range(world)]
+    for p in ps:
+        p.start()
+    got = [q.get(timeout=300) for _ in range(world)]
+    for p in ps:
+        p.join(120)
+        assert p.exitcode == 0
+    case, meta = cavity.generate(10, re=400.0, permute_seed=5)
+    rng = np.random.default_rng(5)
+    b = rng.standard_normal(case.n_inner)
+    x0 = rng.standard_normal(case.n_owned) * 0.1
+    xr, it, rr = oracle_mod.pcg(case.ops["L"], b, x0, maxit=maxit, mode=0)
+    x = np.full(case.n_owned, np.nan)
+    for _, ids, xs in got:
+        x[ids] = xs
+    k = case.n_inner
+    assert not np.isnan(x[:k]).any()
+    assert np.abs(x[:k] - xr[:k]).max() / np.abs(xr[:k]).max() < 1e-10
