@@ -506,15 +506,9 @@ __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __r
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
-  // the next slice's slot range is loaded while this slice's gathers are in flight
-  long long b0 = 0, b1 = 0;
-  if (gw < A.nslices) b0 = __ldg(A.sptr + gw), b1 = __ldg(A.sptr + gw + 1);
   for (int s = gw; s < A.nslices; s += nw) {
-    long long n0 = 0, n1 = 0;
-    if (s + nw < A.nslices) n0 = __ldg(A.sptr + s + nw), n1 = __ldg(A.sptr + s + nw + 1);
-    const T sum = amg_row_at<T, 4, V>(A, x, b0, (int)((b1 - b0) >> 5), lane, xs);
-    b0 = n0;
-    b1 = n1;
+    const long long b0 = A.sptr[s];
+    const T sum = amg_row_at<T, 4, V>(A, x, b0, (int)((A.sptr[s + 1] - b0) >> 5), lane, xs);
     const int i = s * 32 + lane;
     if (i < A.nrows) {
       // kResid: level 0 may write its residual in aggregate order (yperm)
@@ -696,11 +690,9 @@ __global__ void __launch_bounds__(256, 8) k_amgp_spmv(SellView<float> A, PackedV
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   double acc[1] = {0.0};
-  PackedWords cur, nxt;
-  if (gw < A.nslices) packed_words<NIB>(pk.delta, pk.idx, pk.plain, gw, lane, cur);
-  nxt = cur;
+  PackedWords cur;
   for (int s = gw; s < A.nslices; s += nw) {
-    if (s + nw < A.nslices) packed_words<NIB>(pk.delta, pk.idx, pk.plain, s + nw, lane, nxt);
+    packed_words<NIB>(pk.delta, pk.idx, pk.plain, s, lane, cur);
     const int i = s * 32 + lane;
     float sum;
     if (cur.plain) {
@@ -725,7 +717,6 @@ __global__ void __launch_bounds__(256, 8) k_amgp_spmv(SellView<float> A, PackedV
         acc[0] += (double)ri * (double)zi;
       }
     }
-    cur = nxt;
   }
   if (MODE == kSmooth) grid_reduce<SumOp, 1>(acc, rs, CycleFinish{S, first});
 }
@@ -837,6 +828,18 @@ int host_hierarchy(int n, const int* rp, const int* ci, const double* v, const d
     const int na = aggregate(A, d, agg);
     if (na == 0 || na > 0.8 * A.nr)
       return fail(GIPB200_ERR_ARG, "AMG: level %d (%d unknowns) coarsens only to %d", l, A.nr, na);
+    // aggregates numbered by their first row: the coarse unknowns follow the fine order
+    // (the greedy passes number the leftover aggregates last, far from their neighbours)
+    {
+      std::vector<int> first((size_t)na, A.nr);
+      for (int i = 0; i < A.nr; ++i) first[agg[i]] = std::min(first[agg[i]], i);
+      std::vector<int> ord((size_t)na);
+      for (int a = 0; a < na; ++a) ord[a] = a;
+      std::sort(ord.begin(), ord.end(), [&](int a, int b) { return first[a] < first[b]; });
+      std::vector<int> relabel((size_t)na);
+      for (int k = 0; k < na; ++k) relabel[ord[k]] = k;
+      for (int i = 0; i < A.nr; ++i) agg[i] = relabel[agg[i]];
+    }
     std::vector<double> nrm((size_t)na, 0.0);
     for (int i = 0; i < A.nr; ++i) nrm[agg[i]] += z[i] * z[i];
     for (auto& q : nrm) q = std::sqrt(q);

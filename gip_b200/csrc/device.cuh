@@ -102,9 +102,9 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[K], ReduceScratch 
 // ------------------------------------------------------------------ packed FP32 rows
 // The mixed form's compressed operator: per row one 16-byte word of eight 16-bit column
 // deltas from per-(slice, slot) int32 bases, and eight value-table indices (4 or 8 bits).
-// A kernel loads a slice's words one slice ahead of their use (software pipelining): the
-// words' memory latency then overlaps the previous slice's gathers instead of adding a
-// second dependent round trip to every row.
+// (Loading a slice's words one slice ahead of their use measured slower at the 32
+// registers these kernels keep for full occupancy: 147.7 against 138.6 us per CG SpMV-dot
+// on the 256^3 cavity.)
 struct PackedWords {
   uint4 d;          // column deltas
   unsigned w0, w1;  // value-table indices
@@ -226,6 +226,51 @@ __device__ __forceinline__ void sell_row_f64_pair(const SellView<V>& A, const do
         sum2 = dadd(sum2, dmul(b[t], (double)v[t]));
         any = true;
       }
+  }
+}
+
+// Three sliced operators' rows walked together (sum_k = row s of M_k . x_k, each summed slot
+// by slot with GIP's rounding, any_k = the row has a stored nonzero): the slot loads of all
+// three and then their gathers are in flight at once, three dependent round trips per row
+// instead of nine.  The same results as three sell_row_f64 calls.
+__device__ __forceinline__ void sell_rows3_f64(const SellView<double> (&M)[3],
+                                               const double* const (&x)[3], int s, int lane,
+                                               double (&sum)[3], bool (&any)[3]) {
+  long long base[3];
+  int len[3], len_max = 0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    base[k] = 0;
+    len[k] = 0;
+    if (s < M[k].nslices) {
+      base[k] = M[k].sptr[s];
+      len[k] = (int)((M[k].sptr[s + 1] - base[k]) >> 5);
+    }
+    len_max = max(len_max, len[k]);
+  }
+  for (int j0 = 0; j0 < len_max; j0 += 2) {
+    int c[3][2];
+    double v[3][2], xv[3][2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int j = j0 + t;
+        c[k][t] = (j < len[k]) ? ld_stream(M[k].col + base[k] + 32LL * j + lane) : -1;
+        v[k][t] = (j < len[k]) ? ld_stream(M[k].val + base[k] + 32LL * j + lane) : 0.0;
+      }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int t = 0; t < 2; ++t) xv[k][t] = (c[k][t] >= 0) ? __ldg(x[k] + c[k][t]) : 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int t = 0; t < 2; ++t)
+        if (c[k][t] >= 0) {
+          sum[k] = dadd(sum[k], dmul(xv[k][t], v[k][t]));
+          any[k] = true;
+        }
   }
 }
 

@@ -111,11 +111,13 @@ __global__ void __launch_bounds__(256) k_dns_rhs(SellView<double> Mx, SellView<d
   const int ns = max(Mx.nslices, max(My.nslices, Mz.nslices));
   for (int s = gw; s < ns; s += nw) {
     const int i = s * 32 + lane;
-    double sx = 0, sy = 0, sz = 0;
-    bool ax = false, ay = false, az = false;
-    if (s < Mx.nslices) sell_row_f64(Mx, u, s, lane, sx, ax);
-    if (s < My.nslices) sell_row_f64(My, v, s, lane, sy, ay);
-    if (s < Mz.nslices) sell_row_f64(Mz, w, s, lane, sz, az);
+    const SellView<double> M[3] = {Mx, My, Mz};
+    const double* const X[3] = {u, v, w};
+    double sm[3] = {0, 0, 0};
+    bool an[3] = {false, false, false};
+    sell_rows3_f64(M, X, s, lane, sm, an);
+    const double sx = sm[0], sy = sm[1], sz = sm[2];
+    bool ax = an[0], ay = an[1], az = an[2];
     ax = ax && i < Mx.nrows;
     ay = ay && i < My.nrows;
     az = az && i < Mz.nrows;
@@ -154,11 +156,13 @@ __global__ void __launch_bounds__(256) k_dns_gradcorr(SellView<double> Gx, SellV
   const int ns = max(max(Gx.nslices, Gy.nslices), max(Gz.nslices, (n_inner + 31) / 32));
   for (int s = gw; s < ns; s += nw) {
     const int i = s * 32 + lane;
-    double sx = 0, sy = 0, sz = 0;
-    bool ax = false, ay = false, az = false;
-    if (s < Gx.nslices) sell_row_f64(Gx, p, s, lane, sx, ax);
-    if (s < Gy.nslices) sell_row_f64(Gy, p, s, lane, sy, ay);
-    if (s < Gz.nslices) sell_row_f64(Gz, p, s, lane, sz, az);
+    const SellView<double> G[3] = {Gx, Gy, Gz};
+    const double* const X[3] = {p, p, p};
+    double sm[3] = {0, 0, 0};
+    bool an[3] = {false, false, false};
+    sell_rows3_f64(G, X, s, lane, sm, an);
+    const double sx = sm[0], sy = sm[1], sz = sm[2];
+    const bool ax = an[0], ay = an[1], az = an[2];
     if (ax && i < Gx.nrows) gpx[i] = sx;
     if (ay && i < Gy.nrows) gpy[i] = sy;
     if (az && i < Gz.nrows) gpz[i] = sz;
@@ -193,48 +197,60 @@ __global__ void __launch_bounds__(256) k_dns_massflux3(
     const int f = s * 32 + lane;
     double so = 0;
     bool a0 = false;
-    if (s < SO.nslices) sell_row_f64(SO, p, s, lane, so, a0);
     double gx = 0, gy = 0, gz = 0, ux = 0, uy = 0, uz = 0;
     int cx = 0, cy = 0, cz = 0;
+    // SO and the merged SF rows are walked together, so the slot loads of both and then
+    // the gathers of both are in flight at once (three dependent round trips per face)
+    long long ob = 0, fb = 0;
+    int ol = 0, fl = 0;
+    if (s < SO.nslices) ob = SO.sptr[s], ol = (int)((SO.sptr[s + 1] - ob) >> 5);
     if (s < SF.nslices) {
+      fb = SF.sptr[s];
+      fl = (int)((SF.sptr[s + 1] - fb) >> 5);
       const unsigned c = (f < SF.nrows) ? cnt[f] : 0u;
       cx = c & 15u;
       cy = (c >> 4) & 15u;
       cz = (c >> 8) & 15u;
-      const long long base = SF.sptr[s];
-      const int len = (int)((SF.sptr[s + 1] - base) >> 5);
-      for (int j0 = 0; j0 < len; j0 += 2) {
-        int col[2];
-        double val[2];
+    }
+    const int len = max(ol, fl);
+    for (int j0 = 0; j0 < len; j0 += 2) {
+      int oc[2], fc[2];
+      double ov[2], fv[2];
 #pragma unroll
-        for (int t = 0; t < 2; ++t) {
-          const long long k = base + 32LL * (j0 + t) + lane;
-          col[t] = (j0 + t < len) ? ld_stream(SF.col + k) : -1;
-          val[t] = (j0 + t < len) ? ld_stream(SF.val + k) : 0.0;
+      for (int t = 0; t < 2; ++t) {
+        const int j = j0 + t;
+        oc[t] = (j < ol) ? ld_stream(SO.col + ob + 32LL * j + lane) : -1;
+        ov[t] = (j < ol) ? ld_stream(SO.val + ob + 32LL * j + lane) : 0.0;
+        fc[t] = (j < fl) ? ld_stream(SF.col + fb + 32LL * j + lane) : -1;
+        fv[t] = (j < fl) ? ld_stream(SF.val + fb + 32LL * j + lane) : 0.0;
+      }
+      double op[2], a[2], b[2];
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int j = j0 + t;
+        const double* g = (j < cx) ? gpx : (j < cx + cy) ? gpy : gpz;
+        const double* q = (j < cx) ? u : (j < cx + cy) ? v : w;
+        op[t] = (oc[t] >= 0) ? __ldg(p + oc[t]) : 0.0;
+        a[t] = (fc[t] >= 0) ? __ldg(g + fc[t]) : 0.0;
+        b[t] = (fc[t] >= 0) ? __ldg(q + fc[t]) : 0.0;
+      }
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        if (oc[t] >= 0) {  // SO's row, slot by slot as sell_row_f64 sums it
+          so = dadd(so, dmul(op[t], ov[t]));
+          a0 = true;
         }
-        double a[2], b[2];
-#pragma unroll
-        for (int t = 0; t < 2; ++t) {
-          const int j = j0 + t;
-          const double* g = (j < cx) ? gpx : (j < cx + cy) ? gpy : gpz;
-          const double* q = (j < cx) ? u : (j < cx + cy) ? v : w;
-          a[t] = (col[t] >= 0) ? __ldg(g + col[t]) : 0.0;
-          b[t] = (col[t] >= 0) ? __ldg(q + col[t]) : 0.0;
-        }
-#pragma unroll
-        for (int t = 0; t < 2; ++t) {
-          if (col[t] < 0) continue;
-          const int j = j0 + t;
-          if (j < cx) {
-            gx = dadd(gx, dmul(a[t], val[t]));
-            ux = dadd(ux, dmul(b[t], val[t]));
-          } else if (j < cx + cy) {
-            gy = dadd(gy, dmul(a[t], val[t]));
-            uy = dadd(uy, dmul(b[t], val[t]));
-          } else {
-            gz = dadd(gz, dmul(a[t], val[t]));
-            uz = dadd(uz, dmul(b[t], val[t]));
-          }
+        if (fc[t] < 0) continue;
+        const int j = j0 + t;
+        if (j < cx) {
+          gx = dadd(gx, dmul(a[t], fv[t]));
+          ux = dadd(ux, dmul(b[t], fv[t]));
+        } else if (j < cx + cy) {
+          gy = dadd(gy, dmul(a[t], fv[t]));
+          uy = dadd(uy, dmul(b[t], fv[t]));
+        } else {
+          gz = dadd(gz, dmul(a[t], fv[t]));
+          uz = dadd(uz, dmul(b[t], fv[t]));
         }
       }
     }

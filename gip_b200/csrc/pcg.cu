@@ -529,11 +529,9 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   double acc[1] = {0.0};
-  PackedWords cur, nxt;
-  if (gw < A.nslices) packed_words<NIB>(delta, idx, plain, gw, lane, cur);
-  nxt = cur;
+  PackedWords cur;
   for (int s = gw; s < A.nslices; s += nw) {
-    if (s + nw < A.nslices) packed_words<NIB>(delta, idx, plain, s + nw, lane, nxt);
+    packed_words<NIB>(delta, idx, plain, s, lane, cur);
     const int i = s * 32 + lane;
     float sum;
     if (cur.plain) {  // rare fallback: few registers
@@ -556,7 +554,6 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
       Ap[i] = api;
       acc[0] += (double)pi * (double)api;
     }
-    cur = nxt;
   }
   grid_reduce<SumOp, 1>(acc, rs, AlphaFinish32{S});
 }
