@@ -9,11 +9,19 @@ kernels (CUDA events over live launches, ``gipb200_dns_kernel_time``) for a few 
 grid, and keeps the fastest of each.  The slice height (32 rows, one warp) and the block
 (256 threads) are fixed by the sliced layout and the reductions.  Results are cached per
 (kernel, rows, nnz) in memory and, if ``path`` is given, in a JSON file.
+
+For a batch solved by the persistent launch (``tune_batch``) the tuner times whole batch
+steps for each launch shape -- threads per CTA (128, 256, 512) and rows per warp pass (32:
+one slice per warp; 64: two slices interleaved) -- keeps the fastest, then re-splits the
+CTAs by the measured work (rows times the iterations of the last steps) and keeps that
+split if it is faster.
 """
 from __future__ import annotations
 
 import json
 import os
+
+import numpy as np
 from typing import Dict, Optional, Sequence
 
 _CACHE: Dict[str, dict] = {}
@@ -61,3 +69,40 @@ def tune(engine, kernel: str = "mixed", rows: int = 0, nnz: int = 0,
         with open(path, "w") as f:
             json.dump(_CACHE, f)
     return dict(out, cached=False, ms=timings)
+
+
+BATCH_SHAPES = ((128, 32), (256, 32), (512, 32), (128, 64), (256, 64), (512, 64))
+
+
+def tune_batch(batch, stream, shapes: Sequence = BATCH_SHAPES, steps: int = 2) -> dict:
+    """Pick the persistent solve's launch shape and CTA split for `batch` (a DnsBatch) by
+    timing `steps` whole batch steps per candidate (the instances advance meanwhile)."""
+    import torch
+
+    def timed():
+        batch.advance(1, stream)  # capture outside the timed steps
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        batch.advance(steps, stream)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms = {}
+    for block, rpw in shapes:
+        batch.set_solver(True, block, rpw)
+        ms[(block, rpw)] = timed()
+    best = min(ms, key=ms.get)
+    batch.set_solver(True, *best)
+    t_default = timed()
+    rows = np.array([e.n_inner for e in batch.instances], np.float64)
+    iters = np.array([max(float(np.mean(e.history()["iters"][-steps:])), 1.0)
+                      for e in batch.instances])
+    batch.balance(rows * iters)
+    t_measured = timed()
+    balanced = t_measured < t_default
+    if not balanced:
+        batch.balance(None)
+    return {"block": best[0], "rows_per_warp": best[1], "balanced_by_iterations": balanced,
+            "ms": {f"{b}x{r}": round(v, 3) for (b, r), v in ms.items()},
+            "ms_default_split": round(t_default, 3), "ms_measured_split": round(t_measured, 3)}

@@ -478,57 +478,66 @@ int Dns::enqueue_initial_dt(cudaStream_t s) {
   return GIPB200_OK;
 }
 
-int Dns::enqueue_step(cudaStream_t s, bool host_sync) {
+int Dns::enqueue_step(cudaStream_t s, bool host_sync, int part) {
   const DnsHistory H = history();
   const long long pcg_before = pcg.launches;
   auto mark = [&](int k) {
     if (phase_events) cudaEventRecord(phase_events[k], s);
     if (stamps_on) k_dns_stamp<<<1, 1, 0, s>>>(sc.p, H, k);
   };
-  mark(0);
-  // PredictorVelocity: C's values from the face fluxes, then D/C products and AB2
-  if (ec_slot)
-    GIPB_TRY(launch_csr_spmv(ec_rows, ec_rp.p, ec_col.p, ec_val.p, mf.p, cval.p, nullptr, 0.0, 0.0,
-                             0, s));
-  else
-    GIPB_TRY(launch_csr_spmv(Ec.nrows, Ec.rowptr.p, Ec.csr_col.p, Ec.csr_val.p, mf.p, cval.p,
-                             D.pos.p, 0.0, 0.0, 0, s));
-  k_dns_convdiff<<<grid.convdiff, 256, 0, s>>>(D.view(), cval.p, u.p, v.p, w.p, ax.p, ay.p, az.p);
-  k_dns_ab2<<<grid.ab2, 256, 0, s>>>(N, u.p, v.p, w.p, ax.p, ay.p, az.p, ax0.p, ay0.p, az0.p, sc.p);
-  mark(1);
-  // PoissonEquation
-  k_dns_rhs<<<grid.rhs, 256, 0, s>>>(Mx.view(), My.view(), Mz.view(), u.p, v.p, w.p, rhs.p, sc.p);
-  GIPB_LAUNCH_CHECK();
-  mark(2);
-  GIPB_TRY(pcg.enqueue(rhs.p, p.p, p0.p, s, host_sync));
-  mark(3);
-  k_dns_pcopy<<<blocks_owned, 256, 0, s>>>(N, NO, p.p, p0.p);
-  GIPB_LAUNCH_CHECK();
-  GIPB_TRY(launch_sell_spmv(Lb, Lb.val.p, p0.p, p.p, 1.0, 1.0, 1, s));
-  mark(4);
-  // VelocityCorrection
-  k_dns_gradcorr<<<grid.gradcorr, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p, gpx.p, gpy.p,
-                                               gpz.p, u.p, v.p, w.p, N, prm.rho, sc.p);
-  mark(5);
-  // MassFluxes
-  if (SF3.on)
-    k_dns_massflux3<<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p, p.p, gpx.p,
-                                                  gpy.p, gpz.p, u.p, v.p, w.p, mf.p, prm.rho,
-                                                  sc.p);
-  else
-    k_dns_massflux<<<grid.massflux, 256, 0, s>>>(SO.view(), SFx.view(), SFy.view(), SFz.view(),
-                                                 p.p, gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p,
-                                                 prm.rho, sc.p);
-  mark(6);
-  // CFLCondition
-  k_dns_massr<<<grid.massr, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
-  k_dns_cfl<<<grid.cfl, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p, H,
-                                        pcg.sc.p, 1, prm.pcg.mode == GIPB200_PCG_MIXED, dt_seq.p,
-                                        dt_seq_len, rs);
-  GIPB_LAUNCH_CHECK();
-  mark(7);
-  GIPB_LAUNCH_CHECK();
-  launches += 10 + H.stamp_kernels + (pcg.launches - pcg_before);
+  if (part != 2) {
+    mark(0);
+    // PredictorVelocity: C's values from the face fluxes, then D/C products and AB2
+    if (ec_slot)
+      GIPB_TRY(launch_csr_spmv(ec_rows, ec_rp.p, ec_col.p, ec_val.p, mf.p, cval.p, nullptr, 0.0,
+                               0.0, 0, s));
+    else
+      GIPB_TRY(launch_csr_spmv(Ec.nrows, Ec.rowptr.p, Ec.csr_col.p, Ec.csr_val.p, mf.p, cval.p,
+                               D.pos.p, 0.0, 0.0, 0, s));
+    k_dns_convdiff<<<grid.convdiff, 256, 0, s>>>(D.view(), cval.p, u.p, v.p, w.p, ax.p, ay.p,
+                                                 az.p);
+    k_dns_ab2<<<grid.ab2, 256, 0, s>>>(N, u.p, v.p, w.p, ax.p, ay.p, az.p, ax0.p, ay0.p, az0.p,
+                                       sc.p);
+    mark(1);
+    // PoissonEquation
+    k_dns_rhs<<<grid.rhs, 256, 0, s>>>(Mx.view(), My.view(), Mz.view(), u.p, v.p, w.p, rhs.p,
+                                       sc.p);
+    GIPB_LAUNCH_CHECK();
+    mark(2);
+  }
+  if (part == 0) GIPB_TRY(pcg.enqueue(rhs.p, p.p, p0.p, s, host_sync));
+  if (part != 1) {
+    mark(3);
+    k_dns_pcopy<<<blocks_owned, 256, 0, s>>>(N, NO, p.p, p0.p);
+    GIPB_LAUNCH_CHECK();
+    GIPB_TRY(launch_sell_spmv(Lb, Lb.val.p, p0.p, p.p, 1.0, 1.0, 1, s));
+    mark(4);
+    // VelocityCorrection
+    k_dns_gradcorr<<<grid.gradcorr, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p, gpx.p,
+                                                 gpy.p, gpz.p, u.p, v.p, w.p, N, prm.rho, sc.p);
+    mark(5);
+    // MassFluxes
+    if (SF3.on)
+      k_dns_massflux3<<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p, p.p,
+                                                    gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p,
+                                                    prm.rho, sc.p);
+    else
+      k_dns_massflux<<<grid.massflux, 256, 0, s>>>(SO.view(), SFx.view(), SFy.view(), SFz.view(),
+                                                   p.p, gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p,
+                                                   prm.rho, sc.p);
+    mark(6);
+    // CFLCondition
+    k_dns_massr<<<grid.massr, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
+    k_dns_cfl<<<grid.cfl, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p, H,
+                                          pcg.sc.p, 1, prm.pcg.mode == GIPB200_PCG_MIXED,
+                                          dt_seq.p, dt_seq_len, rs);
+    GIPB_LAUNCH_CHECK();
+    mark(7);
+  }
+  // the step's kernels: 4 before the solve, 6 after it, and the phase stamps
+  const int own = part == 0 ? 10 : part == 1 ? 4 : 6;
+  const int stamps = H.stamp_kernels == 0 ? 0 : part == 0 ? kPhaseMarks : part == 1 ? 3 : 5;
+  launches += own + stamps + (pcg.launches - pcg_before);
   return GIPB200_OK;
 }
 

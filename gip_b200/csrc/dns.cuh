@@ -112,7 +112,9 @@ struct Dns {
   // Algorithmic bytes of each phase of one timestep, in gipb200_dns_step_phases order
   // (the PCG entry is 0: its bytes are iterations x iteration_bytes + replacements).
   void phase_bytes(double out[7]) const;
-  int enqueue_step(cudaStream_t s, bool host_sync);
+  // part 0: the whole step; 1: the phases before the pressure solve; 2: those after it
+  // (a batch runs the solves of all its instances in between).
+  int enqueue_step(cudaStream_t s, bool host_sync, int part = 0);
   int enqueue_initial_dt(cudaStream_t s);
   double* field(const std::string& name, int* n);
 };

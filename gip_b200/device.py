@@ -486,6 +486,33 @@ class DnsBatch:
     def advance(self, nsteps: int, stream=None) -> None:
         L.call("gipb200_batch_advance", self.handle, nsteps, _stream(stream))
 
+    def set_solver(self, persistent: bool, block: int = 256, rows_per_warp: int = 32) -> None:
+        """Pressure solves in one persistent cooperative launch per step (every instance
+        mixed with Jacobi) or, persistent=False, inside each instance's graph branch."""
+        L.call("gipb200_batch_set_solver", self.handle, int(persistent), int(block),
+               int(rows_per_warp))
+
+    def balance(self, weights=None) -> None:
+        """CTA shares of the persistent solve (None: rows x rows^(1/3))."""
+        if weights is None:
+            L.call("gipb200_batch_balance", self.handle, None)
+            return
+        w = np.ascontiguousarray(weights, np.float64)
+        L.call("gipb200_batch_balance", self.handle, w.ctypes.data)
+
+    def layout(self):
+        """(grid, CTAs per instance) of the persistent solve; (0, zeros) when off."""
+        g = C.c_int()
+        n = np.zeros(len(self.instances), np.int32)
+        L.call("gipb200_batch_layout", self.handle, C.byref(g), n.ctypes.data)
+        return g.value, n
+
+    def solver_status(self, stream=None) -> int:
+        """Nonzero when a barrier of the persistent solve gave up since the last call."""
+        e = C.c_int()
+        L.call("gipb200_batch_solver_status", self.handle, _stream(stream), C.byref(e))
+        return e.value
+
     def close(self):
         if getattr(self, "handle", None):
             for e in self.instances:

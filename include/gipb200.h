@@ -416,6 +416,27 @@ int gipb200_batch_destroy(gipb200_batch B);
 int gipb200_batch_instance(gipb200_batch B, int i, gipb200_dns* out);
 /* nsteps timesteps of every instance, one graph launch each, on `stream`. */
 int gipb200_batch_advance(gipb200_batch B, int nsteps, void* stream);
+/* How the batch solves its pressure systems.  persistent = 0 (the default): inside each
+ * instance's graph branch, as a single instance does.  persistent = 1: one cooperative
+ * launch per timestep solves every instance's system, the launch's CTAs split into one
+ * group per instance (shares set by gipb200_batch_balance); each group runs its instance's
+ * mixed-form Jacobi-PCG and leaves when that instance has converged.  Needs every instance
+ * in GIPB200_PCG_MIXED with GIPB200_PRECOND_JACOBI.  block: threads per CTA (128, 256 or
+ * 512); rows_per_warp: 32 (one 32-row slice per warp pass) or 64 (two slices interleaved).
+ * The step graph is captured again at the next advance. */
+int gipb200_batch_set_solver(gipb200_batch B, int persistent, int block, int rows_per_warp);
+/* CTA shares of the persistent solve: weights[i] >= 0 is instance i's expected work (for
+ * example rows times iterations of the last step); null restores the default, rows times
+ * the cube root of rows (Jacobi-PCG iterations grow with the grid edge).  Waits for the
+ * device; a captured step graph keeps working (same grid, new tables). */
+int gipb200_batch_balance(gipb200_batch B, const double* weights);
+/* The persistent solve's grid and each instance's CTAs (h_ncta: one per instance, or
+ * null); 0 when the batch solves inside its branches. */
+int gipb200_batch_layout(gipb200_batch B, int* grid, int* h_ncta);
+/* *h_err = nonzero when a group barrier of the persistent solve gave up waiting (about 2 s)
+ * since the last call, which clears it; the instances' results are then not valid.
+ * Synchronises `stream`. */
+int gipb200_batch_solver_status(gipb200_batch B, void* stream, int* h_err);
 
 /* ------------------------------------------------------------------ discrete adjoint */
 /* No counterpart in the reference (GIP has no derivatives).  FP64 discrete adjoint of

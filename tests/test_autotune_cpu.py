@@ -57,3 +57,61 @@ def test_grid_capped_and_classes_separate(monkeypatch):
     assert "vec_blocks" not in r                 # the FP64 forms tune the SpMV grid only
     E2 = FakeEngine({2000: 0.1, 4000: 0.2, 8192: 0.25})
     assert autotune.tune(E2, "fp64", rows=6, nnz=9, multiples=(1, 2, 8))["blocks"] == 2000
+
+
+class FakeBatch:
+    """A batch whose step time depends on the persistent launch shape and the CTA split."""
+
+    class Inst:
+        def __init__(self, n, iters):
+            self.n_inner, self._it = n, iters
+
+        def history(self):
+            import numpy as np
+            return {"iters": np.array([self._it] * 4)}
+
+    def __init__(self, ms_by_shape, ms_balanced):
+        self.ms, self.ms_bal = ms_by_shape, ms_balanced
+        self.shape, self.weights = None, None
+        self.instances = [self.Inst(1000, 50), self.Inst(8000, 120)]
+
+    def set_solver(self, persistent, block, rpw):
+        self.shape = (block, rpw)
+
+    def balance(self, w):
+        self.weights = None if w is None else list(w)
+
+    def advance(self, n, stream=None):
+        pass
+
+
+def test_tune_batch_picks_shape_and_split(monkeypatch):
+    import types
+    ms = {(128, 32): 3.0, (256, 32): 2.0, (512, 32): 2.5, (128, 64): 2.8, (256, 64): 1.5,
+          (512, 64): 1.9}
+    B = FakeBatch(ms, 1.2)
+    clock = {"t": 0.0}
+
+    class Ev:
+        def __init__(self, enable_timing=True):
+            self.t = 0.0
+
+        def record(self, stream=None):
+            clock["t"] += B.ms_bal if B.weights else B.ms[B.shape]
+            self.t = clock["t"]
+
+        def synchronize(self):
+            pass
+
+        def elapsed_time(self, other):
+            return (other.t - self.t) * 2  # two timed steps
+
+    fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(Event=Ev))
+    monkeypatch.setitem(__import__("sys").modules, "torch", fake_torch)
+    r = autotune.tune_batch(B, None, steps=2)
+    assert (r["block"], r["rows_per_warp"]) == (256, 64) and B.shape == (256, 64)
+    assert r["balanced_by_iterations"] and B.weights == [1000 * 50.0, 8000 * 120.0]
+    B2 = FakeBatch(ms, 9.0)  # the measured split is slower: the default split is restored
+    B = B2
+    r = autotune.tune_batch(B2, None, steps=2)
+    assert not r["balanced_by_iterations"] and B2.weights is None

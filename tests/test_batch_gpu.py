@@ -37,3 +37,56 @@ def test_autotune_picks_a_grid(gpu):
     assert r["blocks"] > 0
     E.advance(2)  # the re-captured step still converges
     assert np.all(E.history()["massr"] < 1e-4)
+
+
+@pytest.mark.parametrize("block,rows_per_warp", [(256, 32), (128, 64), (512, 32)])
+def test_persistent_solve_matches_branch_solves(gpu, block, rows_per_warp):
+    """The persistent launch (one CTA group per instance, the group's own convergence loop)
+    against the same batch solving inside its graph branches: same algorithm (mixed
+    Jacobi-PCG with reliable updates), so the steps agree to the solve's tolerance; every
+    group barrier completed."""
+    from gip_b200.device import DnsBatch, dns_params
+    specs = [(6, 100.0), (10, 400.0), (8, 1000.0), (12, 250.0)]
+    cases = [cavity.generate(n, re=re, permute_seed=7)[0] for n, re in specs]
+    kw = dict(pcg_mode="mixed", maxit=4000, tol=1e-10, inner_tol=0.3, max_outer=200)
+    params = [dns_params(gamma=1.0 / re, **kw) for _, re in specs]
+    A = DnsBatch(cases, params)
+    A.advance(5)
+    B = DnsBatch(cases, params)
+    B.set_solver(True, block, rows_per_warp)
+    grid, ncta = B.layout()
+    assert grid > 0 and ncta.min() >= 1 and ncta.sum() <= grid
+    B.advance(5)
+    assert B.solver_status() == 0
+    for (n, re), ea, eb in zip(specs, A.instances, B.instances):
+        ha, hb = ea.history(), eb.history()
+        assert np.all(hb["massr"] < 1e-6), (n, hb["massr"])
+        assert np.all(np.abs(hb["iters"] - ha["iters"]) <= 0.1 * ha["iters"] + 3), (n, ha, hb)
+        assert np.allclose(hb["time"], ha["time"], rtol=1e-7, atol=0)
+        scale = np.abs(ea.field("u")).max()
+        for k in ("u", "v", "w"):
+            err = np.abs(eb.field(k) - ea.field(k)).max() / scale
+            assert err < 1e-8, (n, k, err)
+    # one launch for the whole batch's solves, counted on the first instance
+    k0 = B.instances[0].history()["kernels"]
+    k1 = B.instances[1].history()["kernels"]
+    assert np.all(k0 == 11) and np.all(k1 == 10)
+
+
+def test_persistent_balance_keeps_graph(gpu):
+    """New CTA shares take effect in the already-captured step graph."""
+    from gip_b200.device import DnsBatch, dns_params
+    specs = [(8, 100.0), (14, 1000.0)]
+    cases = [cavity.generate(n, re=re)[0] for n, re in specs]
+    kw = dict(pcg_mode="mixed", maxit=4000, tol=1e-8, inner_tol=0.3, max_outer=200)
+    B = DnsBatch(cases, [dns_params(gamma=1.0 / re, **kw) for _, re in specs])
+    B.set_solver(True, 256, 32)
+    B.advance(2)
+    g0, n0 = B.layout()
+    B.balance([1.0, 0.0])  # the second instance gets the minimum share
+    g1, n1 = B.layout()
+    assert g1 == g0 and n1[1] == 1 and n1[0] > n0[0] - 1
+    B.advance(2)
+    assert B.solver_status() == 0
+    for e in B.instances:
+        assert np.all(e.history()["massr"] < 1e-6)
