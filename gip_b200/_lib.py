@@ -138,6 +138,7 @@ _SIGNATURES = {
     "gipb200_batch_balance": (_I, [_VP, _VP]),
     "gipb200_batch_layout": (_I, [_VP, C.POINTER(_I), _VP]),
     "gipb200_batch_solver_status": (_I, [_VP, _VP, C.POINTER(_I)]),
+    "gipb200_batch_check_bounded_wait": (_I, [_VP, C.POINTER(_I)]),
     "gipb200_dns_create": (_I, [C.POINTER(DnsOps), _VP, _VP, _VP, _VP, C.POINTER(DnsParams),
                                 C.POINTER(_VP)]),
     "gipb200_dns_destroy": (_I, [_VP]),

@@ -352,4 +352,9 @@ int gipb200_batch_solver_status(gipb200_batch H, void* stream, int* h_err) {
   return GIPB200_OK;
 }
 
+int gipb200_batch_check_bounded_wait(void* stream, int* h_status) {
+  if (!h_status) return fail(GIPB200_ERR_ARG, "null status");
+  return batch_pcg_check_timeout(as_stream(stream), h_status);
+}
+
 }  // extern "C"

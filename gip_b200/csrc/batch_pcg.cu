@@ -482,6 +482,44 @@ int dispatch(const BatchShape& sh, int grid, const BatchSolve* inst, const int* 
 
 }  // namespace
 
+// One CTA whose group claims two: its first barrier waits for a CTA that does not exist and
+// gives up after the bounded spin.
+int batch_pcg_check_timeout(cudaStream_t s, int* h_status) {
+  DevBuf<BatchSolve> inst;
+  DevBuf<int> owner, err;
+  DevBuf<unsigned> bar;
+  DevBuf<double> part;
+  DevBuf<PcgScalars> sc;
+  GIPB_TRY(inst.alloc(1));
+  GIPB_TRY(owner.alloc(1));
+  GIPB_TRY(err.alloc(1));
+  GIPB_TRY(bar.alloc(1));
+  GIPB_TRY(part.alloc((size_t)2 * kBatchWidth * kBatchGroupMax));
+  GIPB_TRY(sc.alloc(1));
+  GIPB_TRY(err.zero(s));
+  GIPB_TRY(bar.zero(s));
+  GIPB_TRY(sc.zero(s));
+  BatchSolve h{};
+  h.S = sc.p;
+  h.part = part.p;
+  h.bar = bar.p;
+  h.pin_row = -1;
+  h.cta0 = 0;
+  h.ncta = 2;
+  const int o = 0;
+  GIPB_CUDA(cudaMemcpyAsync(inst.p, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+  GIPB_CUDA(cudaMemcpyAsync(owner.p, &o, sizeof(int), cudaMemcpyHostToDevice, s));
+  BatchShape sh;
+  GIPB_TRY(batch_pcg_launch(sh, 1, inst.p, owner.p, err.p, s));
+  int e = 0;
+  PcgScalars r{};
+  GIPB_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaMemcpyAsync(&r, sc.p, sizeof(r), cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaStreamSynchronize(s));
+  *h_status = (e != 0 && r.status == GIPB200_ERR_TIMEOUT) ? GIPB200_ERR_TIMEOUT : GIPB200_OK;
+  return GIPB200_OK;
+}
+
 bool batch_shape_valid(const BatchShape& sh) {
   return (sh.block == 128 || sh.block == 256 || sh.block == 512) &&
          (sh.rows_per_warp == 32 || sh.rows_per_warp == 64);

@@ -50,4 +50,8 @@ int batch_pcg_capacity(const BatchShape& sh, int* ctas);
 int batch_pcg_launch(const BatchShape& sh, int grid, const BatchSolve* inst, const int* owner,
                      int* err, cudaStream_t s);
 
+// Runs one persistent launch whose group barrier can never complete and reports
+// GIPB200_ERR_TIMEOUT in *h_status when the bounded wait gave up as designed.
+int batch_pcg_check_timeout(cudaStream_t s, int* h_status);
+
 }  // namespace gipb200

@@ -437,6 +437,10 @@ int gipb200_batch_layout(gipb200_batch B, int* grid, int* h_ncta);
  * since the last call, which clears it; the instances' results are then not valid.
  * Synchronises `stream`. */
 int gipb200_batch_solver_status(gipb200_batch B, void* stream, int* h_err);
+/* Runs one persistent-solve launch whose group barrier waits for a CTA that does not exist:
+ * *h_status = GIPB200_ERR_TIMEOUT when the wait gave up (about 2 s) and the kernel returned
+ * with the error recorded, as designed; the context stays usable.  Synchronises `stream`. */
+int gipb200_batch_check_bounded_wait(void* stream, int* h_status);
 
 /* ------------------------------------------------------------------ discrete adjoint */
 /* No counterpart in the reference (GIP has no derivatives).  FP64 discrete adjoint of

@@ -90,3 +90,19 @@ def test_persistent_balance_keeps_graph(gpu):
     assert B.solver_status() == 0
     for e in B.instances:
         assert np.all(e.history()["massr"] < 1e-6)
+
+
+def test_persistent_barrier_wait_is_bounded(gpu):
+    """A group barrier that can never complete (the group claims a CTA that does not
+    exist) gives up after its bounded spin, records the timeout and returns; the context
+    stays usable."""
+    import ctypes as C
+
+    import torch
+
+    from gip_b200 import _lib
+    st = C.c_int(-1)
+    _lib.call("gipb200_batch_check_bounded_wait", None, C.byref(st))
+    assert st.value == _lib.ERR_TIMEOUT
+    x = torch.ones(1024, device="cuda")
+    assert float(x.sum()) == 1024.0
