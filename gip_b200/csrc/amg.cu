@@ -428,6 +428,7 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool c
 // ------------------------------------------------------------------ V-cycle kernels
 // All of them count their launch and return at once when the solve has finished.
 __device__ __forceinline__ bool amg_enter(PcgScalars* S) {
+  dep_begin();
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&S->kernels, 1);
   return S->done != 0;
 }
@@ -596,14 +597,14 @@ template <typename T, int MODE, typename V>
 void amg_mv_v(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const T* b,
               const T* dinv, T* y, PcgScalars* S, cudaStream_t s, T w, const T* xs) {
   if (M.lanes == 0) {
-    k_amg_spmv<T, MODE, V><<<vec_blocks(M.nslices * 32), 256, 0, s>>>(view, x, b, dinv, y, S, w,
-                                                                      nullptr, xs);
+    launch_dep(k_amg_spmv<T, MODE, V>, vec_blocks(M.nslices * 32), 256, s, view, x, b, dinv, y, S,
+               w, (const int*)nullptr, xs);
     return;
   }
   const int nb = vec_blocks((int)std::min<long long>((long long)M.nrows * M.lanes, 1LL << 30));
   const int* rp = M.rp.p;
 #define GIPB_CSR(L, CI, COLS) \
-  k_amg_csr<T, MODE, L, V, CI><<<nb, 256, 0, s>>>(M.nrows, rp, COLS, v, x, b, dinv, y, S, w, xs)
+  launch_dep(k_amg_csr<T, MODE, L, V, CI>, nb, 256, s, M.nrows, rp, COLS, v, x, b, dinv, y, S, w, xs)
   if (M.short_cols) {
     if (M.lanes == 32) GIPB_CSR(32, short, M.dcol.p);
     else if (M.lanes == 16) GIPB_CSR(16, short, M.dcol.p);
@@ -726,13 +727,13 @@ void launch_amgp(const PackedView& pk, SellView<float> A, int nb, const float* x
                  const float* dinv, float* y, PcgScalars* S, ReduceScratch rs, int first,
                  cudaStream_t s, float w, const int* yperm) {
   if (pk.nib == 4 && pk.slots == 7)
-    k_amgp_spmv<4, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w, yperm);
+    launch_dep(k_amgp_spmv<4, 7, MODE>, nb, 256, s, A, pk, x, b, dinv, y, S, rs, first, w, yperm);
   else if (pk.nib == 4)
-    k_amgp_spmv<4, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w, yperm);
+    launch_dep(k_amgp_spmv<4, 8, MODE>, nb, 256, s, A, pk, x, b, dinv, y, S, rs, first, w, yperm);
   else if (pk.slots == 7)
-    k_amgp_spmv<8, 7, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w, yperm);
+    launch_dep(k_amgp_spmv<8, 7, MODE>, nb, 256, s, A, pk, x, b, dinv, y, S, rs, first, w, yperm);
   else
-    k_amgp_spmv<8, 8, MODE><<<nb, 256, 0, s>>>(A, pk, x, b, dinv, y, S, rs, first, w, yperm);
+    launch_dep(k_amgp_spmv<8, 8, MODE>, nb, 256, s, A, pk, x, b, dinv, y, S, rs, first, w, yperm);
 }
 
 // Coarsest level: x = C b, one warp per row of the dense inverse.
@@ -989,7 +990,7 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     const bool fold = l > 0;
     if (!skip && !fold) {
       GIPB_TRY(mark(l, GIPB200_CYCLE_JACOBI0, 3.0 * n * w));
-      k_amg_jacobi0<T><<<vec_blocks(V.n), 256, 0, s>>>(V.n, V.dinv.p, b, V.x.p, S);
+      launch_dep(k_amg_jacobi0<T>, vec_blocks(V.n), 256, s, V.n, (const T*)V.dinv.p, b, V.x.p, S);
     }
     GIPB_TRY(mark(l, GIPB200_CYCLE_RESIDUAL, a_bytes(l) + (skip ? 2.0 : 3.0) * n * w +
                                                  (l == 0 && perm0.p ? 4.0 * n : 0.0)));
@@ -999,8 +1000,9 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
         launch_packed0<kResid>(*pk, A0, bs, skip ? r : V.x.p, b, (const T*)nullptr, V.t.p, S, rs,
                                first, s, skip ? (T)omega0 : T(1), perm0.p);
       else
-        k_amg_spmv<T, kResid><<<bs, 256, 0, s>>>(A0, skip ? r : V.x.p, b, nullptr, V.t.p, S,
-                                                  skip ? (T)omega0 : T(1), perm0.p);
+        launch_dep(k_amg_spmv<T, kResid, T>, bs, 256, s, A0, skip ? r : (const T*)V.x.p, b,
+                   (const T*)nullptr, V.t.p, S, skip ? (T)omega0 : T(1), (const int*)perm0.p,
+                   (const T*)nullptr);
     } else {  // t = b - A (D^-1 b)
       amg_mv<T, kResid>(V.A, b, b, (const T*)nullptr, V.t.p, S, s, T(1), V.dinv.p);
     }
@@ -1009,8 +1011,8 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
   }
   const AmgLevel<T>& C = *lv[L - 1];
   GIPB_TRY(mark(L - 1, GIPB200_CYCLE_DENSE, ((double)nc * nc + 2.0 * nc) * w));
-  k_amg_dense<T><<<std::min(kMaxReduceBlocks, (nc + 7) / 8), 256, 0, s>>>(nc, cinv.p, C.b.p,
-                                                                            C.x.p, S);
+  launch_dep(k_amg_dense<T>, std::min(kMaxReduceBlocks, (nc + 7) / 8), 256, s, nc,
+             (const T*)cinv.p, (const T*)C.b.p, C.x.p, S);
   // upward: prolongation, post-smoothing (level 0 also reduces r.z)
   for (int l = L - 2; l >= 0; --l) {
     const AmgLevel<T>& V = *lv[l];
@@ -1033,8 +1035,8 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
         launch_packed0<kSmooth>(*pk, A0, bs, V.x.p, r, skip ? (const T*)nullptr : V.dinv.p, z0,
                                 S, rs, first, s, (T)omega0);
       else
-        k_amg_smooth_dot<T><<<bs, 256, 0, s>>>(A0, V.x.p, r, skip ? (const T*)nullptr : V.dinv.p,
-                                               z0, S, rs, first, (T)omega0);
+        launch_dep(k_amg_smooth_dot<T>, bs, 256, s, A0, (const T*)V.x.p, r,
+                   skip ? (const T*)nullptr : (const T*)V.dinv.p, z0, S, rs, first, (T)omega0);
     } else {
       amg_mv<T, kSmooth>(V.A, V.x.p, V.b.p, V.dinv.p, V.t.p, S, s);
     }

@@ -4,6 +4,7 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 
 #include "device.cuh"
@@ -24,6 +25,11 @@ int fail(int status, const char* fmt, ...) {
   return status;
 }
 void clear_error() { g_last_error.clear(); }
+
+bool pdl_enabled() {
+  const char* e = getenv("GIPB200_PDL");  // read at each launch (captured graphs keep it)
+  return e && e[0] == '1';
+}
 
 // ------------------------------------------------------------------ device info
 int device_info(DeviceInfo* out) {

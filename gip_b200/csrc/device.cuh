@@ -14,6 +14,14 @@ __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
 
+// Start of a kernel that may be launched dependent on its predecessor: wait for the
+// predecessor's completion (a no-op for an ordinary launch), then let the next kernel in
+// the stream be scheduled.
+__device__ __forceinline__ void dep_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 template <typename T>
 __device__ __forceinline__ T ld_stream(const T* p) {
   return __ldcs(p);

@@ -110,6 +110,27 @@ int one_wave(K kernel, int blocks, int* out) {
 
 int reduce_scratch_alloc(DevBuf<double>* partials, DevBuf<unsigned>* ticket, ReduceScratch* out);
 
+// ------------------------------------------------------------------ dependent launches
+// Programmatic dependent launch (GIPB200_PDL=1): a kernel of the PCG loop is scheduled
+// while its predecessor in the stream is still running, so launch latency overlaps the
+// predecessor's tail.  Every such kernel waits for its predecessor's completion
+// (griddepcontrol.wait) before its first memory access, so results are unchanged.
+bool pdl_enabled();
+template <typename... KArgs, typename... Args>
+void launch_dep(void (*kernel)(KArgs...), int grid, int block, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  (void)cudaLaunchKernelEx(&cfg, kernel, args...);  // failures surface in GIPB_LAUNCH_CHECK
+}
+
 // ------------------------------------------------------------------ sliced ELL (SELL-32)
 // Rows are grouped in slices of 32; slice s stores its rows' nonzeros column-major
 // (slot j of lane l at sptr[s] + 32*j + l), padded to the slice's longest row with

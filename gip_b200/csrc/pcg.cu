@@ -43,6 +43,7 @@ __device__ __forceinline__ void set_loop(int use, cudaGraphConditionalHandle h, 
 // iteration, also sets the loop's graph condition from the stop flag.
 __device__ __forceinline__ void mx_enter(PcgScalars* S, int use_cond,
                                          cudaGraphConditionalHandle loop_cond) {
+  dep_begin();
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     atomicAdd(&S->kernels, 1);
     set_loop(use_cond, loop_cond, !S->done);
@@ -1263,15 +1264,15 @@ int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaS
       cudaGraphConditionalHandle hu;
       GIPB_TRY(make_handle(os, 0, 0, &hu));
       launch_mx_spmv(*this, pin, pout, apin, apout, sc.p, 1, hl, os);
-      k_mx_update<<<blocks_vec, 256, 0, os>>>(n, y32.p, r32.p, pout, apout, sc.p, rs,
-                                               prm.inner_tol, prm.maxit, pin_row, scale.p, 1, hu,
-                                               amg ? 1 : 0);
+      launch_dep(k_mx_update, blocks_vec, 256, os, n, y32.p, r32.p, (const float*)pout,
+                 (const float*)apout, sc.p, rs, prm.inner_tol, prm.maxit, pin_row,
+                 (const double*)scale.p, 1, hu, amg ? 1 : 0);
       GIPB_LAUNCH_CHECK();
       cudaGraph_t if_body;
       GIPB_TRY(add_if(os, hu, &if_body));
       GIPB_CUDA(cudaStreamBeginCaptureToGraph(is, if_body, nullptr, nullptr, 0,
                                               cudaStreamCaptureModeRelaxed));
-      k_mx_apply<<<blocks_vec, 256, 0, is>>>(n, x, y32.p, scale.p, sc.p);
+      launch_dep(k_mx_apply, blocks_vec, 256, is, n, x, y32.p, (const double*)scale.p, sc.p);
       int rst = launch_mixed_residual(b, x, 0, is, 0, 0);
       cudaError_t le = cudaGetLastError();
       cudaGraph_t out = nullptr;
@@ -1337,14 +1338,15 @@ static void launch_mx_spmv(const Pcg& P, const float* pin, float* pout, const fl
   const float* r = P.amg ? P.z32.p : P.r32.p;  // direction from the preconditioned residual
   const void* ix = c.index_bits == 4 ? (const void*)c.idx4.p : (const void*)c.idx8.p;
 #define GIPB_MXP(NIB, K, REC)                                                                 \
-  k_mxp_spmv_dot<NIB, K, REC><<<nb, 256, 0, s>>>(A, c.delta.p, ix, c.base.p, c.plain.p,      \
-                                                 c.table.p, r, pin, pout, Ap, sc, P.rs,       \
-                                                 use_cond, h, Apin)
+  launch_dep(k_mxp_spmv_dot<NIB, K, REC>, nb, 256, s, A, (const uint4*)c.delta.p, ix,           \
+             (const int*)c.base.p, (const unsigned char*)c.plain.p, (const float*)c.table.p, r,  \
+             pin, pout, Ap, sc, P.rs, use_cond, h, Apin)
   if (!c.enabled) {
     if (P.rec)
-      k_mx_spmv_dot<true><<<nb, 256, 0, s>>>(A, r, pin, pout, Ap, sc, P.rs, use_cond, h, Apin);
+      launch_dep(k_mx_spmv_dot<true>, nb, 256, s, A, r, pin, pout, Ap, sc, P.rs, use_cond, h, Apin);
     else
-      k_mx_spmv_dot<false><<<nb, 256, 0, s>>>(A, r, pin, pout, Ap, sc, P.rs, use_cond, h, Apin);
+      launch_dep(k_mx_spmv_dot<false>, nb, 256, s, A, r, pin, pout, Ap, sc, P.rs, use_cond, h,
+                 Apin);
   } else if (c.index_bits == 4 && c.slots == 7) {
     if (P.rec) GIPB_MXP(4, 7, true); else GIPB_MXP(4, 7, false);
   } else if (c.index_bits == 4) {
@@ -1359,10 +1361,9 @@ static void launch_mx_spmv(const Pcg& P, const float* pin, float* pout, const fl
 
 int Pcg::launch_mixed_residual(const double* b, const double* x, int first, cudaStream_t s,
                                int use_cond, cudaGraphConditionalHandle h) {
-  k_mx_residual<<<blocks_spmv, 256, 0, s>>>(L->view(), x, b, scale.p, r32.p, p32.p, y32.p, sc.p,
-                                             rs, first, prm.tol, prm.inner_tol, prm.maxit,
-                                             prm.max_outer, pin_row, pin_val, use_cond, h,
-                                             amg ? 1 : 0);
+  launch_dep(k_mx_residual, blocks_spmv, 256, s, L->view(), (const double*)x, b,
+             (const double*)scale.p, r32.p, p32.p, y32.p, sc.p, rs, first, prm.tol, prm.inner_tol,
+             prm.maxit, prm.max_outer, pin_row, pin_val, use_cond, h, amg ? 1 : 0);
   GIPB_LAUNCH_CHECK();
   launches += 1;
   return GIPB200_OK;
@@ -1382,9 +1383,10 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
     float* apin = (rec && (k & 1)) ? Ap32b.p : Ap32.p;
     float* apout = rec ? ((k & 1) ? Ap32.p : Ap32b.p) : Ap32.p;
     launch_mx_spmv(*this, pin, pout, apin, apout, sc.p, 0, 0, s);
-    k_mx_update<<<blocks_vec, 256, 0, s>>>(n, y32.p, r32.p, pout, apout, sc.p, rs, prm.inner_tol,
-                                            prm.maxit, pin_row, scale.p, 0, 0, amg ? 1 : 0);
-    k_mx_apply<<<blocks_vec, 256, 0, s>>>(n, x, y32.p, scale.p, sc.p);
+    launch_dep(k_mx_update, blocks_vec, 256, s, n, y32.p, r32.p, (const float*)pout,
+               (const float*)apout, sc.p, rs, prm.inner_tol, prm.maxit, pin_row,
+               (const double*)scale.p, 0, (cudaGraphConditionalHandle)0, amg ? 1 : 0);
+    launch_dep(k_mx_apply, blocks_vec, 256, s, n, x, y32.p, (const double*)scale.p, sc.p);
     GIPB_LAUNCH_CHECK();
     GIPB_TRY(launch_mixed_residual(b, x, 0, s, 0, 0));
     if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s, &pk0));
