@@ -829,9 +829,10 @@ int host_hierarchy(int n, const int* rp, const int* ci, const double* v, const d
     const int na = aggregate(A, d, agg);
     if (na == 0 || na > 0.8 * A.nr)
       return fail(GIPB200_ERR_ARG, "AMG: level %d (%d unknowns) coarsens only to %d", l, A.nr, na);
-    // aggregates numbered by their first row: the coarse unknowns follow the fine order
-    // (the greedy passes number the leftover aggregates last, far from their neighbours)
-    {
+    // GIPB200_AMG_RELABEL=1: aggregates numbered by their first row instead of in the
+    // order the greedy passes create them (measured on the 256^3 cavity: 4% more FP32
+    // iterations and slower level-1 products, so off by default)
+    if (getenv("GIPB200_AMG_RELABEL")) {
       std::vector<int> first((size_t)na, A.nr);
       for (int i = 0; i < A.nr; ++i) first[agg[i]] = std::min(first[agg[i]], i);
       std::vector<int> ord((size_t)na);
@@ -911,11 +912,12 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
       // both round the same values), halving their value stream
       const bool half = std::is_same<T, float>::value;
       GIPB_TRY(upload(*H.P, &L.P, s, half));
-      if (H.l == 0 && !getenv("GIPB200_AMG_NO_AGG_ORDER")) {
-        // Level 0's residual is written in aggregate order (the rows of aggregate 0, then
-        // of aggregate 1, ..., each in row order), and the restriction reads it there: a
-        // coarse row's columns (its aggregate and the neighbours' cells) then lie close
-        // together instead of across three breadth-first levels of the fine numbering.
+      if (H.l == 0 && getenv("GIPB200_AMG_AGG_ORDER")) {
+        // GIPB200_AMG_AGG_ORDER=1: level 0's residual is written in aggregate order (the
+        // rows of aggregate 0, then of aggregate 1, ..., each in row order), and the
+        // restriction reads it there, so a coarse row's columns lie close together.
+        // Measured on the 256^3 cavity: the scattered residual writes cost 27 us and the
+        // restriction gained nothing, so off by default.
         const std::vector<int>& agg = *H.agg;
         std::vector<int> start((size_t)H.R->nr + 1, 0);
         for (int a : agg) start[(size_t)a + 1]++;
@@ -987,7 +989,7 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     const double n = V.n, nn = lv[l + 1]->n;
     const bool skip = l == 0 && u0;
     // levels >= 1 gather D^-1 b where they would gather the Jacobi start x = D^-1 b
-    const bool fold = l > 0;
+    const bool fold = l > 0 && fold_coarse;
     if (!skip && !fold) {
       GIPB_TRY(mark(l, GIPB200_CYCLE_JACOBI0, 3.0 * n * w));
       launch_dep(k_amg_jacobi0<T>, vec_blocks(V.n), 256, s, V.n, (const T*)V.dinv.p, b, V.x.p, S);
@@ -1019,7 +1021,7 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     const T* xc = (l + 1 == L - 1) ? lv[l + 1]->x.p : lv[l + 1]->t.p;
     const double n = V.n, nn = lv[l + 1]->n;
     const bool skip = l == 0 && u0;
-    const bool fold = l > 0;
+    const bool fold = l > 0 && fold_coarse;
     GIPB_TRY(mark(l, GIPB200_CYCLE_PROLONG,
                   stream_bytes(V.P) + (nn + (fold ? 3.0 : 2.0) * n) * w));
     if (skip)  // x0 = omega0 r + P x1
@@ -1056,7 +1058,7 @@ double AmgT<T>::cycle_bytes(double a0_stream_bytes) const {
     const double n = V.n, nn = lv[l + 1]->n;
     const double a = l == 0 ? a0_stream_bytes : stream_bytes(V.A);
     const bool skip = l == 0 && unit0;                   // x0 = omega0 r not formed
-    const bool fold = l > 0;                             // x = D^-1 b formed where gathered
+    const bool fold = l > 0 && fold_coarse;              // x = D^-1 b formed where gathered
     if (!skip && !fold) b += 3.0 * n * w;                // x = dinv b
     b += a + (skip ? 2.0 : 3.0) * n * w;                 // t = b - A x
     if (l == 0 && perm0.p) b += 4.0 * n;                 // its aggregate-order positions

@@ -2,6 +2,8 @@
 // the mixed form's inner CG (an addition beyond GIP, whose solver is Jacobi-PCG).
 #pragma once
 
+#include <cstdlib>
+
 #include <cuda_fp16.h>
 
 #include <memory>
@@ -80,6 +82,9 @@ struct AmgT {
   // gathers r and scales the product) and reads no diagonal.  A fixed symmetric smoother
   // like the per-row one, so the cycle stays a symmetric positive definite operator.
   bool unit0 = false;
+  // levels >= 1 fold their Jacobi start x = D^-1 b into the kernels that gather it
+  // (GIPB200_AMG_NO_FOLD=1: a separate kernel forms it)
+  bool fold_coarse = getenv("GIPB200_AMG_NO_FOLD") == nullptr;
   double omega0 = 0.0;
   // Level 0's residual position in aggregate order (empty: written in row order); the
   // level-0 restriction's columns are numbered in that order.

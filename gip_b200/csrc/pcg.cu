@@ -791,7 +791,9 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
     GIPB_TRY(Ap32.alloc(n));
     GIPB_TRY(Ap32.zero(s));
     // the product recurrence on the AMG path (beta small): its second product buffer
-    rec = prm.precond == GIPB200_PRECOND_AMG && !getenv("GIPB200_NO_AP_RECURRENCE");
+    // (GIPB200_AP_RECURRENCE=1; measured on the 256^3 cavity it saves no time: the
+    // kernel is bound by latency, not by its second gather)
+    rec = prm.precond == GIPB200_PRECOND_AMG && getenv("GIPB200_AP_RECURRENCE") != nullptr;
     if (rec) {
       GIPB_TRY(Ap32b.alloc(n));
       GIPB_TRY(Ap32b.zero(s));

@@ -9,8 +9,8 @@ library applies it, step by step, so the tests can compare level sizes and nonze
 * aggregation, three greedy passes over the rows in order: (1) a row whose strong
   neighbours are all free starts an aggregate with them; (2) a free row joins the aggregate
   (from pass 1) of its strongest neighbour, the first in stored order on ties; (3) each row
-  still free starts an aggregate with its free neighbours; the aggregates are then
-  numbered by their first row;
+  still free starts an aggregate with its free neighbours; aggregates are numbered in the
+  order the passes create them;
 * tentative prolongator P0[i, agg(i)] = z_i / |z over agg(i)|, smoothed by one weighted
   Jacobi step, P = (I - w D^-1 A) P0 with w = 4 / (3 rho), rho the Gershgorin bound of
   D^-1 A; coarse near-null vector = the aggregate norms;
@@ -66,12 +66,7 @@ def aggregate(A: sp.csr_matrix):
             if agg[ci[k]] == -1:
                 agg[ci[k]] = na
         na += 1
-    # aggregates renumbered by their first row (coarse unknowns follow the fine order)
-    first = np.full(na, n, np.int64)
-    np.minimum.at(first, agg, np.arange(n))
-    relabel = np.empty(na, np.int64)
-    relabel[np.argsort(first, kind="stable")] = np.arange(na)
-    return relabel[agg], na
+    return agg, na
 
 
 def prolongator(A: sp.csr_matrix, d, agg, p0, na: int, w: float) -> sp.csr_matrix:
