@@ -825,8 +825,10 @@ int host_hierarchy(int n, const int* rp, const int* ci, const double* v, const d
       H.cinv = &inv;
       return emit(H);
     }
+    setup_mark("AMG level: diagonal, bound");
     std::vector<int> agg;
     const int na = aggregate(A, d, agg);
+    setup_mark("AMG level: aggregation");
     if (na == 0 || na > 0.8 * A.nr)
       return fail(GIPB200_ERR_ARG, "AMG: level %d (%d unknowns) coarsens only to %d", l, A.nr, na);
     // GIPB200_AMG_RELABEL=1: aggregates numbered by their first row instead of in the
@@ -849,14 +851,18 @@ int host_hierarchy(int n, const int* rp, const int* ci, const double* v, const d
     for (int i = 0; i < A.nr; ++i) p0[i] = nrm[agg[i]] > 0.0 ? z[i] / nrm[agg[i]] : 0.0;
     HCsr P = smoothed_prolongator(A, d, agg, p0, na, H.w);
     HCsr R = transpose(P);
+    setup_mark("AMG level: prolongator");
     HCsr AP, Ac;
     GIPB_TRY(spgemm(A, P, AP));
     GIPB_TRY(spgemm(R, AP, Ac));
+    setup_mark("AMG level: Galerkin product");
     if (drop > 0.0) sparsify(Ac, nrm, drop);
+    setup_mark("AMG level: sparsification");
     H.P = &P;
     H.R = &R;
     H.agg = &agg;
     GIPB_TRY(emit(H));
+    setup_mark("AMG level: device upload");
     A = std::move(Ac);
     z = std::move(nrm);
   }

@@ -4,6 +4,7 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdlib>
 #include <mutex>
 
@@ -25,6 +26,15 @@ int fail(int status, const char* fmt, ...) {
   return status;
 }
 void clear_error() { g_last_error.clear(); }
+
+void setup_mark(const char* what) {
+  static thread_local std::chrono::steady_clock::time_point last = std::chrono::steady_clock::now();
+  if (!getenv("GIPB200_SETUP_TRACE")) return;
+  const auto now = std::chrono::steady_clock::now();
+  fprintf(stderr, "gipb200 setup: %-28s %8.3f s\n", what,
+          std::chrono::duration<double>(now - last).count());
+  last = now;
+}
 
 bool pdl_enabled() {
   const char* e = getenv("GIPB200_PDL");  // read at each launch (captured graphs keep it)

@@ -772,7 +772,10 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
   auto since = [](std::chrono::steady_clock::time_point t) {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
   };
+  auto trace = [](const char* what) { setup_mark(what); };
+  trace("start");
   GIPB_TRY(check_dns_ops(ops));
+  trace("operator checks");
   if (prm->pcg.mode < 0 || prm->pcg.mode > 2) return fail(GIPB200_ERR_ARG, "bad PCG mode");
   const int N = ops->n_inner, NO = ops->n_owned, NF = ops->n_faces;
     E.N = N;
@@ -796,22 +799,26 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     const double *pu = h_u, *pv = h_v, *pw = h_w, *pdx = h_dxs;
     if (can_reorder) {
       std::vector<int> inv_c = bfs_cells(ops->L, N);  // new -> old (inner)
+      trace("breadth-first cells");
       inv_c.resize(NO);
       for (int g = N; g < NO; ++g) inv_c[g] = g;
       std::vector<int> perm_c(NO);
       for (int r = 0; r < NO; ++r) perm_c[inv_c[r]] = r;
-      // faces ordered by the first (renumbered) inner cell that has them
-      std::vector<long long> key(NF);
-      for (int f = 0; f < NF; ++f) key[f] = (long long)NO * NF + f;
+      // faces ordered by the first (renumbered) inner cell that has them, then by face
+      // index (faces of no inner cell last): a counting sort on that cell, filled in face
+      // order
+      std::vector<int> first_cell(NF, NO);
       for (int i = 0; i < ops->Mres.nrows; ++i)
         for (int k = ops->Mres.rowptr[i]; k < ops->Mres.rowptr[i + 1]; ++k) {
           const int f = ops->Mres.col[k];
-          const long long kk = (long long)perm_c[i] * NF + f;
-          if (kk < key[f]) key[f] = kk;
+          first_cell[f] = std::min(first_cell[f], perm_c[i]);
         }
+      std::vector<int> bucket((size_t)NO + 2, 0);
+      for (int f = 0; f < NF; ++f) bucket[(size_t)first_cell[f] + 1]++;
+      for (int c = 0; c <= NO; ++c) bucket[(size_t)c + 1] += bucket[c];
       std::vector<int> inv_f(NF);
-      for (int f = 0; f < NF; ++f) inv_f[f] = f;
-      std::sort(inv_f.begin(), inv_f.end(), [&](int a, int b) { return key[a] < key[b]; });
+      for (int f = 0; f < NF; ++f) inv_f[bucket[first_cell[f]]++] = f;
+      trace("face order");
       std::vector<int> perm_f(NF);
       for (int r = 0; r < NF; ++r) perm_f[inv_f[r]] = r;
       auto cell_op = [&](const gipb200_host_csr& m, OwnedCsr* o, bool face_cols) {
@@ -840,6 +847,7 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
       for (int r = 0; r < N; ++r)
         for (int k = ops->D.rowptr[inv_c[r]]; k < ops->D.rowptr[inv_c[r] + 1]; ++k) ec_src.push_back(k);
       permute_rows(ops->Ec, ec_src.data(), perm_f.data(), &own[14]);
+      trace("operators renumbered");
       rops.D = own[0].view();
       rops.L = own[1].view();
       rops.Lb = own[2].view();
@@ -878,24 +886,39 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     const auto t_ops = std::chrono::steady_clock::now();
     const gipb200_dns_ops* bops = &rops;
     GIPB_TRY(build_op(&E.D, bops->D));
+    trace("sliced D");
     // Ec is only ever read row by row in CSR form (C's values, the adjoint's convective
     // term): no sliced copy
     GIPB_TRY(csr_build(&E.Ec, bops->Ec.nrows, bops->Ec.ncols, bops->Ec.nnz, bops->Ec.rowptr,
                        bops->Ec.col, bops->Ec.val, 0));
     GIPB_TRY(build_op(&E.L, bops->L));
+    trace("sliced L");
     GIPB_TRY(build_op(&E.Lb, bops->Lb));
+    trace("sliced Lb");
     GIPB_TRY(build_op(&E.Mx, bops->Mx));
+    trace("sliced Mx");
     GIPB_TRY(build_op(&E.My, bops->My));
+    trace("sliced My");
     GIPB_TRY(build_op(&E.Mz, bops->Mz));
+    trace("sliced Mz");
     GIPB_TRY(build_op(&E.Mres, bops->Mres));
+    trace("sliced Mres");
     GIPB_TRY(build_op(&E.Gx, bops->Gx));
+    trace("sliced Gx");
     GIPB_TRY(build_op(&E.Gy, bops->Gy));
+    trace("sliced Gy");
     GIPB_TRY(build_op(&E.Gz, bops->Gz));
+    trace("sliced Gz");
     GIPB_TRY(build_op(&E.SFx, bops->SFx));
+    trace("sliced SFx");
     GIPB_TRY(build_op(&E.SFy, bops->SFy));
+    trace("sliced SFy");
     GIPB_TRY(build_op(&E.SFz, bops->SFz));
+    trace("sliced SFz");
     GIPB_TRY(build_op(&E.SO, bops->SO));
+    trace("sliced SO");
     GIPB_TRY(build_ec_slot(E, bops->D, bops->Ec));
+    trace("Ec in C's slot order");
     {
       const gipb200_host_csr* sf[3] = {&bops->SFx, &bops->SFy, &bops->SFz};
       GIPB_TRY(build_face3(&E.SF3, sf, NF, NO));
@@ -923,9 +946,11 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     GIPB_CUDA(cudaMemcpy(E.v.p, pv, (size_t)NO * 8, cudaMemcpyHostToDevice));
     GIPB_CUDA(cudaMemcpy(E.w.p, pw, (size_t)NO * 8, cudaMemcpyHostToDevice));
     GIPB_CUDA(cudaMemcpy(E.dxs.p, pdx, (size_t)NO * 8, cudaMemcpyHostToDevice));
+    trace("merged faces, fields");
     E.setup_s[1] = since(t_ops);  // device layouts of the operators, fields
     const auto t_pcg = std::chrono::steady_clock::now();
     GIPB_TRY(E.pcg.init(&E.L, NO, prm->pcg, 0));
+    trace("pressure solver");
     E.setup_s[2] = since(t_pcg);  // the pressure solver (FP32 operator, packing, AMG)
     GIPB_TRY(E.sc.alloc(1));
     GIPB_TRY(E.sc.zero());

@@ -110,6 +110,11 @@ int one_wave(K kernel, int blocks, int* out) {
 
 int reduce_scratch_alloc(DevBuf<double>* partials, DevBuf<unsigned>* ticket, ReduceScratch* out);
 
+// ------------------------------------------------------------------ setup trace
+// GIPB200_SETUP_TRACE=1: prints `what` with the wall time since the previous mark (and
+// restarts the clock) on stderr; otherwise does nothing.
+void setup_mark(const char* what);
+
 // ------------------------------------------------------------------ dependent launches
 // Programmatic dependent launch (GIPB200_PDL=1): a kernel of the PCG loop is scheduled
 // while its predecessor in the stream is still running, so launch latency overlaps the

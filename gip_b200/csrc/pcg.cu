@@ -805,6 +805,7 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
       GIPB_TRY(grid_blocks(256, n, 1, 0, &b));
       k_mx_scale<<<b, 256, 0, s>>>(n, L->rowptr.p, L->csr_col.p, L->csr_val.p, scale.p);
       GIPB_LAUNCH_CHECK();
+      setup_mark("solver buffers, scale");
       // pinned-Neumann detection on the host copy of L
       {
         std::vector<double> hval((size_t)std::max(L->nnz, 1));
@@ -830,10 +831,14 @@ int Pcg::init(const Sell* Lm, int nall, const gipb200_pcg_params& params, cudaSt
           pin_val = pval;
         }
       }
+      setup_mark("pinned-Neumann detection");
       k_mx_lhat<<<blocks_spmv, 256, 0, s>>>(L->view(), scale.p, n, pin_row, pin_val, lhat.p);
       GIPB_LAUNCH_CHECK();
       GIPB_TRY(sort_fp32_rows(s));
+      GIPB_CUDA(cudaStreamSynchronize(s));
+      setup_mark("FP32 operator");
       if (prm.mode == GIPB200_PCG_MIXED && !getenv("GIPB200_NO_COMPRESS")) GIPB_TRY(build_compressed(s));
+      setup_mark("packed FP32 operator");
       if (prm.precond == GIPB200_PRECOND_AMG) GIPB_TRY(build_amg(s));
     }
   } else {
@@ -882,6 +887,7 @@ int Pcg::build_amg(cudaStream_t s) {
   }
   std::vector<double> z((size_t)n);
   for (int i = 0; i < n; ++i) z[i] = hs[i] > 0.0 ? 1.0 / hs[i] : 0.0;
+  setup_mark("AMG: scaled operator on host");
   amg.reset(new Amg());
   GIPB_TRY(amg->build(n, rp.data(), ci.data(), v.data(), z.data(), pin_row >= 0, n, s));
   GIPB_TRY(z32.alloc((size_t)n_all));
