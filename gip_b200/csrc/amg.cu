@@ -353,8 +353,8 @@ bool dense_inverse(int m, std::vector<double>& M, std::vector<double>& inv) {
   return true;
 }
 
-// compact: a long-row (CSR) operator whose column offsets from the row all fit in int16 is
-// stored with 16-bit offsets and FP16 values (the FP32 cycle's coarse operators).
+// compact: a long-row (CSR) operator whose rows each span at most 65536 columns is stored
+// with 16-bit offsets from each row's smallest column (the FP32 cycle); half: FP16 values.
 template <typename T>
 int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool compact = false) {
   S->half = half;
@@ -368,16 +368,20 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool c
     S->lanes = avg >= 48.0 ? 32 : avg >= 24.0 ? 16 : 8;
     GIPB_TRY(S->rp.upload(A.rp.data(), A.rp.size(), s));
     bool fits = compact && std::is_same<T, float>::value;
-    for (int r = 0; r < A.nr && fits; ++r)
-      for (int k = A.rp[r]; k < A.rp[r + 1] && fits; ++k)
-        fits = std::abs(A.ci[k] - r) <= 32767;
+    std::vector<int> cb((size_t)std::max(A.nr, 1), 0);
+    for (int r = 0; r < A.nr && fits; ++r) {
+      int lo = A.nc, hi = -1;
+      for (int k = A.rp[r]; k < A.rp[r + 1]; ++k) lo = std::min(lo, A.ci[k]), hi = std::max(hi, A.ci[k]);
+      cb[r] = hi >= 0 ? lo : 0;
+      fits = hi < 0 || hi - lo <= 65535;
+    }
     if (fits) {
       S->short_cols = true;
-      S->half = half = true;
-      std::vector<short> dc(std::max<size_t>(A.ci.size(), 1), 0);
+      std::vector<unsigned short> dc(std::max<size_t>(A.ci.size(), 1), 0);
       for (int r = 0; r < A.nr; ++r)
-        for (int k = A.rp[r]; k < A.rp[r + 1]; ++k) dc[k] = (short)(A.ci[k] - r);
+        for (int k = A.rp[r]; k < A.rp[r + 1]; ++k) dc[k] = (unsigned short)(A.ci[k] - cb[r]);
       GIPB_TRY(S->dcol.upload(dc.data(), dc.size(), s));
+      GIPB_TRY(S->cbase.upload(cb.data(), cb.size(), s));
     } else {
       GIPB_TRY(S->col.upload(A.ci.data(), std::max<size_t>(A.ci.size(), 1), s));
     }
@@ -536,24 +540,32 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
                                                  const V* __restrict__ val, const T* __restrict__ x,
                                                  const T* __restrict__ b,
                                                  const T* __restrict__ dinv, T* __restrict__ y,
-                                                 PcgScalars* S, T w, const T* __restrict__ xs) {
+                                                 PcgScalars* S, T w, const T* __restrict__ xs,
+                                                 const int* __restrict__ cbase) {
   if (amg_enter(S)) return;
   constexpr int RPW = 32 / LANES;  // rows per warp per pass
   constexpr int U = 4;             // entries a lane loads before their gathers
   const int lane = threadIdx.x & 31, sub = lane % LANES;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
+  constexpr bool kShort = sizeof(CI) == 2;  // 16-bit offsets from each row's base column
   int r0 = gw * RPW;
-  int kb = 0, ke = 0;
+  int kb = 0, ke = 0, cb = 0;
   {
     const int i = r0 + lane / LANES;
-    if (i < nrows) kb = __ldg(rp + i), ke = __ldg(rp + i + 1);
+    if (i < nrows) {
+      kb = __ldg(rp + i), ke = __ldg(rp + i + 1);
+      if (kShort) cb = __ldg(cbase + i);
+    }
   }
   for (; r0 < nrows; r0 += nw * RPW) {
     const int i = r0 + lane / LANES;
-    int kbn = 0, ken = 0;  // the next pass's row, loaded ahead
+    int kbn = 0, ken = 0, cbn = 0;  // the next pass's row, loaded ahead
     const int in = i + nw * RPW;
-    if (in < nrows) kbn = __ldg(rp + in), ken = __ldg(rp + in + 1);
+    if (in < nrows) {
+      kbn = __ldg(rp + in), ken = __ldg(rp + in + 1);
+      if (kShort) cbn = __ldg(cbase + in);
+    }
     T sum = T(0);
     for (int k0 = kb + sub; k0 < ke; k0 += U * LANES) {
       int c[U];
@@ -561,9 +573,7 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int k = k0 + u * LANES;
-        // 16-bit columns are offsets from the row
-        c[u] = (k < ke) ? (sizeof(CI) == 2 ? i + (int)ld_stream(col + k) : (int)ld_stream(col + k))
-                        : -1;
+        c[u] = (k < ke) ? (kShort ? cb + (int)ld_stream(col + k) : (int)ld_stream(col + k)) : -1;
         v[u] = (k < ke) ? ld_stream(val + k) : V(0);
       }
       T xv[U];
@@ -587,6 +597,7 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
     }
     kb = kbn;
     ke = ken;
+    cb = cbn;
   }
 }
 
@@ -603,12 +614,13 @@ void amg_mv_v(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const
   }
   const int nb = vec_blocks((int)std::min<long long>((long long)M.nrows * M.lanes, 1LL << 30));
   const int* rp = M.rp.p;
-#define GIPB_CSR(L, CI, COLS) \
-  launch_dep(k_amg_csr<T, MODE, L, V, CI>, nb, 256, s, M.nrows, rp, COLS, v, x, b, dinv, y, S, w, xs)
+#define GIPB_CSR(L, CI, COLS)                                                                    \
+  launch_dep(k_amg_csr<T, MODE, L, V, CI>, nb, 256, s, M.nrows, rp, (const CI*)COLS, v, x, b, dinv, \
+             y, S, w, xs, (const int*)M.cbase.p)
   if (M.short_cols) {
-    if (M.lanes == 32) GIPB_CSR(32, short, M.dcol.p);
-    else if (M.lanes == 16) GIPB_CSR(16, short, M.dcol.p);
-    else GIPB_CSR(8, short, M.dcol.p);
+    if (M.lanes == 32) GIPB_CSR(32, unsigned short, M.dcol.p);
+    else if (M.lanes == 16) GIPB_CSR(16, unsigned short, M.dcol.p);
+    else GIPB_CSR(8, unsigned short, M.dcol.p);
   } else {
     if (M.lanes == 32) GIPB_CSR(32, int, M.col.p);
     else if (M.lanes == 16) GIPB_CSR(16, int, M.col.p);
@@ -906,7 +918,9 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
     if (H.l > 0) {  // level 0 runs on the solver's own operator
       GIPB_TRY(L.b.alloc((size_t)A.nr));
       // the FP32 cycle stores its long-row coarse operators compactly where they fit
-      GIPB_TRY(upload(A, &L.A, s, false, !getenv("GIPB200_AMG_WIDE")));
+      // (GIPB200_AMG_COARSE_HALF=1: their values in FP16 as well)
+      GIPB_TRY(upload(A, &L.A, s, std::is_same<T, float>::value && getenv("GIPB200_AMG_COARSE_HALF"),
+                      !getenv("GIPB200_AMG_WIDE")));
     }
     nnz_all += (double)A.nnz();
     if (H.cinv) {
@@ -917,7 +931,8 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
       // the FP32 cycle keeps its transfer operators in FP16 (R = P^T still holds exactly:
       // both round the same values), halving their value stream
       const bool half = std::is_same<T, float>::value;
-      GIPB_TRY(upload(*H.P, &L.P, s, half));
+      const bool compact = !getenv("GIPB200_AMG_WIDE");
+      GIPB_TRY(upload(*H.P, &L.P, s, half, compact));
       if (H.l == 0 && getenv("GIPB200_AMG_AGG_ORDER")) {
         // GIPB200_AMG_AGG_ORDER=1: level 0's residual is written in aggregate order (the
         // rows of aggregate 0, then of aggregate 1, ..., each in row order), and the
@@ -940,10 +955,10 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
             Rp.v[k] = e[k - Rp.rp[j]].second;
           }
         }
-        GIPB_TRY(upload(Rp, &L.R, s, half));
+        GIPB_TRY(upload(Rp, &L.R, s, half, compact));
         GIPB_TRY(perm0.upload(perm.data(), perm.size(), s));
       } else {
-        GIPB_TRY(upload(*H.R, &L.R, s, half));
+        GIPB_TRY(upload(*H.R, &L.R, s, half, compact));
       }
     }
     lv.push_back(std::move(Lp));

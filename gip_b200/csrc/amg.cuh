@@ -29,9 +29,11 @@ struct SellT {
   DevBuf<int> rp;
   bool half = false;           // values stored in FP16 (hval) instead of T (val)
   DevBuf<__half> hval;
-  // CSR form with 16-bit columns: column = row + dcol[k] (every offset fits in int16)
+  // CSR form with 16-bit columns: column = cbase[row] + dcol[k], cbase the row's smallest
+  // column (every row's columns span at most 65536)
   bool short_cols = false;
-  DevBuf<short> dcol;
+  DevBuf<unsigned short> dcol;
+  DevBuf<int> cbase;
   SellView<T> view() const { return {nrows, nslices, sptr.p, col.p, val.p}; }
   SellView<__half> hview() const { return {nrows, nslices, sptr.p, col.p, hval.p}; }
 };
@@ -113,7 +115,9 @@ struct AmgT {
 template <typename T>
 double stream_bytes(const SellT<T>& M) {
   const double w = M.half ? 2.0 : (double)sizeof(T);
-  if (M.lanes > 0) return (double)M.nnz * ((M.short_cols ? 2.0 : 4.0) + w) + (M.nrows + 1.0) * 4.0;
+  if (M.lanes > 0)
+    return (double)M.nnz * ((M.short_cols ? 2.0 : 4.0) + w) + (M.nrows + 1.0) * 4.0 +
+           (M.short_cols ? 4.0 * M.nrows : 0.0);
   return (double)M.nslots * (4.0 + w) + (M.nslices + 1.0) * 8.0;
 }
 
