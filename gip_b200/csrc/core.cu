@@ -102,7 +102,7 @@ int validate_csr(int nrows, int ncols, int nnz, const int* rowptr, const int* co
 
 // ------------------------------------------------------------------ SELL-32 build
 int sell_build(Sell* S, int nrows, int ncols, int nnz, const int* rp, const int* col,
-               const double* val, cudaStream_t stream) {
+               const double* val, cudaStream_t stream, unsigned keep) {
   // every gather must stay inside an x of ncols entries
   GIPB_TRY(validate_csr(nrows, ncols, nnz, rp, col, ncols, "matrix"));
   S->nrows = nrows;
@@ -123,7 +123,10 @@ int sell_build(Sell* S, int nrows, int ncols, int nnz, const int* rp, const int*
   S->nslots = sptr[S->nslices];
   std::vector<int> scol((size_t)std::max<long long>(S->nslots, 1), -1);
   std::vector<double> sval((size_t)std::max<long long>(S->nslots, 1), 0.0);
-  std::vector<int> pos((size_t)std::max(nnz, 1), 0);
+  if (S->nslots > 0x7fffffffLL)
+    return fail(GIPB200_ERR_ARG, "matrix too large for 32-bit slot indices");
+  const bool want_pos = (keep & kKeepPos) != 0;
+  std::vector<int> pos(want_pos ? (size_t)std::max(nnz, 1) : 0, 0);
 #pragma omp parallel for schedule(static)
   for (int r = 0; r < nrows; ++r) {
     int s = r >> 5, lane = r & 31;
@@ -131,25 +134,27 @@ int sell_build(Sell* S, int nrows, int ncols, int nnz, const int* rp, const int*
       long long slot = sptr[s] + 32LL * (k - rp[r]) + lane;
       scol[slot] = col[k];
       sval[slot] = val ? val[k] : 0.0;
-      pos[k] = (int)slot;
+      if (want_pos) pos[k] = (int)slot;
     }
   }
-  if (S->nslots > 0x7fffffffLL)
-    return fail(GIPB200_ERR_ARG, "matrix too large for 32-bit slot indices");
   GIPB_TRY(S->sptr.upload(sptr.data(), sptr.size(), stream));
   GIPB_TRY(S->col.upload(scol.data(), scol.size(), stream));
   GIPB_TRY(S->val.upload(sval.data(), sval.size(), stream));
-  GIPB_TRY(S->pos.upload(pos.data(), pos.size(), stream));
-  GIPB_TRY(S->rowptr.upload(rp, (size_t)nrows + 1, stream));
-  GIPB_TRY(S->csr_col.upload(col, (size_t)std::max(nnz, 1), stream));
-  if (val) {
-    GIPB_TRY(S->csr_val.upload(val, (size_t)std::max(nnz, 1), stream));
-  } else {
-    GIPB_TRY(S->csr_val.alloc((size_t)std::max(nnz, 1)));
-    GIPB_TRY(S->csr_val.zero(stream));
+  if (want_pos) GIPB_TRY(S->pos.upload(pos.data(), pos.size(), stream));
+  if (keep & kKeepDeviceCsr) {
+    GIPB_TRY(S->rowptr.upload(rp, (size_t)nrows + 1, stream));
+    GIPB_TRY(S->csr_col.upload(col, (size_t)std::max(nnz, 1), stream));
+    if (val) {
+      GIPB_TRY(S->csr_val.upload(val, (size_t)std::max(nnz, 1), stream));
+    } else {
+      GIPB_TRY(S->csr_val.alloc((size_t)std::max(nnz, 1)));
+      GIPB_TRY(S->csr_val.zero(stream));
+    }
   }
-  S->h_rowptr.assign(rp, rp + nrows + 1);
-  S->h_col.assign(col, col + nnz);
+  if (keep & kKeepHost) {
+    S->h_rowptr.assign(rp, rp + nrows + 1);
+    S->h_col.assign(col, col + nnz);
+  }
   GIPB_CUDA(cudaStreamSynchronize(stream));  // host staging vectors go out of scope
   return GIPB200_OK;
 }

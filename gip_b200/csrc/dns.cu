@@ -556,8 +556,9 @@ void Dns::phase_bytes(double out[7]) const {
   out[2] = 0.0;                                                      // PCG
   out[3] = 16.0 * no + op(Lb) + 24.0 * Lb.nnz;                       // p0/p copies, ghosts
   out[4] = op(Gx) + op(Gy) + op(Gz) + 8.0 * no + 24.0 * no + 48.0 * n;  // gp, u -= gp
-  out[5] = op(SO) + op(SFx) + op(SFy) + op(SFz) + 56.0 * no + 16.0 * nf +  // mf
-           (SF3.on ? 2.0 * nf : 0.0);                                        // face counts
+  out[5] = op(SO) + (SF3.on ? op(SF3.S) + 2.0 * nf   // merged faces and their counts
+                             : op(SFx) + op(SFy) + op(SFz)) +
+           56.0 * no + 16.0 * nf;  // mf
   out[6] = op(Mres) + 8.0 * nf + 8.0 * n + 32.0 * n;                 // massr, CFL
 }
 
@@ -666,8 +667,18 @@ static int check_op(const gipb200_host_csr& m, const char* name, int rows_max, i
   return validate_csr(m.nrows, m.ncols, m.nnz, m.rowptr, m.col, col_bound, name);
 }
 
-static int build_op(Sell* S, const gipb200_host_csr& m) {
-  return sell_build(S, m.nrows, m.ncols, m.nnz, m.rowptr, m.col, m.val, 0);
+// The engine's sliced operators keep only what it reads: D its CSR columns and slot map
+// (C's values, the adjoint), L everything (the solver's set-up), the others nothing.
+static int build_op(Sell* S, const gipb200_host_csr& m, unsigned keep = 0) {
+  return sell_build(S, m.nrows, m.ncols, m.nnz, m.rowptr, m.col, m.val, 0, keep);
+}
+
+// Sizes of an operator whose sliced layout is never read (phase byte counts only).
+static void op_sizes(Sell* S, const gipb200_host_csr& m) {
+  S->nrows = m.nrows;
+  S->ncols = m.ncols;
+  S->nnz = m.nnz;
+  S->nslices = (m.nrows + 31) / 32;
 }
 
 // Ec in D's slot order (Dns::ec_slot): slot t of D's sliced layout holds the nonzero k of
@@ -734,7 +745,7 @@ static int build_face3(FaceOps3* F, const gipb200_host_csr* const op[3], int NF,
     cnt[f] = (unsigned short)packed;
     rp[f + 1] = (int)col.size();
   }
-  GIPB_TRY(sell_build(&F->S, NF, NO, (int)col.size(), rp.data(), col.data(), val.data(), 0));
+  GIPB_TRY(sell_build(&F->S, NF, NO, (int)col.size(), rp.data(), col.data(), val.data(), 0, 0u));
   GIPB_TRY(F->cnt.upload(cnt.data(), cnt.size(), 0));
   GIPB_CUDA(cudaStreamSynchronize(0));
   F->on = true;
@@ -885,13 +896,13 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     E.setup_s[0] = since(t_begin);  // checks and renumbering
     const auto t_ops = std::chrono::steady_clock::now();
     const gipb200_dns_ops* bops = &rops;
-    GIPB_TRY(build_op(&E.D, bops->D));
+    GIPB_TRY(build_op(&E.D, bops->D, kKeepDeviceCsr | kKeepPos));
     trace("sliced D");
     // Ec is only ever read row by row in CSR form (C's values, the adjoint's convective
     // term): no sliced copy
     GIPB_TRY(csr_build(&E.Ec, bops->Ec.nrows, bops->Ec.ncols, bops->Ec.nnz, bops->Ec.rowptr,
                        bops->Ec.col, bops->Ec.val, 0));
-    GIPB_TRY(build_op(&E.L, bops->L));
+    GIPB_TRY(build_op(&E.L, bops->L, kKeepAll));
     trace("sliced L");
     GIPB_TRY(build_op(&E.Lb, bops->Lb));
     trace("sliced Lb");
@@ -909,28 +920,25 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     trace("sliced Gy");
     GIPB_TRY(build_op(&E.Gz, bops->Gz));
     trace("sliced Gz");
-    GIPB_TRY(build_op(&E.SFx, bops->SFx));
-    trace("sliced SFx");
-    GIPB_TRY(build_op(&E.SFy, bops->SFy));
-    trace("sliced SFy");
-    GIPB_TRY(build_op(&E.SFz, bops->SFz));
-    trace("sliced SFz");
+    {
+      // SFx, SFy, SFz merged per face where they fit; their own layouts only otherwise
+      const gipb200_host_csr* sf[3] = {&bops->SFx, &bops->SFy, &bops->SFz};
+      GIPB_TRY(build_face3(&E.SF3, sf, NF, NO));
+      if (E.SF3.on) {
+        op_sizes(&E.SFx, bops->SFx);
+        op_sizes(&E.SFy, bops->SFy);
+        op_sizes(&E.SFz, bops->SFz);
+      } else {
+        GIPB_TRY(build_op(&E.SFx, bops->SFx));
+        GIPB_TRY(build_op(&E.SFy, bops->SFy));
+        GIPB_TRY(build_op(&E.SFz, bops->SFz));
+      }
+    }
+    trace("face operators");
     GIPB_TRY(build_op(&E.SO, bops->SO));
     trace("sliced SO");
     GIPB_TRY(build_ec_slot(E, bops->D, bops->Ec));
     trace("Ec in C's slot order");
-    {
-      const gipb200_host_csr* sf[3] = {&bops->SFx, &bops->SFy, &bops->SFz};
-      GIPB_TRY(build_face3(&E.SF3, sf, NF, NO));
-      if (E.SF3.on)  // the separate sliced copies are no longer read on the device
-        for (Sell* S : {&E.SFx, &E.SFy, &E.SFz}) {
-          S->col.release();
-          S->val.release();
-          S->pos.release();
-          S->csr_col.release();
-          S->csr_val.release();
-        }
-    }
     // C starts with D's values (C.postConstruct reads the D file, GIP_DNS.h:151)
     GIPB_TRY(E.cval.alloc((size_t)std::max<long long>(E.D.nslots, 1)));
     GIPB_CUDA(cudaMemcpy(E.cval.p, E.D.val.p, E.cval.n * 8, cudaMemcpyDeviceToDevice));

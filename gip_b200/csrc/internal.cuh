@@ -168,9 +168,12 @@ struct Sell {
   SellView<float> view32() const { return {nrows, nslices, sptr.p, col.p, val32.p}; }
 };
 
-// Builds SELL-32 (and keeps a device CSR copy) from host CSR arrays.
+// Builds SELL-32 from host CSR arrays, keeping what `keep` asks for: a device CSR copy
+// (rowptr, csr_col, csr_val), the CSR -> slot position map (pos) and the host CSR structure
+// (h_rowptr, h_col).
+enum : unsigned { kKeepDeviceCsr = 1u, kKeepPos = 2u, kKeepHost = 4u, kKeepAll = 7u };
 int sell_build(Sell* S, int nrows, int ncols, int nnz, const int* h_rowptr, const int* h_col,
-               const double* h_val, cudaStream_t stream);
+               const double* h_val, cudaStream_t stream, unsigned keep = kKeepAll);
 // Only the device CSR copy (operators read row by row, never sliced).
 int csr_build(Sell* S, int nrows, int ncols, int nnz, const int* h_rowptr, const int* h_col,
               const double* h_val, cudaStream_t stream);
