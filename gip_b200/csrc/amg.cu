@@ -405,19 +405,40 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool c
   }
   S->nslots = sptr[S->nslices];
   if (S->nslots > 0x7fffffffLL) return fail(GIPB200_ERR_ARG, "AMG operator too large");
-  std::vector<int> col((size_t)std::max<long long>(S->nslots, 1), -1);
+  // compact: 16-bit slot columns from a per-row base (0xffff marks padding) when every
+  // row spans at most 65535 columns
+  bool fits16 = compact && std::is_same<T, float>::value;
+  std::vector<int> cb(fits16 ? (size_t)std::max(A.nr, 1) : 0, 0);
+  for (int r = 0; r < A.nr && fits16; ++r) {
+    int lo = A.nc, hi = -1;
+    for (int k = A.rp[r]; k < A.rp[r + 1]; ++k) lo = std::min(lo, A.ci[k]), hi = std::max(hi, A.ci[k]);
+    cb[r] = hi >= 0 ? lo : 0;
+    fits16 = hi < 0 || hi - lo < 65535;
+  }
+  std::vector<int> col(fits16 ? 0 : (size_t)std::max<long long>(S->nslots, 1), -1);
+  std::vector<unsigned short> col16(fits16 ? (size_t)std::max<long long>(S->nslots, 1) : 0,
+                                    (unsigned short)0xffff);
   std::vector<T> val((size_t)std::max<long long>(S->nslots, 1), T(0));
 #pragma omp parallel for schedule(static)
   for (int r = 0; r < A.nr; ++r) {
     const int sl = r >> 5, lane = r & 31;
     for (int k = A.rp[r]; k < A.rp[r + 1]; ++k) {
       const long long slot = sptr[sl] + 32LL * (k - A.rp[r]) + lane;
-      col[slot] = A.ci[k];
+      if (fits16)
+        col16[slot] = (unsigned short)(A.ci[k] - cb[r]);
+      else
+        col[slot] = A.ci[k];
       val[slot] = (T)A.v[k];
     }
   }
   GIPB_TRY(S->sptr.upload(sptr.data(), sptr.size(), s));
-  GIPB_TRY(S->col.upload(col.data(), col.size(), s));
+  if (fits16) {
+    S->short_cols = true;
+    GIPB_TRY(S->dcol.upload(col16.data(), col16.size(), s));
+    GIPB_TRY(S->cbase.upload(cb.data(), cb.size(), s));
+  } else {
+    GIPB_TRY(S->col.upload(col.data(), col.size(), s));
+  }
   if (half) {
     std::vector<__half> hv(val.size());
     for (size_t k = 0; k < val.size(); ++k) hv[k] = __float2half_rn((float)val[k]);
@@ -479,6 +500,35 @@ __device__ __forceinline__ T amg_row_at(const SellView<V>& A, const T* __restric
   return sum;
 }
 
+// The same row with 16-bit slot columns: column = cb + d (cb the row's base column), the
+// offset 0xffff marking padding.
+template <typename T, int CH, typename V>
+__device__ __forceinline__ T amg_row_at16(const unsigned short* __restrict__ dcol,
+                                          const V* __restrict__ val, const T* __restrict__ x,
+                                          long long base, int len, int lane, int cb,
+                                          const T* __restrict__ xs) {
+  const unsigned short* cp = dcol + base + lane;
+  const V* vp = val + base + lane;
+  T sum = T(0);
+  for (int j0 = 0; j0 < len; j0 += CH) {
+    int c[CH];
+    T v[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+      const unsigned d = (j0 + t < len) ? (unsigned)ld_stream(cp + (size_t)(j0 + t) * 32) : 0xffffu;
+      c[t] = (d == 0xffffu) ? -1 : cb + (int)d;
+      v[t] = (j0 + t < len) ? (T)to_arith(ld_stream(vp + (size_t)(j0 + t) * 32)) : T(0);
+    }
+    T xv[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t)
+      xv[t] = (c[t] >= 0) ? (xs ? mulr(__ldg(xs + c[t]), __ldg(x + c[t])) : __ldg(x + c[t])) : T(0);
+#pragma unroll
+    for (int t = 0; t < CH; ++t) sum = fmat(xv[t], v[t], sum);
+  }
+  return sum;
+}
+
 template <typename T, int CH, typename V = T>
 __device__ __forceinline__ T amg_row(const SellView<V>& A, const T* __restrict__ x, int s, int lane) {
   const long long base = A.sptr[s];
@@ -500,21 +550,31 @@ enum { kResid = 0, kPlain = 1, kAdd = 2, kSmooth = 3, kScaleAdd = 4, kDiagAdd = 
 // the cycle no longer forms: rounded as the two separate steps round it)
 // kResid: y = b - A x;  kPlain: y = A x;  kAdd: y += A x;  kSmooth: y = x + dinv (b - A x);
 // kScaleAdd: y = w b + A x (the level-0 prolongation onto x0 = w r, never formed)
-template <typename T, int MODE, typename V = T>
+// C16: 16-bit slot columns (dcol, offsets from the row's base column cbase[row]).
+template <typename T, int MODE, typename V = T, bool C16 = false>
 __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __restrict__ x,
                                                      const T* __restrict__ b,
                                                      const T* __restrict__ dinv,
                                                      T* __restrict__ y, PcgScalars* S, T w,
-                                                     const int* __restrict__ yperm = nullptr,
-                                                     const T* __restrict__ xs = nullptr) {
+                                                     const int* __restrict__ yperm,
+                                                     const T* __restrict__ xs,
+                                                     const unsigned short* __restrict__ dcol,
+                                                     const int* __restrict__ cbase) {
   if (amg_enter(S)) return;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int s = gw; s < A.nslices; s += nw) {
     const long long b0 = A.sptr[s];
-    const T sum = amg_row_at<T, 4, V>(A, x, b0, (int)((A.sptr[s + 1] - b0) >> 5), lane, xs);
+    const int len = (int)((A.sptr[s + 1] - b0) >> 5);
     const int i = s * 32 + lane;
+    T sum;
+    if (C16) {
+      const int cb = (i < A.nrows) ? __ldg(cbase + i) : 0;
+      sum = amg_row_at16<T, 4, V>(dcol, A.val, x, b0, len, lane, cb, xs);
+    } else {
+      sum = amg_row_at<T, 4, V>(A, x, b0, len, lane, xs);
+    }
     if (i < A.nrows) {
       // kResid: level 0 may write its residual in aggregate order (yperm)
       if (MODE == kResid) y[yperm ? yperm[i] : i] = (w == T(1)) ? b[i] - sum : fmat(-w, sum, b[i]);
@@ -608,8 +668,14 @@ template <typename T, int MODE, typename V>
 void amg_mv_v(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const T* b,
               const T* dinv, T* y, PcgScalars* S, cudaStream_t s, T w, const T* xs) {
   if (M.lanes == 0) {
-    launch_dep(k_amg_spmv<T, MODE, V>, vec_blocks(M.nslices * 32), 256, s, view, x, b, dinv, y, S,
-               w, (const int*)nullptr, xs);
+    if (M.short_cols)
+      launch_dep(k_amg_spmv<T, MODE, V, true>, vec_blocks(M.nslices * 32), 256, s, view, x, b,
+                 dinv, y, S, w, (const int*)nullptr, xs, (const unsigned short*)M.dcol.p,
+                 (const int*)M.cbase.p);
+    else
+      launch_dep(k_amg_spmv<T, MODE, V, false>, vec_blocks(M.nslices * 32), 256, s, view, x, b,
+                 dinv, y, S, w, (const int*)nullptr, xs, (const unsigned short*)nullptr,
+                 (const int*)nullptr);
     return;
   }
   const int nb = vec_blocks((int)std::min<long long>((long long)M.nrows * M.lanes, 1LL << 30));
@@ -1023,9 +1089,9 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
         launch_packed0<kResid>(*pk, A0, bs, skip ? r : V.x.p, b, (const T*)nullptr, V.t.p, S, rs,
                                first, s, skip ? (T)omega0 : T(1), perm0.p);
       else
-        launch_dep(k_amg_spmv<T, kResid, T>, bs, 256, s, A0, skip ? r : (const T*)V.x.p, b,
-                   (const T*)nullptr, V.t.p, S, skip ? (T)omega0 : T(1), (const int*)perm0.p,
-                   (const T*)nullptr);
+        launch_dep(k_amg_spmv<T, kResid, T, false>, bs, 256, s, A0, skip ? r : (const T*)V.x.p,
+                   b, (const T*)nullptr, V.t.p, S, skip ? (T)omega0 : T(1), (const int*)perm0.p,
+                   (const T*)nullptr, (const unsigned short*)nullptr, (const int*)nullptr);
     } else {  // t = b - A (D^-1 b)
       amg_mv<T, kResid>(V.A, b, b, (const T*)nullptr, V.t.p, S, s, T(1), V.dinv.p);
     }

@@ -29,8 +29,8 @@ struct SellT {
   DevBuf<int> rp;
   bool half = false;           // values stored in FP16 (hval) instead of T (val)
   DevBuf<__half> hval;
-  // CSR form with 16-bit columns: column = cbase[row] + dcol[k], cbase the row's smallest
-  // column (every row's columns span at most 65536)
+  // 16-bit columns: column = cbase[row] + dcol[k], cbase the row's smallest column (every
+  // row's columns span at most 65536; in the sliced form 0xffff marks padding slots)
   bool short_cols = false;
   DevBuf<unsigned short> dcol;
   DevBuf<int> cbase;
@@ -118,7 +118,8 @@ double stream_bytes(const SellT<T>& M) {
   if (M.lanes > 0)
     return (double)M.nnz * ((M.short_cols ? 2.0 : 4.0) + w) + (M.nrows + 1.0) * 4.0 +
            (M.short_cols ? 4.0 * M.nrows : 0.0);
-  return (double)M.nslots * (4.0 + w) + (M.nslices + 1.0) * 8.0;
+  return (double)M.nslots * ((M.short_cols ? 2.0 : 4.0) + w) + (M.nslices + 1.0) * 8.0 +
+         (M.short_cols ? 4.0 * M.nrows : 0.0);
 }
 
 using Amg = AmgT<float>;
