@@ -98,11 +98,13 @@ def tune_batch(batch, stream, shapes: Sequence = BATCH_SHAPES, steps: int = 2) -
     rows = np.array([e.n_inner for e in batch.instances], np.float64)
     iters = np.array([max(float(np.mean(e.history()["iters"][-steps:])), 1.0)
                       for e in batch.instances])
-    batch.balance(rows * iters)
+    weights = rows * iters
+    batch.balance(weights)
     t_measured = timed()
     balanced = t_measured < t_default
     if not balanced:
         batch.balance(None)
     return {"block": best[0], "rows_per_warp": best[1], "balanced_by_iterations": balanced,
+            "weights": weights.tolist() if balanced else None,
             "ms": {f"{b}x{r}": round(v, 3) for (b, r), v in ms.items()},
             "ms_default_split": round(t_default, 3), "ms_measured_split": round(t_measured, 3)}

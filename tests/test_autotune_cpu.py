@@ -111,7 +111,8 @@ def test_tune_batch_picks_shape_and_split(monkeypatch):
     r = autotune.tune_batch(B, None, steps=2)
     assert (r["block"], r["rows_per_warp"]) == (256, 64) and B.shape == (256, 64)
     assert r["balanced_by_iterations"] and B.weights == [1000 * 50.0, 8000 * 120.0]
+    assert r["weights"] == [1000 * 50.0, 8000 * 120.0]
     B2 = FakeBatch(ms, 9.0)  # the measured split is slower: the default split is restored
     B = B2
     r = autotune.tune_batch(B2, None, steps=2)
-    assert not r["balanced_by_iterations"] and B2.weights is None
+    assert not r["balanced_by_iterations"] and B2.weights is None and r["weights"] is None
