@@ -364,8 +364,13 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool c
   S->nnz = A.nnz();
   S->nslices = (A.nr + 31) / 32;
   const double avg = (double)A.nnz() / std::max(A.nr, 1);
-  if (avg >= 12.0) {  // long rows: CSR, 8 to 32 threads per row
-    S->lanes = avg >= 48.0 ? 32 : avg >= 24.0 ? 16 : 8;
+  if (avg >= 12.0) {  // long rows: CSR, 4 to 32 threads per row
+    // FP32 cycle: as few threads per row as cover its entries in one pass (4 threads x 8
+    // entries, 8 x 4, ...), so that a warp works on more rows per dependent round trip;
+    // GIPB200_AMG_WIDE_ROWS=1 (and the FP64 cycle): 8 to 32 threads per row
+    const bool narrow = std::is_same<T, float>::value && !getenv("GIPB200_AMG_WIDE_ROWS");
+    S->lanes = narrow ? (avg < 32.0 ? 4 : avg < 64.0 ? 8 : avg < 128.0 ? 16 : 32)
+                      : (avg >= 48.0 ? 32 : avg >= 24.0 ? 16 : 8);
     GIPB_TRY(S->rp.upload(A.rp.data(), A.rp.size(), s));
     bool fits = compact && std::is_same<T, float>::value;
     std::vector<int> cb((size_t)std::max(A.nr, 1), 0);
@@ -591,9 +596,10 @@ __global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __r
 // of the row, combined by a fixed shuffle tree (deterministic).  The row loop is uniform
 // across the warp (32 / LANES rows per warp per pass), so every lane takes part in the
 // shuffles.  Software-pipelined: the next pass's row bounds are loaded while this pass's
-// gathers are in flight, and each lane loads up to U of its entries before gathering
-// them, so a pass costs two dependent memory round trips instead of two per entry plus
-// one for the bounds.  Each lane still adds its entries in increasing order.
+// gathers are in flight, and each lane loads up to U of its entries (8 with 4 threads per
+// row, else 4) before gathering them, so a pass costs two dependent memory round trips
+// instead of two per entry plus one for the bounds.  Each lane still adds its entries in
+// increasing order.
 template <typename T, int MODE, int LANES, typename V = T, typename CI = int>
 __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restrict__ rp,
                                                  const CI* __restrict__ col,
@@ -603,8 +609,8 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
                                                  PcgScalars* S, T w, const T* __restrict__ xs,
                                                  const int* __restrict__ cbase) {
   if (amg_enter(S)) return;
-  constexpr int RPW = 32 / LANES;  // rows per warp per pass
-  constexpr int U = 4;             // entries a lane loads before their gathers
+  constexpr int RPW = 32 / LANES;        // rows per warp per pass
+  constexpr int U = LANES <= 4 ? 8 : 4;  // entries a lane loads before their gathers
   const int lane = threadIdx.x & 31, sub = lane % LANES;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -686,11 +692,13 @@ void amg_mv_v(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const
   if (M.short_cols) {
     if (M.lanes == 32) GIPB_CSR(32, unsigned short, M.dcol.p);
     else if (M.lanes == 16) GIPB_CSR(16, unsigned short, M.dcol.p);
-    else GIPB_CSR(8, unsigned short, M.dcol.p);
+    else if (M.lanes == 8) GIPB_CSR(8, unsigned short, M.dcol.p);
+    else GIPB_CSR(4, unsigned short, M.dcol.p);
   } else {
     if (M.lanes == 32) GIPB_CSR(32, int, M.col.p);
     else if (M.lanes == 16) GIPB_CSR(16, int, M.col.p);
-    else GIPB_CSR(8, int, M.col.p);
+    else if (M.lanes == 8) GIPB_CSR(8, int, M.col.p);
+    else GIPB_CSR(4, int, M.col.p);
   }
 #undef GIPB_CSR
 }
