@@ -557,7 +557,7 @@ enum { kResid = 0, kPlain = 1, kAdd = 2, kSmooth = 3, kScaleAdd = 4, kDiagAdd = 
 // kScaleAdd: y = w b + A x (the level-0 prolongation onto x0 = w r, never formed)
 // C16: 16-bit slot columns (dcol, offsets from the row's base column cbase[row]).
 template <typename T, int MODE, typename V = T, bool C16 = false>
-__global__ void __launch_bounds__(256, 8) k_amg_spmv(SellView<V> A, const T* __restrict__ x,
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 6 : 8) k_amg_spmv(SellView<V> A, const T* __restrict__ x,
                                                      const T* __restrict__ b,
                                                      const T* __restrict__ dinv,
                                                      T* __restrict__ y, PcgScalars* S, T w,
