@@ -566,6 +566,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 6 : 8) k_amg_spmv(SellVi
                                                      const unsigned short* __restrict__ dcol,
                                                      const int* __restrict__ cbase) {
   if (amg_enter(S)) return;
+  // slots a lane loads before gathering: 8 in FP32 (a prolongation row's slots in one
+  // round trip), 4 in FP64
+  constexpr int kCh = sizeof(T) == 4 ? 8 : 4;
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -576,9 +579,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 6 : 8) k_amg_spmv(SellVi
     T sum;
     if (C16) {
       const int cb = (i < A.nrows) ? __ldg(cbase + i) : 0;
-      sum = amg_row_at16<T, 4, V>(dcol, A.val, x, b0, len, lane, cb, xs);
+      sum = amg_row_at16<T, kCh, V>(dcol, A.val, x, b0, len, lane, cb, xs);
     } else {
-      sum = amg_row_at<T, 4, V>(A, x, b0, len, lane, xs);
+      sum = amg_row_at<T, kCh, V>(A, x, b0, len, lane, xs);
     }
     if (i < A.nrows) {
       // kResid: level 0 may write its residual in aggregate order (yperm)
