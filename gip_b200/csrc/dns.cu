@@ -270,6 +270,86 @@ __global__ void __launch_bounds__(256) k_dns_massflux3(
   }
 }
 
+// k_dns_massflux3 for the common case in which every merged face row holds entries of one
+// operator only (a structured grid's face is an x, y or z face): one gradient and one
+// velocity sum per face, so the kernel fits the registers of six blocks per SM.  The
+// updates keep their order: mf = fact1 SO p (a0), then fact2 SF_d gp_d, then rho SF_d u_d.
+__global__ void __launch_bounds__(256, 5) k_dns_massflux1(
+    SellView<double> SO, SellView<double> SF, const unsigned short* __restrict__ cnt,
+    const double* __restrict__ p, const double* __restrict__ gpx, const double* __restrict__ gpy,
+    const double* __restrict__ gpz, const double* __restrict__ u, const double* __restrict__ v,
+    const double* __restrict__ w, double* __restrict__ mf, double rho, const DnsScalars* S) {
+  const double sigma = S->sigma;
+  const double fact1 = ddiv(-1.0, sigma);
+  const double fact2 = ddiv(1.0, sigma);
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int ns = max(SO.nslices, SF.nslices);
+  for (int s = gw; s < ns; s += nw) {
+    const int f = s * 32 + lane;
+    long long ob = 0, fb = 0;
+    int ol = 0, fl = 0;
+    const double* g = gpx;
+    const double* q = u;
+    bool any_f = false;
+    if (s < SO.nslices) ob = SO.sptr[s], ol = (int)((SO.sptr[s + 1] - ob) >> 5);
+    if (s < SF.nslices) {
+      fb = SF.sptr[s];
+      fl = (int)((SF.sptr[s + 1] - fb) >> 5);
+      const unsigned c = (f < SF.nrows) ? cnt[f] : 0u;
+      any_f = c != 0u;
+      if ((c & 15u) == 0u) {
+        g = ((c >> 4) & 15u) ? gpy : gpz;
+        q = ((c >> 4) & 15u) ? v : w;
+      }
+    }
+    double so = 0.0, gs = 0.0, us = 0.0;
+    bool a0 = false;
+    const int len = max(ol, fl);
+    for (int j0 = 0; j0 < len; j0 += 2) {
+      int oc[2], fc[2];
+      double ov[2], fv[2];
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int j = j0 + t;
+        oc[t] = (j < ol) ? ld_stream(SO.col + ob + 32LL * j + lane) : -1;
+        ov[t] = (j < ol) ? ld_stream(SO.val + ob + 32LL * j + lane) : 0.0;
+        fc[t] = (j < fl) ? ld_stream(SF.col + fb + 32LL * j + lane) : -1;
+        fv[t] = (j < fl) ? ld_stream(SF.val + fb + 32LL * j + lane) : 0.0;
+      }
+      double op[2], a[2], b[2];
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        op[t] = (oc[t] >= 0) ? __ldg(p + oc[t]) : 0.0;
+        a[t] = (fc[t] >= 0) ? __ldg(g + fc[t]) : 0.0;
+        b[t] = (fc[t] >= 0) ? __ldg(q + fc[t]) : 0.0;
+      }
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        if (oc[t] >= 0) {
+          so = dadd(so, dmul(op[t], ov[t]));
+          a0 = true;
+        }
+        if (fc[t] >= 0) {
+          gs = dadd(gs, dmul(a[t], fv[t]));
+          us = dadd(us, dmul(b[t], fv[t]));
+        }
+      }
+    }
+    a0 = a0 && f < SO.nrows;
+    if (a0 || any_f) {
+      double m = mf[f];
+      if (a0) m = axpby_row(fact1, so, 0.0, m);
+      if (any_f) {
+        m = axpby_row(fact2, gs, 1.0, m);
+        m = axpby_row(rho, us, 1.0, m);
+      }
+      mf[f] = m;
+    }
+  }
+}
+
 // mf = -dt SO p + dt SF gp + rho SF u, as seven ordered SpMV updates -- GIP_DNS.h:381-390
 __global__ void __launch_bounds__(256) k_dns_massflux(
     SellView<double> SO, SellView<double> SFx, SellView<double> SFy, SellView<double> SFz,
@@ -517,7 +597,11 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync, int part) {
                                                  gpy.p, gpz.p, u.p, v.p, w.p, N, prm.rho, sc.p);
     mark(5);
     // MassFluxes
-    if (SF3.on)
+    if (SF3.on && SF3.single)
+      k_dns_massflux1<<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p, p.p,
+                                                    gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p,
+                                                    prm.rho, sc.p);
+    else if (SF3.on)
       k_dns_massflux3<<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p, p.p,
                                                     gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p,
                                                     prm.rho, sc.p);
@@ -729,14 +813,16 @@ static int build_face3(FaceOps3* F, const gipb200_host_csr* const op[3], int NF,
   std::vector<int> rp((size_t)NF + 1, 0), col;
   std::vector<double> val;
   std::vector<unsigned short> cnt((size_t)NF, 0);
+  bool single = true;
   for (int f = 0; f < NF; ++f) {
-    unsigned packed = 0;
+    unsigned packed = 0, ops_here = 0;
     for (int o = 0; o < 3; ++o) {
       const gipb200_host_csr& m = *op[o];
       if (f >= m.nrows) continue;
       const int c = m.rowptr[f + 1] - m.rowptr[f];
       if (c > 15) return GIPB200_OK;
       packed |= (unsigned)c << (4 * o);
+      ops_here += c > 0 ? 1u : 0u;
       for (int k = m.rowptr[f]; k < m.rowptr[f + 1]; ++k) {
         col.push_back(m.col[k]);
         val.push_back(m.val[k]);
@@ -744,11 +830,13 @@ static int build_face3(FaceOps3* F, const gipb200_host_csr* const op[3], int NF,
     }
     cnt[f] = (unsigned short)packed;
     rp[f + 1] = (int)col.size();
+    single = single && ops_here <= 1;
   }
   GIPB_TRY(sell_build(&F->S, NF, NO, (int)col.size(), rp.data(), col.data(), val.data(), 0, 0u));
   GIPB_TRY(F->cnt.upload(cnt.data(), cnt.size(), 0));
   GIPB_CUDA(cudaStreamSynchronize(0));
   F->on = true;
+  F->single = single && !getenv("GIPB200_NO_FACE1");
   return GIPB200_OK;
 }
 
@@ -972,7 +1060,12 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     GIPB_TRY(one_wave(k_dns_ab2, E.blocks_vec, &E.grid.ab2));
     GIPB_TRY(one_wave(k_dns_rhs, E.blocks_cells, &E.grid.rhs));
     GIPB_TRY(one_wave(k_dns_gradcorr, E.blocks_owned, &E.grid.gradcorr));
-    GIPB_TRY(one_wave(k_dns_massflux, E.blocks_faces, &E.grid.massflux));
+    if (E.SF3.on && E.SF3.single)
+      GIPB_TRY(one_wave(k_dns_massflux1, E.blocks_faces, &E.grid.massflux));
+    else if (E.SF3.on)
+      GIPB_TRY(one_wave(k_dns_massflux3, E.blocks_faces, &E.grid.massflux));
+    else
+      GIPB_TRY(one_wave(k_dns_massflux, E.blocks_faces, &E.grid.massflux));
     GIPB_TRY(one_wave(k_dns_massr, E.blocks_cells, &E.grid.massr));
     GIPB_TRY(one_wave(k_dns_cfl, E.blocks_vec, &E.grid.cfl));
     GIPB_CUDA(cudaStreamCreateWithFlags(&E.cap_stream, cudaStreamNonBlocking));

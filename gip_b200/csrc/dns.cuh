@@ -37,6 +37,7 @@ constexpr int kPhaseMarks = 8;
 // padding.  Each operator's row sum keeps its own order, so results are unchanged.
 struct FaceOps3 {
   bool on = false;
+  bool single = false;               // every face's entries belong to one operator only
   Sell S;                            // merged rows (NF rows)
   DevBuf<unsigned short> cnt;        // per face: cx | cy << 4 | cz << 8
 };

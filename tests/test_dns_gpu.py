@@ -274,12 +274,16 @@ def test_phase_stamps_time_graph_steps_without_changing_them(gpu, mode):
     assert np.isnan(ph["pcg"][5]) and E.history()["kernels"][5] == G.history()["kernels"][5]
 
 
-def test_merged_face_operators_are_exact(gpu, monkeypatch):
-    # the mass-flux kernel over SFx/SFy/SFz merged per face gives the same fields, bit for
+@pytest.mark.parametrize("general", [False, True])
+def test_merged_face_operators_are_exact(gpu, monkeypatch, general):
+    # the mass-flux kernel over SFx/SFy/SFz merged per face (its one-operator-per-face form
+    # by default, its general form with GIPB200_NO_FACE1) gives the same fields, bit for
     # bit, as the kernel walking the three operators separately
     from gip_b200.device import DnsEngine
     case, _ = cavity.generate(12, re=400.0, permute_seed=5)
     kw = dict(gamma=1.0 / 400, pcg_mode="fixed", maxit=100, reorder=True)
+    if general:
+        monkeypatch.setenv("GIPB200_NO_FACE1", "1")
     E = DnsEngine(case, **kw)
     monkeypatch.setenv("GIPB200_NO_FACE3", "1")
     P = DnsEngine(case, **kw)
