@@ -783,13 +783,13 @@ __global__ void __launch_bounds__(256, 8) k_amgp_spmv(SellView<float> A, PackedV
   PackedWords cur;
   for (int s = gw; s < A.nslices; s += nw) {
     packed_words<NIB>(pk.delta, pk.idx, pk.plain, s, lane, cur);
+    int c[8];
+    packed_cols(pk.base, s, cur.d, c);
     const int i = s * 32 + lane;
     float sum;
     if (cur.plain) {
       sum = amg_row<float, 2>(A, x, s, lane);
     } else {
-      int c[8];
-      packed_cols(pk.base, s, cur.d, c);
       float xv[K];
 #pragma unroll
       for (int j = 0; j < K; ++j) xv[j] = __ldg(x + c[j]);

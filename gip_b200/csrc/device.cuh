@@ -119,6 +119,8 @@ struct PackedWords {
   int plain;        // the slice is stored in the plain sliced layout instead
 };
 
+// The words are loaded whatever the slice's plain flag (every row has them), so the flag,
+// the words and the slot bases are one round trip, not two.
 template <int NIB>
 __device__ __forceinline__ void packed_words(const uint4* __restrict__ delta,
                                              const void* __restrict__ idx,
@@ -126,11 +128,6 @@ __device__ __forceinline__ void packed_words(const uint4* __restrict__ delta,
                                              int lane, PackedWords& o) {
   const int i = s * 32 + lane;
   o.plain = __ldg(plain + s);
-  if (o.plain) {
-    o.d = make_uint4(0u, 0u, 0u, 0u);
-    o.w0 = o.w1 = 0u;
-    return;
-  }
   o.d = ld_stream(delta + i);
   if (NIB == 4) {
     o.w0 = ld_stream(static_cast<const unsigned*>(idx) + i);

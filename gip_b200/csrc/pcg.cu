@@ -533,13 +533,13 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
   PackedWords cur;
   for (int s = gw; s < A.nslices; s += nw) {
     packed_words<NIB>(delta, idx, plain, s, lane, cur);
+    int c[8];
+    packed_cols(base, s, cur.d, c);
     const int i = s * 32 + lane;
     float sum;
     if (cur.plain) {  // rare fallback: few registers
       sum = REC ? sell_row_f32<2>(A, r, s, lane) : sell_row_dir<2>(A, r, pin, beta, s, lane);
     } else {
-      int c[8];
-      packed_cols(base, s, cur.d, c);
       float xv[K];
 #pragma unroll
       for (int j = 0; j < K; ++j)
