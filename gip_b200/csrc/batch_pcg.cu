@@ -126,8 +126,7 @@ __device__ __forceinline__ void rows_l(const SellView<double>& L, const double* 
     base[u] = 0;
     len[u] = 0;
     if (s[u] < L.nslices) {
-      base[u] = L.sptr[s[u]];
-      len[u] = (int)((L.sptr[s[u] + 1] - base[u]) >> 5);
+      slice_range(L, s[u], base[u], len[u]);
     }
     lmax = max(lmax, len[u]);
   }
@@ -169,8 +168,7 @@ __device__ __forceinline__ void rows_dir(const SellView<float>& A, const float* 
     base[u] = 0;
     len[u] = 0;
     if (s[u] < A.nslices) {
-      base[u] = A.sptr[s[u]];
-      len[u] = (int)((A.sptr[s[u] + 1] - base[u]) >> 5);
+      slice_range(A, s[u], base[u], len[u]);
     }
     lmax = max(lmax, len[u]);
   }

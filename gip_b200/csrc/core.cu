@@ -121,6 +121,13 @@ int sell_build(Sell* S, int nrows, int ncols, int nnz, const int* rp, const int*
   }
   S->rows_nonempty = nonempty;
   S->nslots = sptr[S->nslices];
+  S->uslots = 0;
+  if (S->nslices > 0 && S->nslots > 0) {
+    const long long l0 = sptr[1] - sptr[0];
+    bool uniform = true;
+    for (int s = 1; s < S->nslices && uniform; ++s) uniform = sptr[s + 1] - sptr[s] == l0;
+    if (uniform) S->uslots = (int)(l0 / 32);
+  }
   std::vector<int> scol((size_t)std::max<long long>(S->nslots, 1), -1);
   std::vector<double> sval((size_t)std::max<long long>(S->nslots, 1), 0.0);
   if (S->nslots > 0x7fffffffLL)

@@ -165,8 +165,9 @@ __device__ __forceinline__ unsigned packed_index(const PackedWords& w, int j) {
 template <typename V, typename X, int CH = 8>
 __device__ __forceinline__ void sell_row_f64(const SellView<V>& A, const X* __restrict__ x,
                                              int s, int lane, double& sum, bool& any) {
-  const long long base = A.sptr[s];
-  const int len = (int)((A.sptr[s + 1] - base) >> 5);
+  long long base;
+  int len;
+  slice_range(A, s, base, len);
   const int* cp = A.col + base + lane;
   const V* vp = A.val + base + lane;
   for (int j0 = 0; j0 < len; j0 += CH) {
@@ -201,8 +202,9 @@ template <typename V, int CH = 4>
 __device__ __forceinline__ void sell_row_f64_pair(const SellView<V>& A, const double* __restrict__ x1,
                                                   const double* __restrict__ x2, int s, int lane,
                                                   double& sum1, double& sum2, bool& any) {
-  const long long base = A.sptr[s];
-  const int len = (int)((A.sptr[s + 1] - base) >> 5);
+  long long base;
+  int len;
+  slice_range(A, s, base, len);
   const int* cp = A.col + base + lane;
   const V* vp = A.val + base + lane;
   for (int j0 = 0; j0 < len; j0 += CH) {
@@ -248,8 +250,7 @@ __device__ __forceinline__ void sell_rows3_f64(const SellView<double> (&M)[3],
     base[k] = 0;
     len[k] = 0;
     if (s < M[k].nslices) {
-      base[k] = M[k].sptr[s];
-      len[k] = (int)((M[k].sptr[s + 1] - base[k]) >> 5);
+      slice_range(M[k], s, base[k], len[k]);
     }
     len_max = max(len_max, len[k]);
   }
@@ -283,8 +284,9 @@ __device__ __forceinline__ void sell_rows3_f64(const SellView<double> (&M)[3],
 template <int CH = 8>
 __device__ __forceinline__ float sell_row_f32(const SellView<float>& A, const float* __restrict__ x,
                                               int s, int lane) {
-  const long long base = A.sptr[s];
-  const int len = (int)((A.sptr[s + 1] - base) >> 5);
+  long long base;
+  int len;
+  slice_range(A, s, base, len);
   const int* cp = A.col + base + lane;
   const float* vp = A.val + base + lane;
   float sum = 0.f;

@@ -27,8 +27,9 @@ __device__ __forceinline__ void dc_row(const SellView<double>& D, const double* 
                                        const double* __restrict__ u, const double* __restrict__ v,
                                        const double* __restrict__ w, int s, int lane,
                                        double (&sd)[3], double (&sc)[3], bool& any) {
-  const long long base = D.sptr[s];
-  const int len = (int)((D.sptr[s + 1] - base) >> 5);
+  long long base;
+  int len;
+  slice_range(D, s, base, len);
   for (int j = 0; j < len; ++j) {
     const long long k = base + 32LL * j + lane;
     const int c = ld_stream(D.col + k);
@@ -203,10 +204,9 @@ __global__ void __launch_bounds__(256) k_dns_massflux3(
     // the gathers of both are in flight at once (three dependent round trips per face)
     long long ob = 0, fb = 0;
     int ol = 0, fl = 0;
-    if (s < SO.nslices) ob = SO.sptr[s], ol = (int)((SO.sptr[s + 1] - ob) >> 5);
+    if (s < SO.nslices) slice_range(SO, s, ob, ol);
     if (s < SF.nslices) {
-      fb = SF.sptr[s];
-      fl = (int)((SF.sptr[s + 1] - fb) >> 5);
+      slice_range(SF, s, fb, fl);
       const unsigned c = (f < SF.nrows) ? cnt[f] : 0u;
       cx = c & 15u;
       cy = (c >> 4) & 15u;
@@ -293,10 +293,9 @@ __global__ void __launch_bounds__(256, 5) k_dns_massflux1(
     const double* g = gpx;
     const double* q = u;
     bool any_f = false;
-    if (s < SO.nslices) ob = SO.sptr[s], ol = (int)((SO.sptr[s + 1] - ob) >> 5);
+    if (s < SO.nslices) slice_range(SO, s, ob, ol);
     if (s < SF.nslices) {
-      fb = SF.sptr[s];
-      fl = (int)((SF.sptr[s + 1] - fb) >> 5);
+      slice_range(SF, s, fb, fl);
       const unsigned c = (f < SF.nrows) ? cnt[f] : 0u;
       any_f = c != 0u;
       if ((c & 15u) == 0u) {

@@ -148,12 +148,27 @@ struct SellView {
   const long long* __restrict__ sptr;
   const int* __restrict__ col;
   const V* __restrict__ val;
+  int uslots;  // > 0: every slice has this many slots (slice s starts at 32 * uslots * s)
 };
+
+// Slot range of slice s: computed when the slices are uniform, else read from sptr.
+template <typename V>
+__host__ __device__ __forceinline__ void slice_range(const SellView<V>& A, int s, long long& base,
+                                                     int& len) {
+  if (A.uslots > 0) {
+    base = 32LL * A.uslots * s;
+    len = A.uslots;
+  } else {
+    base = A.sptr[s];
+    len = (int)((A.sptr[s + 1] - base) >> 5);
+  }
+}
 
 struct Sell {
   int nrows = 0, ncols = 0, nnz = 0, nslices = 0;
   long long nslots = 0;
   bool rows_nonempty = true;  // no empty row
+  int uslots = 0;             // > 0: every slice has this many slots
   DevBuf<long long> sptr;
   DevBuf<int> col;
   DevBuf<double> val;
@@ -163,9 +178,11 @@ struct Sell {
   DevBuf<int> csr_col;
   DevBuf<double> csr_val;
   std::vector<int> h_rowptr, h_col;  // host CSR structure (setup only)
-  SellView<double> view() const { return {nrows, nslices, sptr.p, col.p, val.p}; }
-  SellView<double> view_vals(const double* v) const { return {nrows, nslices, sptr.p, col.p, v}; }
-  SellView<float> view32() const { return {nrows, nslices, sptr.p, col.p, val32.p}; }
+  SellView<double> view() const { return {nrows, nslices, sptr.p, col.p, val.p, uslots}; }
+  SellView<double> view_vals(const double* v) const {
+    return {nrows, nslices, sptr.p, col.p, v, uslots};
+  }
+  SellView<float> view32() const { return {nrows, nslices, sptr.p, col.p, val32.p, uslots}; }
 };
 
 // Builds SELL-32 from host CSR arrays, keeping what `keep` asks for: a device CSR copy

@@ -425,8 +425,9 @@ template <int CH>
 __device__ __forceinline__ float sell_row_dir(const SellView<float>& A, const float* __restrict__ r,
                                               const float* __restrict__ pin, float beta, int s,
                                               int lane) {
-  const long long base = A.sptr[s];
-  const int len = (int)((A.sptr[s + 1] - base) >> 5);
+  long long base;
+  int len;
+  slice_range(A, s, base, len);
   const int* cp = A.col + base + lane;
   const float* vp = A.val + base + lane;
   float sum = 0.f;
@@ -712,8 +713,9 @@ __global__ void k_mx_lhat(SellView<double> L, const double* __restrict__ scale, 
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int s = gw; s < L.nslices; s += nw) {
-    const long long base = L.sptr[s];
-    const int len = (int)((L.sptr[s + 1] - base) >> 5);
+    long long base;
+    int len;
+    slice_range(L, s, base, len);
     const int i = s * 32 + lane;
     for (int j = 0; j < len; ++j) {
       const long long k = base + 32LL * j + lane;

@@ -88,7 +88,9 @@ struct Pcg {
   int sort_fp32_rows(cudaStream_t s);
   void launch_pcg_update(double* x, cudaStream_t s);
   int build_compressed(cudaStream_t s);
-  SellView<float> a32() const { return {L->nrows, L->nslices, L->sptr.p, col32.p, lhat.p}; }
+  SellView<float> a32() const {
+    return {L->nrows, L->nslices, L->sptr.p, col32.p, lhat.p, L->uslots};
+  }
   PackedView packed() const {
     PackedView v;
     v.on = cop.enabled;
