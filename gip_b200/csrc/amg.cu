@@ -478,9 +478,10 @@ __device__ __forceinline__ double to_arith(double v) { return v; }
 
 // One row of a sliced operator whose slice starts at slot `base` and has `len` slots,
 // summed slot by slot (padding: column -1, skipped).
-// xs (optional): the gathered vector is xs * x elementwise, each product rounded on its
-// own (the same value a separate x = xs * x pass would store).
-template <typename T, int CH, typename V = T>
+// XS: the gathered vector is xs * x elementwise, each product rounded on its own (the
+// same value a separate x = xs * x pass would store).  A compile-time choice: a run-time
+// test in the gather loop measured 8-21% slower on the kernels that never scale.
+template <typename T, int CH, typename V = T, bool XS = false>
 __device__ __forceinline__ T amg_row_at(const SellView<V>& A, const T* __restrict__ x,
                                         long long base, int len, int lane,
                                         const T* __restrict__ xs = nullptr) {
@@ -498,7 +499,7 @@ __device__ __forceinline__ T amg_row_at(const SellView<V>& A, const T* __restric
     T xv[CH];
 #pragma unroll
     for (int t = 0; t < CH; ++t)
-      xv[t] = (c[t] >= 0) ? (xs ? mulr(__ldg(xs + c[t]), __ldg(x + c[t])) : __ldg(x + c[t])) : T(0);
+      xv[t] = (c[t] >= 0) ? (XS ? mulr(__ldg(xs + c[t]), __ldg(x + c[t])) : __ldg(x + c[t])) : T(0);
 #pragma unroll
     for (int t = 0; t < CH; ++t) sum = fmat(xv[t], v[t], sum);
   }
@@ -507,7 +508,7 @@ __device__ __forceinline__ T amg_row_at(const SellView<V>& A, const T* __restric
 
 // The same row with 16-bit slot columns: column = cb + d (cb the row's base column), the
 // offset 0xffff marking padding.
-template <typename T, int CH, typename V>
+template <typename T, int CH, typename V, bool XS>
 __device__ __forceinline__ T amg_row_at16(const unsigned short* __restrict__ dcol,
                                           const V* __restrict__ val, const T* __restrict__ x,
                                           long long base, int len, int lane, int cb,
@@ -527,7 +528,7 @@ __device__ __forceinline__ T amg_row_at16(const unsigned short* __restrict__ dco
     T xv[CH];
 #pragma unroll
     for (int t = 0; t < CH; ++t)
-      xv[t] = (c[t] >= 0) ? (xs ? mulr(__ldg(xs + c[t]), __ldg(x + c[t])) : __ldg(x + c[t])) : T(0);
+      xv[t] = (c[t] >= 0) ? (XS ? mulr(__ldg(xs + c[t]), __ldg(x + c[t])) : __ldg(x + c[t])) : T(0);
 #pragma unroll
     for (int t = 0; t < CH; ++t) sum = fmat(xv[t], v[t], sum);
   }
@@ -556,7 +557,7 @@ enum { kResid = 0, kPlain = 1, kAdd = 2, kSmooth = 3, kScaleAdd = 4, kDiagAdd = 
 // kResid: y = b - A x;  kPlain: y = A x;  kAdd: y += A x;  kSmooth: y = x + dinv (b - A x);
 // kScaleAdd: y = w b + A x (the level-0 prolongation onto x0 = w r, never formed)
 // C16: 16-bit slot columns (dcol, offsets from the row's base column cbase[row]).
-template <typename T, int MODE, typename V = T, bool C16 = false>
+template <typename T, int MODE, typename V = T, bool C16 = false, bool XS = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 6 : 8) k_amg_spmv(SellView<V> A, const T* __restrict__ x,
                                                      const T* __restrict__ b,
                                                      const T* __restrict__ dinv,
@@ -579,9 +580,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 6 : 8) k_amg_spmv(SellVi
     T sum;
     if (C16) {
       const int cb = (i < A.nrows) ? __ldg(cbase + i) : 0;
-      sum = amg_row_at16<T, kCh, V>(dcol, A.val, x, b0, len, lane, cb, xs);
+      sum = amg_row_at16<T, kCh, V, XS>(dcol, A.val, x, b0, len, lane, cb, xs);
     } else {
-      sum = amg_row_at<T, kCh, V>(A, x, b0, len, lane, xs);
+      sum = amg_row_at<T, kCh, V, XS>(A, x, b0, len, lane, xs);
     }
     if (i < A.nrows) {
       // kResid: level 0 may write its residual in aggregate order (yperm)
@@ -603,7 +604,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 6 : 8) k_amg_spmv(SellVi
 // row, else 4) before gathering them, so a pass costs two dependent memory round trips
 // instead of two per entry plus one for the bounds.  Each lane still adds its entries in
 // increasing order.
-template <typename T, int MODE, int LANES, typename V = T, typename CI = int>
+template <typename T, int MODE, int LANES, typename V = T, typename CI = int, bool XS = false>
 __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restrict__ rp,
                                                  const CI* __restrict__ col,
                                                  const V* __restrict__ val, const T* __restrict__ x,
@@ -648,7 +649,7 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
       T xv[U];
 #pragma unroll
       for (int u = 0; u < U; ++u)
-        xv[u] = (c[u] >= 0) ? (xs ? mulr(__ldg(xs + c[u]), __ldg(x + c[u])) : __ldg(x + c[u]))
+        xv[u] = (c[u] >= 0) ? (XS ? mulr(__ldg(xs + c[u]), __ldg(x + c[u])) : __ldg(x + c[u]))
                             : T(0);
 #pragma unroll
       for (int u = 0; u < U; ++u)
@@ -672,26 +673,26 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
 
 int vec_blocks(int n);
 
-// y (mode) A x for an AMG operator in either form.
-template <typename T, int MODE, typename V>
-void amg_mv_v(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const T* b,
-              const T* dinv, T* y, PcgScalars* S, cudaStream_t s, T w, const T* xs) {
+// y (mode) A x for an AMG operator in either form; XS: the gathered x scaled by xs.
+template <typename T, int MODE, typename V, bool XS>
+void amg_mv_vx(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const T* b,
+               const T* dinv, T* y, PcgScalars* S, cudaStream_t s, T w, const T* xs) {
   if (M.lanes == 0) {
     if (M.short_cols)
-      launch_dep(k_amg_spmv<T, MODE, V, true>, vec_blocks(M.nslices * 32), 256, s, view, x, b,
-                 dinv, y, S, w, (const int*)nullptr, xs, (const unsigned short*)M.dcol.p,
+      launch_dep(k_amg_spmv<T, MODE, V, true, XS>, vec_blocks(M.nslices * 32), 256, s, view, x,
+                 b, dinv, y, S, w, (const int*)nullptr, xs, (const unsigned short*)M.dcol.p,
                  (const int*)M.cbase.p);
     else
-      launch_dep(k_amg_spmv<T, MODE, V, false>, vec_blocks(M.nslices * 32), 256, s, view, x, b,
-                 dinv, y, S, w, (const int*)nullptr, xs, (const unsigned short*)nullptr,
+      launch_dep(k_amg_spmv<T, MODE, V, false, XS>, vec_blocks(M.nslices * 32), 256, s, view, x,
+                 b, dinv, y, S, w, (const int*)nullptr, xs, (const unsigned short*)nullptr,
                  (const int*)nullptr);
     return;
   }
   const int nb = vec_blocks((int)std::min<long long>((long long)M.nrows * M.lanes, 1LL << 30));
   const int* rp = M.rp.p;
-#define GIPB_CSR(L, CI, COLS)                                                                    \
-  launch_dep(k_amg_csr<T, MODE, L, V, CI>, nb, 256, s, M.nrows, rp, (const CI*)COLS, v, x, b, dinv, \
-             y, S, w, xs, (const int*)M.cbase.p)
+#define GIPB_CSR(L, CI, COLS)                                                                \
+  launch_dep(k_amg_csr<T, MODE, L, V, CI, XS>, nb, 256, s, M.nrows, rp, (const CI*)COLS, v, x, \
+             b, dinv, y, S, w, xs, (const int*)M.cbase.p)
   if (M.short_cols) {
     if (M.lanes == 32) GIPB_CSR(32, unsigned short, M.dcol.p);
     else if (M.lanes == 16) GIPB_CSR(16, unsigned short, M.dcol.p);
@@ -704,6 +705,18 @@ void amg_mv_v(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const
     else GIPB_CSR(4, int, M.col.p);
   }
 #undef GIPB_CSR
+}
+
+template <typename T, int MODE, typename V>
+void amg_mv_v(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const T* b,
+              const T* dinv, T* y, PcgScalars* S, cudaStream_t s, T w, const T* xs) {
+  if constexpr (MODE == kResid) {  // only the folded residual scales its gathers
+    if (xs) {
+      amg_mv_vx<T, MODE, V, true>(M, view, v, x, b, dinv, y, S, s, w, xs);
+      return;
+    }
+  }
+  amg_mv_vx<T, MODE, V, false>(M, view, v, x, b, dinv, y, S, s, w, nullptr);
 }
 
 // y (mode) A x; xs (optional) scales the gathered x elementwise.
@@ -994,10 +1007,10 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
     GIPB_TRY(L.t.alloc((size_t)A.nr));
     if (H.l > 0) {  // level 0 runs on the solver's own operator
       GIPB_TRY(L.b.alloc((size_t)A.nr));
-      // the FP32 cycle stores its long-row coarse operators compactly where they fit
-      // (GIPB200_AMG_COARSE_HALF=1: their values in FP16 as well)
+      // GIPB200_AMG_COMPACT=1: 16-bit columns where they fit; GIPB200_AMG_COARSE_HALF=1:
+      // FP16 values (both off: measured no faster)
       GIPB_TRY(upload(A, &L.A, s, std::is_same<T, float>::value && getenv("GIPB200_AMG_COARSE_HALF"),
-                      !getenv("GIPB200_AMG_WIDE")));
+                      getenv("GIPB200_AMG_COMPACT") != nullptr));
     }
     nnz_all += (double)A.nnz();
     if (H.cinv) {
@@ -1008,7 +1021,9 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
       // the FP32 cycle keeps its transfer operators in FP16 (R = P^T still holds exactly:
       // both round the same values), halving their value stream
       const bool half = std::is_same<T, float>::value;
-      const bool compact = !getenv("GIPB200_AMG_WIDE");
+      // (GIPB200_AMG_COMPACT=1: 16-bit columns where they fit; measured no faster for the
+      // CSR operators and slower for the sliced prolongation, 191 against 163 us)
+      const bool compact = getenv("GIPB200_AMG_COMPACT") != nullptr;
       GIPB_TRY(upload(*H.P, &L.P, s, half, compact));
       if (H.l == 0 && getenv("GIPB200_AMG_AGG_ORDER")) {
         // GIPB200_AMG_AGG_ORDER=1: level 0's residual is written in aggregate order (the
@@ -1086,8 +1101,8 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     const T* b = l == 0 ? r : V.b.p;
     const double n = V.n, nn = lv[l + 1]->n;
     const bool skip = l == 0 && u0;
-    // levels >= 1 gather D^-1 b where they would gather the Jacobi start x = D^-1 b
-    const bool fold = l > 0 && fold_coarse;
+    // small levels >= 1 gather D^-1 b where they would gather the Jacobi start x = D^-1 b
+    const bool fold = folds(l);
     if (!skip && !fold) {
       GIPB_TRY(mark(l, GIPB200_CYCLE_JACOBI0, 3.0 * n * w));
       launch_dep(k_amg_jacobi0<T>, vec_blocks(V.n), 256, s, V.n, (const T*)V.dinv.p, b, V.x.p, S);
@@ -1103,8 +1118,10 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
         launch_dep(k_amg_spmv<T, kResid, T, false>, bs, 256, s, A0, skip ? r : (const T*)V.x.p,
                    b, (const T*)nullptr, V.t.p, S, skip ? (T)omega0 : T(1), (const int*)perm0.p,
                    (const T*)nullptr, (const unsigned short*)nullptr, (const int*)nullptr);
-    } else {  // t = b - A (D^-1 b)
+    } else if (fold) {  // t = b - A (D^-1 b)
       amg_mv<T, kResid>(V.A, b, b, (const T*)nullptr, V.t.p, S, s, T(1), V.dinv.p);
+    } else {  // t = b - A x
+      amg_mv<T, kResid>(V.A, V.x.p, b, (const T*)nullptr, V.t.p, S, s);
     }
     GIPB_TRY(mark(l, GIPB200_CYCLE_RESTRICT, stream_bytes(V.R) + (n + nn) * w));
     amg_mv<T, kPlain>(V.R, V.t.p, (const T*)nullptr, (const T*)nullptr, lv[l + 1]->b.p, S, s);
@@ -1119,7 +1136,7 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     const T* xc = (l + 1 == L - 1) ? lv[l + 1]->x.p : lv[l + 1]->t.p;
     const double n = V.n, nn = lv[l + 1]->n;
     const bool skip = l == 0 && u0;
-    const bool fold = l > 0 && fold_coarse;
+    const bool fold = folds(l);
     GIPB_TRY(mark(l, GIPB200_CYCLE_PROLONG,
                   stream_bytes(V.P) + (nn + (fold ? 3.0 : 2.0) * n) * w));
     if (skip)  // x0 = omega0 r + P x1
@@ -1156,7 +1173,7 @@ double AmgT<T>::cycle_bytes(double a0_stream_bytes) const {
     const double n = V.n, nn = lv[l + 1]->n;
     const double a = l == 0 ? a0_stream_bytes : stream_bytes(V.A);
     const bool skip = l == 0 && unit0;                   // x0 = omega0 r not formed
-    const bool fold = l > 0 && fold_coarse;              // x = D^-1 b formed where gathered
+    const bool fold = folds(l);                          // x = D^-1 b formed where gathered
     if (!skip && !fold) b += 3.0 * n * w;                // x = dinv b
     b += a + (skip ? 2.0 : 3.0) * n * w;                 // t = b - A x
     if (l == 0 && perm0.p) b += 4.0 * n;                 // its aggregate-order positions

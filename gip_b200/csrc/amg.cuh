@@ -84,9 +84,14 @@ struct AmgT {
   // gathers r and scales the product) and reads no diagonal.  A fixed symmetric smoother
   // like the per-row one, so the cycle stays a symmetric positive definite operator.
   bool unit0 = false;
-  // levels >= 1 fold their Jacobi start x = D^-1 b into the kernels that gather it
-  // (GIPB200_AMG_NO_FOLD=1: a separate kernel forms it)
+  // Levels >= 1 of at most kFoldRows unknowns fold their Jacobi start x = D^-1 b into the
+  // kernels that gather it (GIPB200_AMG_NO_FOLD=1: a separate kernel forms it everywhere).
+  // On small levels the saved launch wins; on a level of millions of unknowns the second
+  // gather per nonzero costs more than the separate pass (24 against 10 us on the 2.1M
+  // unknowns of the 256^3 cavity's level 1).
+  static constexpr int kFoldRows = 1 << 19;
   bool fold_coarse = getenv("GIPB200_AMG_NO_FOLD") == nullptr;
+  bool folds(int l) const { return l > 0 && fold_coarse && lv[l]->n <= kFoldRows; }
   double omega0 = 0.0;
   // Level 0's residual position in aggregate order (empty: written in row order); the
   // level-0 restriction's columns are numbered in that order.

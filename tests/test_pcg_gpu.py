@@ -237,11 +237,11 @@ def test_amg_compact_coarse_operators(gpu, monkeypatch, coarse_half):
     L, b = cavity.poisson_problem(48, seed=9)
     A = dv.DeviceMatrix(L)
     its = {}
-    if coarse_half:
-        monkeypatch.setenv("GIPB200_AMG_COARSE_HALF", "1")
-    for wide in ("0", "1"):
-        if wide == "1":
-            monkeypatch.setenv("GIPB200_AMG_WIDE", "1")
+    for wide in ("1", "0"):
+        if wide == "0":  # the compact forms (opt-in)
+            monkeypatch.setenv("GIPB200_AMG_COMPACT", "1")
+            if coarse_half:
+                monkeypatch.setenv("GIPB200_AMG_COARSE_HALF", "1")
         S = dv.PcgSolver(A, mode="mixed", maxit=2000, tol=1e-8, inner_tol=1e-2, max_outer=100,
                          precond="amg")
         x = _t(np.zeros(L.nrows))
