@@ -164,6 +164,13 @@ int Batch::layout(cudaStream_t s) {
     d.cta0 = c;
     d.ncta = ncta[i];
     d.count_launch = (i == 0) ? 1 : 0;
+    const PackedView pk = P.packed();
+    d.pk_nib = pk.on ? pk.nib : 0;
+    d.pk_delta = pk.delta;
+    d.pk_idx = pk.idx;
+    d.pk_base = pk.base;
+    d.pk_plain = pk.plain;
+    d.pk_table = pk.table;
     for (int k = 0; k < ncta[i]; ++k) owner[c + k] = i;
     c += ncta[i];
   }

@@ -196,6 +196,32 @@ __device__ __forceinline__ void rows_dir(const SellView<float>& A, const float* 
   }
 }
 
+// One slice's rows of the packed FP32 operator times p = r + beta p_in, in the FMA order
+// of the single-instance packed kernel (all eight slots: an unused eighth slot adds
+// x * 0.0f, which leaves the sum unchanged); slices stored plain use the sliced layout.
+template <int NIB>
+__device__ __forceinline__ float row_dir_packed(const BatchSolve& B, const float* tab,
+                                                const float* r, const float* pin, float beta,
+                                                int s, int lane) {
+  PackedWords w;
+  packed_words<NIB>(B.pk_delta, B.pk_idx, B.pk_plain, s, lane, w);
+  int c[8];
+  packed_cols(B.pk_base, s, w.d, c);
+  if (w.plain) {
+    const int ss[1] = {s};
+    float sm[1];
+    rows_dir<1>(B.A, r, pin, beta, ss, lane, sm);
+    return sm[0];
+  }
+  float xv[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) xv[j] = fmaf(beta, __ldcg(pin + c[j]), __ldcg(r + c[j]));
+  float sum = 0.f;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) sum = fmaf(xv[j], tab[packed_index<NIB>(w, j)], sum);
+  return sum;
+}
+
 __device__ __forceinline__ float pick(const float4& a, int k) {
   return k == 0 ? a.x : k == 1 ? a.y : k == 2 ? a.z : a.w;
 }
@@ -283,6 +309,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_batch_pcg(const BatchSolve* _
   __shared__ BatchSolve B;
   __shared__ SolveState T;
   __shared__ double sh[kBatchWidth][32];
+  __shared__ float tab[256];  // the packed operator's value table
   __shared__ int s_ok;
   const int g = owner[blockIdx.x];
   if (g < 0) return;  // an idle CTA (the groups do not fill the grid)
@@ -292,6 +319,8 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_batch_pcg(const BatchSolve* _
     T.status = GIPB200_OK;
   }
   __syncthreads();
+  if (B.pk_nib)
+    for (int t = threadIdx.x; t < (1 << B.pk_nib); t += BS) tab[t] = B.pk_table[t];
   Group G{B.bar, B.part, (int)blockIdx.x - B.cta0, B.ncta, 0u, 0};
   const int lane = threadIdx.x & 31;
   const int gw = G.rank * (BS / 32) + (threadIdx.x >> 5), nw = G.ncta * (BS / 32);
@@ -321,12 +350,23 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_batch_pcg(const BatchSolve* _
     {
       const float bf = (float)T.beta;
       double acc[1] = {0.0};
+      const int nib = B.pk_nib;
       for (int s0 = gw; s0 < B.A.nslices; s0 += SPW * nw) {
         int s[SPW];
 #pragma unroll
         for (int u = 0; u < SPW; ++u) s[u] = s0 + u * nw;
         float sum[SPW];
-        rows_dir<SPW>(B.A, B.r, pin_v, bf, s, lane, sum);
+        if (nib == 4) {
+#pragma unroll
+          for (int u = 0; u < SPW; ++u)
+            sum[u] = s[u] < B.A.nslices ? row_dir_packed<4>(B, tab, B.r, pin_v, bf, s[u], lane) : 0.f;
+        } else if (nib == 8) {
+#pragma unroll
+          for (int u = 0; u < SPW; ++u)
+            sum[u] = s[u] < B.A.nslices ? row_dir_packed<8>(B, tab, B.r, pin_v, bf, s[u], lane) : 0.f;
+        } else {
+          rows_dir<SPW>(B.A, B.r, pin_v, bf, s, lane, sum);
+        }
 #pragma unroll
         for (int u = 0; u < SPW; ++u) {
           const int i = s[u] * 32 + lane;

@@ -31,6 +31,13 @@ struct BatchSolve {
   int n, n_all, maxit, max_outer, pin_row;
   int cta0, ncta;       // the instance's CTAs: [cta0, cta0 + ncta)
   int count_launch;     // 1 on the instance whose step history counts the launch
+  // the packed FP32 operator (pk_nib = 4 or 8; 0: the plain sliced layout only)
+  int pk_nib;
+  const uint4* pk_delta;
+  const void* pk_idx;
+  const int* pk_base;
+  const unsigned char* pk_plain;
+  const float* pk_table;
 };
 
 // Launch shape of the persistent kernel: threads per CTA (128, 256 or 512) and rows per
