@@ -12,7 +12,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstddef>
+#include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "device.cuh"
@@ -664,10 +666,31 @@ double* Dns::field(const std::string& name, int* n) {
 }
 
 // ------------------------------------------------------------------ locality renumbering
+// A std::allocator whose value-initialising construct() leaves the element uninitialised
+// (renumbered operators are filled in parallel right after allocation).
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+  template <typename U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <typename U>
+  NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+  template <typename U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... Args>
+  void construct(U* p, Args&&... args) {
+    ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...);
+  }
+};
+
 struct OwnedCsr {
   int nrows = 0, ncols = 0;
-  std::vector<int> rp, col;
-  std::vector<double> val;
+  std::vector<int, NoInitAlloc<int>> rp, col;
+  std::vector<double, NoInitAlloc<double>> val;
   gipb200_host_csr view() const {
     gipb200_host_csr h;
     h.nrows = nrows;
@@ -719,8 +742,11 @@ static void permute_rows(const gipb200_host_csr& m, const int* src, const int* c
                          OwnedCsr* out) {
   out->nrows = m.nrows;
   out->ncols = m.ncols;
-  out->rp.assign((size_t)m.nrows + 1, 0);
-  for (int r = 0; r < m.nrows; ++r) out->rp[r + 1] = out->rp[r] + (m.rowptr[src[r] + 1] - m.rowptr[src[r]]);
+  out->rp.resize((size_t)m.nrows + 1);
+  out->rp[0] = 0;
+#pragma omp parallel for schedule(static)
+  for (int r = 0; r < m.nrows; ++r) out->rp[r + 1] = m.rowptr[src[r] + 1] - m.rowptr[src[r]];
+  for (int r = 0; r < m.nrows; ++r) out->rp[r + 1] += out->rp[r];
   out->col.resize((size_t)m.nnz);
   out->val.resize((size_t)m.nnz);
 #pragma omp parallel for schedule(static)
