@@ -805,21 +805,29 @@ static int build_ec_slot(Dns& E, const gipb200_host_csr& D, const gipb200_host_c
   const long long nslots = sptr[ns];
   if (nslots > 0x7ffffffeLL) return GIPB200_OK;
   std::vector<int> src((size_t)nslots, -1);  // slot -> Ec row (the CSR nonzero of D)
+#pragma omp parallel for schedule(static)
   for (int r = 0; r < D.nrows; ++r)
     for (int k = D.rowptr[r]; k < D.rowptr[r + 1]; ++k)
       src[(size_t)(sptr[r >> 5] + 32LL * (k - D.rowptr[r]) + (r & 31))] = k;
-  std::vector<int> rp((size_t)nslots + 1, 0), col;
-  std::vector<double> val;
-  col.reserve((size_t)Ec.nnz);
-  val.reserve((size_t)Ec.nnz);
+  // row lengths (in parallel), offsets, entries (in parallel)
+  std::vector<int> rp((size_t)nslots + 1, 0);
+#pragma omp parallel for schedule(static)
   for (long long t = 0; t < nslots; ++t) {
     const int k = src[(size_t)t];
-    if (k >= 0)
-      for (int e = Ec.rowptr[k]; e < Ec.rowptr[k + 1]; ++e) {
-        col.push_back(Ec.col[e]);
-        val.push_back(Ec.val[e]);
-      }
-    rp[(size_t)t + 1] = (int)col.size();
+    rp[(size_t)t + 1] = k >= 0 ? Ec.rowptr[k + 1] - Ec.rowptr[k] : 0;
+  }
+  for (long long t = 0; t < nslots; ++t) rp[(size_t)t + 1] += rp[(size_t)t];
+  std::vector<int, NoInitAlloc<int>> col((size_t)rp[(size_t)nslots]);
+  std::vector<double, NoInitAlloc<double>> val((size_t)rp[(size_t)nslots]);
+#pragma omp parallel for schedule(static)
+  for (long long t = 0; t < nslots; ++t) {
+    const int k = src[(size_t)t];
+    if (k < 0) continue;
+    int o = rp[(size_t)t];
+    for (int e = Ec.rowptr[k]; e < Ec.rowptr[k + 1]; ++e, ++o) {
+      col[(size_t)o] = Ec.col[e];
+      val[(size_t)o] = Ec.val[e];
+    }
   }
   GIPB_TRY(E.ec_rp.upload(rp.data(), rp.size(), 0));
   GIPB_TRY(E.ec_col.upload(col.data(), std::max<size_t>(col.size(), 1), 0));
@@ -835,27 +843,43 @@ static int build_ec_slot(Dns& E, const gipb200_host_csr& D, const gipb200_host_c
 static int build_face3(FaceOps3* F, const gipb200_host_csr* const op[3], int NF, int NO) {
   F->on = false;
   if (NF <= 0 || getenv("GIPB200_NO_FACE3")) return GIPB200_OK;
-  std::vector<int> rp((size_t)NF + 1, 0), col;
-  std::vector<double> val;
+  // counts per face (in parallel), offsets, then the entries (in parallel)
+  std::vector<int> rp((size_t)NF + 1, 0);
   std::vector<unsigned short> cnt((size_t)NF, 0);
-  bool single = true;
+  int too_long = 0, mixed = 0;
+#pragma omp parallel for schedule(static) reduction(| : too_long, mixed)
   for (int f = 0; f < NF; ++f) {
     unsigned packed = 0, ops_here = 0;
+    int total = 0;
     for (int o = 0; o < 3; ++o) {
       const gipb200_host_csr& m = *op[o];
       if (f >= m.nrows) continue;
       const int c = m.rowptr[f + 1] - m.rowptr[f];
-      if (c > 15) return GIPB200_OK;
-      packed |= (unsigned)c << (4 * o);
+      if (c > 15) too_long = 1;
+      packed |= (unsigned)(c & 15) << (4 * o);
       ops_here += c > 0 ? 1u : 0u;
-      for (int k = m.rowptr[f]; k < m.rowptr[f + 1]; ++k) {
-        col.push_back(m.col[k]);
-        val.push_back(m.val[k]);
-      }
+      total += c;
     }
     cnt[f] = (unsigned short)packed;
-    rp[f + 1] = (int)col.size();
-    single = single && ops_here <= 1;
+    rp[(size_t)f + 1] = total;
+    if (ops_here > 1) mixed = 1;
+  }
+  if (too_long) return GIPB200_OK;
+  const bool single = !mixed;
+  for (int f = 0; f < NF; ++f) rp[(size_t)f + 1] += rp[f];
+  std::vector<int, NoInitAlloc<int>> col((size_t)rp[NF]);
+  std::vector<double, NoInitAlloc<double>> val((size_t)rp[NF]);
+#pragma omp parallel for schedule(static)
+  for (int f = 0; f < NF; ++f) {
+    int o2 = rp[f];
+    for (int o = 0; o < 3; ++o) {
+      const gipb200_host_csr& m = *op[o];
+      if (f >= m.nrows) continue;
+      for (int k = m.rowptr[f]; k < m.rowptr[f + 1]; ++k, ++o2) {
+        col[(size_t)o2] = m.col[k];
+        val[(size_t)o2] = m.val[k];
+      }
+    }
   }
   GIPB_TRY(sell_build(&F->S, NF, NO, (int)col.size(), rp.data(), col.data(), val.data(), 0, 0u));
   GIPB_TRY(F->cnt.upload(cnt.data(), cnt.size(), 0));
