@@ -356,7 +356,8 @@ bool dense_inverse(int m, std::vector<double>& M, std::vector<double>& inv) {
 // compact: a long-row (CSR) operator whose rows each span at most 65536 columns is stored
 // with 16-bit offsets from each row's smallest column (the FP32 cycle); half: FP16 values.
 template <typename T>
-int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool compact = false) {
+int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool compact = false,
+           bool transfer = false) {
   S->half = half;
   GIPB_TRY(validate_csr(A.nr, A.nc, (int)A.nnz(), A.rp.data(), A.ci.data(), A.nc, "AMG operator"));
   S->nrows = A.nr;
@@ -365,10 +366,13 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool c
   S->nslices = (A.nr + 31) / 32;
   const double avg = (double)A.nnz() / std::max(A.nr, 1);
   if (avg >= 12.0) {  // long rows: CSR, 4 to 32 threads per row
-    // FP32 cycle: as few threads per row as cover its entries in one pass (4 threads x 8
-    // entries, 8 x 4, ...), so that a warp works on more rows per dependent round trip;
-    // GIPB200_AMG_WIDE_ROWS=1 (and the FP64 cycle): 8 to 32 threads per row
-    const bool narrow = std::is_same<T, float>::value && !getenv("GIPB200_AMG_WIDE_ROWS");
+    // FP32 cycle's transfer operators (FP16 values): as few threads per row as cover its
+    // entries in one pass (4 threads x 8 entries, 8 x 4, ...), so that a warp works on more
+    // rows per dependent round trip (restriction of the 256^3 cavity: 128 against 153 us);
+    // coarse operators (FP32 values, where the narrow form measured 107 against 90 us),
+    // the FP64 cycle and GIPB200_AMG_WIDE_ROWS=1: 8 to 32 threads per row
+    const bool narrow = std::is_same<T, float>::value && transfer &&
+                        !getenv("GIPB200_AMG_WIDE_ROWS");
     S->lanes = narrow ? (avg < 32.0 ? 4 : avg < 64.0 ? 8 : avg < 128.0 ? 16 : 32)
                       : (avg >= 48.0 ? 32 : avg >= 24.0 ? 16 : 8);
     GIPB_TRY(S->rp.upload(A.rp.data(), A.rp.size(), s));
@@ -1024,7 +1028,7 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
       // (GIPB200_AMG_COMPACT=1: 16-bit columns where they fit; measured no faster for the
       // CSR operators and slower for the sliced prolongation, 191 against 163 us)
       const bool compact = getenv("GIPB200_AMG_COMPACT") != nullptr;
-      GIPB_TRY(upload(*H.P, &L.P, s, half, compact));
+      GIPB_TRY(upload(*H.P, &L.P, s, half, compact, true));
       if (H.l == 0 && getenv("GIPB200_AMG_AGG_ORDER")) {
         // GIPB200_AMG_AGG_ORDER=1: level 0's residual is written in aggregate order (the
         // rows of aggregate 0, then of aggregate 1, ..., each in row order), and the
@@ -1047,10 +1051,10 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
             Rp.v[k] = e[k - Rp.rp[j]].second;
           }
         }
-        GIPB_TRY(upload(Rp, &L.R, s, half, compact));
+        GIPB_TRY(upload(Rp, &L.R, s, half, compact, true));
         GIPB_TRY(perm0.upload(perm.data(), perm.size(), s));
       } else {
-        GIPB_TRY(upload(*H.R, &L.R, s, half, compact));
+        GIPB_TRY(upload(*H.R, &L.R, s, half, compact, true));
       }
     }
     lv.push_back(std::move(Lp));

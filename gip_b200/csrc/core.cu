@@ -122,7 +122,7 @@ int sell_build(Sell* S, int nrows, int ncols, int nnz, const int* rp, const int*
   S->rows_nonempty = nonempty;
   S->nslots = sptr[S->nslices];
   S->uslots = 0;
-  if (S->nslices > 0 && S->nslots > 0) {
+  if (S->nslices > 0 && S->nslots > 0 && !getenv("GIPB200_NO_UNIFORM")) {
     const long long l0 = sptr[1] - sptr[0];
     bool uniform = true;
     for (int s = 1; s < S->nslices && uniform; ++s) uniform = sptr[s + 1] - sptr[s] == l0;

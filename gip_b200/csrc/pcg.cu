@@ -533,14 +533,16 @@ __global__ void __launch_bounds__(256, 8) k_mxp_spmv_dot(SellView<float> A,
   double acc[1] = {0.0};
   PackedWords cur;
   for (int s = gw; s < A.nslices; s += nw) {
+    // (the slot bases after the plain test: hoisted with the words, as the V-cycle's
+    // packed kernel has them, this kernel measured 150 against 138 us)
     packed_words<NIB>(delta, idx, plain, s, lane, cur);
-    int c[8];
-    packed_cols(base, s, cur.d, c);
     const int i = s * 32 + lane;
     float sum;
     if (cur.plain) {  // rare fallback: few registers
       sum = REC ? sell_row_f32<2>(A, r, s, lane) : sell_row_dir<2>(A, r, pin, beta, s, lane);
     } else {
+      int c[8];
+      packed_cols(base, s, cur.d, c);
       float xv[K];
 #pragma unroll
       for (int j = 0; j < K; ++j)
