@@ -134,7 +134,7 @@ _SIGNATURES = {
     "gipb200_batch_destroy": (_I, [_VP]),
     "gipb200_batch_instance": (_I, [_VP, _I, C.POINTER(_VP)]),
     "gipb200_batch_advance": (_I, [_VP, _I, _VP]),
-    "gipb200_batch_set_solver": (_I, [_VP, _I, _I, _I]),
+    "gipb200_batch_set_solver": (_I, [_VP, _I, _I, _I, _I]),
     "gipb200_batch_balance": (_I, [_VP, _VP]),
     "gipb200_batch_layout": (_I, [_VP, C.POINTER(_I), _VP]),
     "gipb200_batch_solver_status": (_I, [_VP, _VP, C.POINTER(_I)]),

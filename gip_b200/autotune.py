@@ -11,8 +11,9 @@ grid, and keeps the fastest of each.  The slice height (32 rows, one warp) and t
 (kernel, rows, nnz) in memory and, if ``path`` is given, in a JSON file.
 
 For a batch solved by the persistent launch (``tune_batch``) the tuner times whole batch
-steps for each launch shape -- threads per CTA (128, 256, 512) and rows per warp pass (32:
-one slice per warp; 64: two slices interleaved) -- keeps the fastest, then re-splits the
+steps for each launch shape -- threads per CTA (128, 256, 512), rows per warp pass (32:
+one slice per warp; 64: two slices in flight) and resident threads per SM (1024 or 1536,
+the register budget the kernel is compiled for) -- keeps the fastest, then re-splits the
 CTAs by the measured work (rows times the iterations of the last steps) and keeps that
 split if it is faster.
 """
@@ -71,7 +72,7 @@ def tune(engine, kernel: str = "mixed", rows: int = 0, nnz: int = 0,
     return dict(out, cached=False, ms=timings)
 
 
-BATCH_SHAPES = ((128, 32), (256, 32), (512, 32), (128, 64), (256, 64), (512, 64))
+BATCH_SHAPES = tuple((b, r, o) for o in (1024, 1536) for r in (32, 64) for b in (128, 256, 512))
 
 
 def tune_batch(batch, stream, shapes: Sequence = BATCH_SHAPES, steps: int = 2) -> dict:
@@ -89,9 +90,9 @@ def tune_batch(batch, stream, shapes: Sequence = BATCH_SHAPES, steps: int = 2) -
         return e0.elapsed_time(e1) / steps
 
     ms = {}
-    for block, rpw in shapes:
-        batch.set_solver(True, block, rpw)
-        ms[(block, rpw)] = timed()
+    for shape in shapes:
+        batch.set_solver(True, *shape)
+        ms[tuple(shape)] = timed()
     best = min(ms, key=ms.get)
     batch.set_solver(True, *best)
     t_default = timed()
@@ -104,7 +105,9 @@ def tune_batch(batch, stream, shapes: Sequence = BATCH_SHAPES, steps: int = 2) -
     balanced = t_measured < t_default
     if not balanced:
         batch.balance(None)
-    return {"block": best[0], "rows_per_warp": best[1], "balanced_by_iterations": balanced,
+    return {"block": best[0], "rows_per_warp": best[1],
+            "threads_per_sm": best[2] if len(best) > 2 else 1024,
+            "balanced_by_iterations": balanced,
             "weights": weights.tolist() if balanced else None,
-            "ms": {f"{b}x{r}": round(v, 3) for (b, r), v in ms.items()},
+            "ms": {"x".join(str(v) for v in k): round(t, 3) for k, t in ms.items()},
             "ms_default_split": round(t_default, 3), "ms_measured_split": round(t_measured, 3)}

@@ -270,7 +270,8 @@ int gipb200_batch_advance(gipb200_batch H, int nsteps, void* stream) {
   return GIPB200_OK;
 }
 
-int gipb200_batch_set_solver(gipb200_batch H, int persistent, int block, int rows_per_warp) {
+int gipb200_batch_set_solver(gipb200_batch H, int persistent, int block, int rows_per_warp,
+                             int threads_per_sm) {
   if (!H) return fail(GIPB200_ERR_ARG, "null batch");
   Batch& B = H->B;
   if (!persistent) {
@@ -281,8 +282,11 @@ int gipb200_batch_set_solver(gipb200_batch H, int persistent, int block, int row
   BatchShape sh;
   sh.block = block;
   sh.rows_per_warp = rows_per_warp;
+  sh.threads_per_sm = threads_per_sm > 0 ? threads_per_sm : 1024;
   if (!batch_shape_valid(sh))
-    return fail(GIPB200_ERR_ARG, "block must be 128, 256 or 512 and rows_per_warp 32 or 64");
+    return fail(GIPB200_ERR_ARG,
+                "block must be 128, 256 or 512, rows_per_warp 32 or 64, threads_per_sm 1024 "
+                "or 1536");
   for (size_t i = 0; i < B.inst.size(); ++i) {
     const Pcg& P = B.inst[i]->E.pcg;
     if (P.prm.mode != GIPB200_PCG_MIXED || P.prm.precond != GIPB200_PRECOND_JACOBI)

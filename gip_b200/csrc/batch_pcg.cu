@@ -302,8 +302,8 @@ __device__ __forceinline__ void residual_finish(const BatchSolve& B, SolveState&
   }
 }
 
-template <int BS, int SPW>
-__global__ void __launch_bounds__(BS, 1024 / BS) k_batch_pcg(const BatchSolve* __restrict__ inst,
+template <int BS, int SPW, int OCC>
+__global__ void __launch_bounds__(BS, OCC / BS) k_batch_pcg(const BatchSolve* __restrict__ inst,
                                                              const int* __restrict__ owner,
                                                              int* __restrict__ err) {
   __shared__ BatchSolve B;
@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_batch_pcg(const BatchSolve* _
   // r = b - L x with the pin split; false when a barrier gave up
   auto residual = [&](int first) -> bool {
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    residual_rows<SPW>(B, first, gw, nw, acc);
+    residual_rows<1>(B, first, gw, nw, acc);  // rare (replacements): one slice a pass
     if (!group_sum<5>(acc, G, sh, &s_ok)) return false;
     if (lead) residual_finish(B, T, first, G.rank, acc);
     __syncthreads();
@@ -476,10 +476,10 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_batch_pcg(const BatchSolve* _
   }
 }
 
-template <int BS, int SPW>
+template <int BS, int SPW, int OCC>
 int launch_variant(int grid, const BatchSolve* inst, const int* owner, int* err, cudaStream_t s,
                    int* capacity) {
-  auto kern = k_batch_pcg<BS, SPW>;
+  auto kern = k_batch_pcg<BS, SPW, OCC>;
   if (capacity) {
     DeviceInfo di;
     GIPB_TRY(device_info(&di));
@@ -505,17 +505,29 @@ int launch_variant(int grid, const BatchSolve* inst, const int* owner, int* err,
 int dispatch(const BatchShape& sh, int grid, const BatchSolve* inst, const int* owner, int* err,
              cudaStream_t s, int* capacity) {
   const int spw = sh.rows_per_warp / 32;
-  switch (sh.block * 4 + spw) {
-    case 128 * 4 + 1: return launch_variant<128, 1>(grid, inst, owner, err, s, capacity);
-    case 128 * 4 + 2: return launch_variant<128, 2>(grid, inst, owner, err, s, capacity);
-    case 256 * 4 + 1: return launch_variant<256, 1>(grid, inst, owner, err, s, capacity);
-    case 256 * 4 + 2: return launch_variant<256, 2>(grid, inst, owner, err, s, capacity);
-    case 512 * 4 + 1: return launch_variant<512, 1>(grid, inst, owner, err, s, capacity);
-    case 512 * 4 + 2: return launch_variant<512, 2>(grid, inst, owner, err, s, capacity);
+  const int key = (sh.threads_per_sm == 1536 ? 100000 : 0) + sh.block * 4 + spw;
+#define GIPB_BP(BS, SPW, OCC) \
+  case (OCC == 1536 ? 100000 : 0) + BS * 4 + SPW: \
+    return launch_variant<BS, SPW, OCC>(grid, inst, owner, err, s, capacity)
+  switch (key) {
+    GIPB_BP(128, 1, 1024);
+    GIPB_BP(128, 2, 1024);
+    GIPB_BP(256, 1, 1024);
+    GIPB_BP(256, 2, 1024);
+    GIPB_BP(512, 1, 1024);
+    GIPB_BP(512, 2, 1024);
+    GIPB_BP(128, 1, 1536);
+    GIPB_BP(128, 2, 1536);
+    GIPB_BP(256, 1, 1536);
+    GIPB_BP(256, 2, 1536);
+    GIPB_BP(512, 1, 1536);
+    GIPB_BP(512, 2, 1536);
     default:
-      return fail(GIPB200_ERR_ARG, "unsupported batch shape: block %d, rows per warp %d",
-                  sh.block, sh.rows_per_warp);
+      return fail(GIPB200_ERR_ARG,
+                  "unsupported batch shape: block %d, rows per warp %d, threads per SM %d",
+                  sh.block, sh.rows_per_warp, sh.threads_per_sm);
   }
+#undef GIPB_BP
 }
 
 }  // namespace
@@ -560,7 +572,8 @@ int batch_pcg_check_timeout(cudaStream_t s, int* h_status) {
 
 bool batch_shape_valid(const BatchShape& sh) {
   return (sh.block == 128 || sh.block == 256 || sh.block == 512) &&
-         (sh.rows_per_warp == 32 || sh.rows_per_warp == 64);
+         (sh.rows_per_warp == 32 || sh.rows_per_warp == 64) &&
+         (sh.threads_per_sm == 1024 || sh.threads_per_sm == 1536);
 }
 
 int batch_pcg_capacity(const BatchShape& sh, int* ctas) {

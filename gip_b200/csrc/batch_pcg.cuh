@@ -40,12 +40,13 @@ struct BatchSolve {
   const float* pk_table;
 };
 
-// Launch shape of the persistent kernel: threads per CTA (128, 256 or 512) and rows per
-// warp pass (32: one slice of 32 rows per warp; 64: two slices interleaved, twice the
-// gathers in flight).
+// Launch shape of the persistent kernel: threads per CTA (128, 256 or 512), rows per
+// warp pass (32: one slice of 32 rows per warp; 64: two slices in flight) and resident
+// threads per SM it is compiled for (1024: 64 registers a thread; 1536: 40, a few spilled).
 struct BatchShape {
   int block = 256;
   int rows_per_warp = 32;
+  int threads_per_sm = 1024;
 };
 
 bool batch_shape_valid(const BatchShape& sh);

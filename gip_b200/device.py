@@ -486,11 +486,12 @@ class DnsBatch:
     def advance(self, nsteps: int, stream=None) -> None:
         L.call("gipb200_batch_advance", self.handle, nsteps, _stream(stream))
 
-    def set_solver(self, persistent: bool, block: int = 256, rows_per_warp: int = 32) -> None:
+    def set_solver(self, persistent: bool, block: int = 256, rows_per_warp: int = 32,
+                   threads_per_sm: int = 1024) -> None:
         """Pressure solves in one persistent cooperative launch per step (every instance
         mixed with Jacobi) or, persistent=False, inside each instance's graph branch."""
         L.call("gipb200_batch_set_solver", self.handle, int(persistent), int(block),
-               int(rows_per_warp))
+               int(rows_per_warp), int(threads_per_sm))
 
     def balance(self, weights=None) -> None:
         """CTA shares of the persistent solve (None: rows x rows^(1/3))."""

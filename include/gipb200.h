@@ -422,9 +422,12 @@ int gipb200_batch_advance(gipb200_batch B, int nsteps, void* stream);
  * group per instance (shares set by gipb200_batch_balance); each group runs its instance's
  * mixed-form Jacobi-PCG and leaves when that instance has converged.  Needs every instance
  * in GIPB200_PCG_MIXED with GIPB200_PRECOND_JACOBI.  block: threads per CTA (128, 256 or
- * 512); rows_per_warp: 32 (one 32-row slice per warp pass) or 64 (two slices interleaved).
+ * 512); rows_per_warp: 32 (one 32-row slice per warp pass) or 64 (two slices in flight);
+ * threads_per_sm: 1024 (64 registers a thread) or 1536 (40; 0 = 1024), the occupancy the
+ * kernel is compiled for.
  * The step graph is captured again at the next advance. */
-int gipb200_batch_set_solver(gipb200_batch B, int persistent, int block, int rows_per_warp);
+int gipb200_batch_set_solver(gipb200_batch B, int persistent, int block, int rows_per_warp,
+                             int threads_per_sm);
 /* CTA shares of the persistent solve: weights[i] >= 0 is instance i's expected work (for
  * example rows times iterations of the last step); null restores the default, rows times
  * the cube root of rows (Jacobi-PCG iterations grow with the grid edge).  Waits for the

@@ -75,7 +75,7 @@ class FakeBatch:
         self.shape, self.weights = None, None
         self.instances = [self.Inst(1000, 50), self.Inst(8000, 120)]
 
-    def set_solver(self, persistent, block, rpw):
+    def set_solver(self, persistent, block, rpw, occ=1024):
         self.shape = (block, rpw)
 
     def balance(self, w):
@@ -108,11 +108,12 @@ def test_tune_batch_picks_shape_and_split(monkeypatch):
 
     fake_torch = types.SimpleNamespace(cuda=types.SimpleNamespace(Event=Ev))
     monkeypatch.setitem(__import__("sys").modules, "torch", fake_torch)
-    r = autotune.tune_batch(B, None, steps=2)
+    shapes = [(b, r, 1024) for (b, r) in ms]
+    r = autotune.tune_batch(B, None, shapes=shapes, steps=2)
     assert (r["block"], r["rows_per_warp"]) == (256, 64) and B.shape == (256, 64)
     assert r["balanced_by_iterations"] and B.weights == [1000 * 50.0, 8000 * 120.0]
     assert r["weights"] == [1000 * 50.0, 8000 * 120.0]
     B2 = FakeBatch(ms, 9.0)  # the measured split is slower: the default split is restored
     B = B2
-    r = autotune.tune_batch(B2, None, steps=2)
+    r = autotune.tune_batch(B2, None, shapes=shapes, steps=2)
     assert not r["balanced_by_iterations"] and B2.weights is None and r["weights"] is None

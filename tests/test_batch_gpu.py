@@ -39,8 +39,9 @@ def test_autotune_picks_a_grid(gpu):
     assert np.all(E.history()["massr"] < 1e-4)
 
 
-@pytest.mark.parametrize("block,rows_per_warp", [(256, 32), (128, 64), (512, 32)])
-def test_persistent_solve_matches_branch_solves(gpu, block, rows_per_warp):
+@pytest.mark.parametrize("block,rows_per_warp,occ", [(256, 32, 1024), (128, 64, 1024),
+                                                     (512, 32, 1536), (128, 64, 1536)])
+def test_persistent_solve_matches_branch_solves(gpu, block, rows_per_warp, occ):
     """The persistent launch (one CTA group per instance, the group's own convergence loop)
     against the same batch solving inside its graph branches: same algorithm (mixed
     Jacobi-PCG with reliable updates), so the steps agree to the solve's tolerance; every
@@ -53,7 +54,7 @@ def test_persistent_solve_matches_branch_solves(gpu, block, rows_per_warp):
     A = DnsBatch(cases, params)
     A.advance(5)
     B = DnsBatch(cases, params)
-    B.set_solver(True, block, rows_per_warp)
+    B.set_solver(True, block, rows_per_warp, occ)
     grid, ncta = B.layout()
     assert grid > 0 and ncta.min() >= 1 and ncta.sum() <= grid
     B.advance(5)
