@@ -1166,6 +1166,15 @@ static int add_while(cudaStream_t cs, cudaGraphConditionalHandle h, cudaGraph_t*
   return GIPB200_OK;
 }
 
+// Host-driven solves read the device's stop flag every 16 iterations (each read is a host
+// wait); GIPB200_HOST_POLL=k reads it every k (profiling: 1 leaves no finished-solve
+// launches in a launch list).
+static int host_poll_interval() {
+  const char* e = getenv("GIPB200_HOST_POLL");
+  const int k = e ? atoi(e) : 16;
+  return k > 0 ? k : 16;
+}
+
 int Pcg::enqueue(const double* b, double* x, const double* x0, cudaStream_t s, bool host_sync) {
   if (!host_sync && prm.mode != GIPB200_PCG_FIXED && capturing(s)) {
     if (!body_stream[0]) {
@@ -1318,7 +1327,7 @@ int Pcg::enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t
     GIPB_TRY(amg64->enqueue(L->view(), r.p, z64.p, sc.p, rs, 1, s));
     k_pcg_pupdate_z<<<blocks_vec, 256, 0, s>>>(n, p.p, z64.p, sc.p, 0, 0);
   }
-  const int poll = 16;
+  const int poll = host_poll_interval();
   for (int k = 0; k < prm.maxit; ++k) {
     k_pcg_spmv_dot<<<blocks_spmv, 256, 0, s>>>(L->view(), p.p, Ap.p, sc.p, rs, prm.mode);
     if (amg64) {
@@ -1388,7 +1397,7 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 0, 0));
   if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s, &pk0));
-  const int poll = 16;
+  const int poll = host_poll_interval();
   for (int k = 0; k < prm.maxit; ++k) {
     float* pin = (k & 1) ? p32b.p : p32.p;
     float* pout = (k & 1) ? p32.p : p32b.p;
