@@ -87,6 +87,7 @@ _SIGNATURES = {
     "gipb200_free": (_I, [_VP]),
     "gipb200_memcpy_h2d": (_I, [_VP, _VP, C.c_size_t, _VP]),
     "gipb200_memcpy_d2h": (_I, [_VP, _VP, C.c_size_t, _VP]),
+    "gipb200_memcpy_d2h_async": (_I, [_VP, _VP, C.c_size_t, _VP]),
     "gipb200_dcopy": (_I, [_I, _VP, _VP, _VP]),
     "gipb200_stream_sync": (_I, [_VP]),
     "gipb200_event_create": (_I, [C.POINTER(_VP)]),

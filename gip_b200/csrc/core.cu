@@ -416,6 +416,10 @@ int gipb200_memcpy_d2h(void* h, const void* d, size_t bytes, void* stream) {
   GIPB_CUDA(cudaStreamSynchronize(as_stream(stream)));
   return GIPB200_OK;
 }
+int gipb200_memcpy_d2h_async(void* h, const void* d, size_t bytes, void* stream) {
+  GIPB_CUDA(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, as_stream(stream)));
+  return GIPB200_OK;
+}
 int gipb200_dcopy(int n, double* d_dst, const double* d_src, void* stream) {
   if (n < 0) return fail(GIPB200_ERR_ARG, "negative size");
   if (n == 0) return GIPB200_OK;

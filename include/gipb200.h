@@ -53,6 +53,9 @@ int gipb200_free(void* d_ptr);
 int gipb200_memcpy_h2d(void* d_dst, const void* h_src, size_t bytes, void* stream);
 /* GIP_cudaMemcpyDToCpu / IToCpu (libgpu.cu:41-49) */
 int gipb200_memcpy_d2h(void* h_dst, const void* d_src, size_t bytes, void* stream);
+/* The same copy enqueued on `stream` without waiting for it (h_dst pinned for the copy to
+ * overlap work on other streams; read it after the stream has passed it). */
+int gipb200_memcpy_d2h_async(void* h_dst, const void* d_src, size_t bytes, void* stream);
 /* GIP_cudaDcopy (libgpu.cu:68-71): d_dst[0:n) = d_src[0:n) */
 int gipb200_dcopy(int n, double* d_dst, const double* d_src, void* stream);
 int gipb200_stream_sync(void* stream);
