@@ -365,7 +365,10 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool c
   S->nnz = A.nnz();
   S->nslices = (A.nr + 31) / 32;
   const double avg = (double)A.nnz() / std::max(A.nr, 1);
-  if (avg >= 12.0) {  // long rows: CSR, 4 to 32 threads per row
+  // rows of at least kCsrRows entries on average are CSR (GIPB200_AMG_CSR_ROWS overrides)
+  const char* csr_env = getenv("GIPB200_AMG_CSR_ROWS");
+  const double csr_rows = csr_env ? atof(csr_env) : 12.0;
+  if (avg >= csr_rows) {  // long rows: CSR, 4 to 32 threads per row
     // FP32 cycle's transfer operators (FP16 values): as few threads per row as cover its
     // entries in one pass (4 threads x 8 entries, 8 x 4, ...), so that a warp works on more
     // rows per dependent round trip (restriction of the 256^3 cavity: 128 against 153 us);
