@@ -32,20 +32,37 @@ __device__ __forceinline__ void dc_row(const SellView<double>& D, const double* 
   long long base;
   int len;
   slice_range(D, s, base, len);
-  for (int j = 0; j < len; ++j) {
-    const long long k = base + 32LL * j + lane;
-    const int c = ld_stream(D.col + k);
-    if (c < 0) continue;
-    const double dv = ld_stream(D.val + k);
-    const double cv = ld_stream(cval + k);
-    const double xu = __ldg(u + c), xv = __ldg(v + c), xw = __ldg(w + c);
-    sd[0] = dadd(sd[0], dmul(xu, dv));
-    sd[1] = dadd(sd[1], dmul(xv, dv));
-    sd[2] = dadd(sd[2], dmul(xw, dv));
-    sc[0] = dadd(sc[0], dmul(xu, cv));
-    sc[1] = dadd(sc[1], dmul(xv, cv));
-    sc[2] = dadd(sc[2], dmul(xw, cv));
-    any = true;
+  // two slots at a time: their columns and values, then their six gathers, are in flight
+  // together (two dependent round trips per pair instead of two per slot)
+  for (int j0 = 0; j0 < len; j0 += 2) {
+    int c[2];
+    double dv[2], cv[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const bool in = j0 + t < len;
+      const long long k = base + 32LL * (j0 + t) + lane;
+      c[t] = in ? ld_stream(D.col + k) : -1;
+      dv[t] = in ? ld_stream(D.val + k) : 0.0;
+      cv[t] = in ? ld_stream(cval + k) : 0.0;
+    }
+    double xu[2], xv[2], xw[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      xu[t] = c[t] >= 0 ? __ldg(u + c[t]) : 0.0;
+      xv[t] = c[t] >= 0 ? __ldg(v + c[t]) : 0.0;
+      xw[t] = c[t] >= 0 ? __ldg(w + c[t]) : 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      if (c[t] < 0) continue;
+      sd[0] = dadd(sd[0], dmul(xu[t], dv[t]));
+      sd[1] = dadd(sd[1], dmul(xv[t], dv[t]));
+      sd[2] = dadd(sd[2], dmul(xw[t], dv[t]));
+      sc[0] = dadd(sc[0], dmul(xu[t], cv[t]));
+      sc[1] = dadd(sc[1], dmul(xv[t], cv[t]));
+      sc[2] = dadd(sc[2], dmul(xw[t], cv[t]));
+      any = true;
+    }
   }
 }
 
