@@ -564,22 +564,18 @@ enum { kResid = 0, kPlain = 1, kAdd = 2, kSmooth = 3, kScaleAdd = 4, kDiagAdd = 
 // kResid: y = b - A x;  kPlain: y = A x;  kAdd: y += A x;  kSmooth: y = x + dinv (b - A x);
 // kScaleAdd: y = w b + A x (the level-0 prolongation onto x0 = w r, never formed)
 // C16: 16-bit slot columns (dcol, offsets from the row's base column cbase[row]).
+// The rows of slices gw, gw + nw, ... (warp gw of nw).
 template <typename T, int MODE, typename V = T, bool C16 = false, bool XS = false>
-__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 6 : 8) k_amg_spmv(SellView<V> A, const T* __restrict__ x,
-                                                     const T* __restrict__ b,
-                                                     const T* __restrict__ dinv,
-                                                     T* __restrict__ y, PcgScalars* S, T w,
-                                                     const int* __restrict__ yperm,
-                                                     const T* __restrict__ xs,
-                                                     const unsigned short* __restrict__ dcol,
-                                                     const int* __restrict__ cbase) {
-  if (amg_enter(S)) return;
+__device__ __forceinline__ void sell_rows(const SellView<V>& A, const T* __restrict__ x,
+                                          const T* __restrict__ b, const T* __restrict__ dinv,
+                                          T* __restrict__ y, T w, const int* __restrict__ yperm,
+                                          const T* __restrict__ xs,
+                                          const unsigned short* __restrict__ dcol,
+                                          const int* __restrict__ cbase, int gw, int nw) {
   // slots a lane loads before gathering: 8 in FP32 (a prolongation row's slots in one
   // round trip), 4 in FP64
   constexpr int kCh = sizeof(T) == 4 ? 8 : 4;
   const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int s = gw; s < A.nslices; s += nw) {
     const long long b0 = A.sptr[s];
     const int len = (int)((A.sptr[s + 1] - b0) >> 5);
@@ -603,6 +599,21 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 6 : 8) k_amg_spmv(SellVi
   }
 }
 
+template <typename T, int MODE, typename V = T, bool C16 = false, bool XS = false>
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 6 : 8) k_amg_spmv(SellView<V> A, const T* __restrict__ x,
+                                                     const T* __restrict__ b,
+                                                     const T* __restrict__ dinv,
+                                                     T* __restrict__ y, PcgScalars* S, T w,
+                                                     const int* __restrict__ yperm,
+                                                     const T* __restrict__ xs,
+                                                     const unsigned short* __restrict__ dcol,
+                                                     const int* __restrict__ cbase) {
+  if (amg_enter(S)) return;
+  sell_rows<T, MODE, V, C16, XS>(A, x, b, dinv, y, w, yperm, xs, dcol, cbase,
+                                 (blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                                 (gridDim.x * blockDim.x) >> 5);
+}
+
 // The same products from the CSR form: LANES threads per row, each summing a strided part
 // of the row, combined by a fixed shuffle tree (deterministic).  The row loop is uniform
 // across the warp (32 / LANES rows per warp per pass), so every lane takes part in the
@@ -612,19 +623,15 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 6 : 8) k_amg_spmv(SellVi
 // instead of two per entry plus one for the bounds.  Each lane still adds its entries in
 // increasing order.
 template <typename T, int MODE, int LANES, typename V = T, typename CI = int, bool XS = false>
-__global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restrict__ rp,
-                                                 const CI* __restrict__ col,
-                                                 const V* __restrict__ val, const T* __restrict__ x,
-                                                 const T* __restrict__ b,
-                                                 const T* __restrict__ dinv, T* __restrict__ y,
-                                                 PcgScalars* S, T w, const T* __restrict__ xs,
-                                                 const int* __restrict__ cbase) {
-  if (amg_enter(S)) return;
+__device__ __forceinline__ void csr_rows(int nrows, const int* __restrict__ rp,
+                                         const CI* __restrict__ col, const V* __restrict__ val,
+                                         const T* __restrict__ x, const T* __restrict__ b,
+                                         const T* __restrict__ dinv, T* __restrict__ y, T w,
+                                         const T* __restrict__ xs, const int* __restrict__ cbase,
+                                         int gw, int nw) {
   constexpr int RPW = 32 / LANES;        // rows per warp per pass
   constexpr int U = LANES <= 4 ? 8 : 4;  // entries a lane loads before their gathers
   const int lane = threadIdx.x & 31, sub = lane % LANES;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
   constexpr bool kShort = sizeof(CI) == 2;  // 16-bit offsets from each row's base column
   int r0 = gw * RPW;
   int kb = 0, ke = 0, cb = 0;
@@ -676,6 +683,20 @@ __global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restric
     ke = ken;
     cb = cbn;
   }
+}
+
+template <typename T, int MODE, int LANES, typename V = T, typename CI = int, bool XS = false>
+__global__ void __launch_bounds__(256) k_amg_csr(int nrows, const int* __restrict__ rp,
+                                                 const CI* __restrict__ col,
+                                                 const V* __restrict__ val, const T* __restrict__ x,
+                                                 const T* __restrict__ b,
+                                                 const T* __restrict__ dinv, T* __restrict__ y,
+                                                 PcgScalars* S, T w, const T* __restrict__ xs,
+                                                 const int* __restrict__ cbase) {
+  if (amg_enter(S)) return;
+  csr_rows<T, MODE, LANES, V, CI, XS>(nrows, rp, col, val, x, b, dinv, y, w, xs, cbase,
+                                      (blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                                      (gridDim.x * blockDim.x) >> 5);
 }
 
 int vec_blocks(int n);
@@ -847,19 +868,144 @@ void launch_amgp(const PackedView& pk, SellView<float> A, int nb, const float* x
 
 // Coarsest level: x = C b, one warp per row of the dense inverse.
 template <typename T>
-__global__ void __launch_bounds__(256) k_amg_dense(int m, const T* __restrict__ C,
-                                                   const T* __restrict__ b, T* __restrict__ x,
-                                                   PcgScalars* S) {
-  if (amg_enter(S)) return;
+__device__ __forceinline__ void dense_rows(int m, const T* __restrict__ C, const T* __restrict__ b,
+                                           T* __restrict__ x, int gw, int nw) {
   const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int i = gw; i < m; i += nw) {
     T acc = T(0);
     for (int j = lane; j < m; j += 32) acc = fmat(C[(size_t)i * m + j], b[j], acc);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if (lane == 0) x[i] = acc;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_amg_dense(int m, const T* __restrict__ C,
+                                                   const T* __restrict__ b, T* __restrict__ x,
+                                                   PcgScalars* S) {
+  if (amg_enter(S)) return;
+  dense_rows<T>(m, C, b, x, (blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                (gridDim.x * blockDim.x) >> 5);
+}
+
+// ------------------------------------------------------------------ coarse tail
+// The FP32 cycle's small levels in one cooperative launch: the products of those levels
+// (the same row functions, so the same results as one kernel each) run one after the other
+// over the whole grid, separated by a grid barrier instead of a kernel boundary; a dozen
+// latency-bound launches of a few microseconds each become one.
+namespace tail {
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// All CTAs of the grid have arrived and their earlier writes are visible; false in every
+// thread when the wait gave up (about 2 s of SM clock).
+__device__ bool grid_sync(unsigned* bar, unsigned target, int* s_ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(bar, 1u);
+    const long long t0 = clock64();
+    int ok = 1;
+    while (ld_acquire(bar) < target)
+      if (clock64() - t0 > 4000000000LL) {
+        ok = 0;
+        break;
+      }
+    __threadfence();
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+template <int MODE, int LANES, typename V, bool XS>
+__device__ __forceinline__ void csr_op(const TailOp& o, int gw, int nw) {
+  csr_rows<float, MODE, LANES, V, int, XS>(o.nrows, o.rp, o.col, (const V*)o.val, o.x, o.b,
+                                           o.dinv, o.y, 1.0f, o.xs, nullptr, gw, nw);
+}
+
+template <int MODE, typename V, bool XS>
+__device__ __forceinline__ void sell_op(const TailOp& o, int gw, int nw) {
+  const SellView<V> A{o.nrows, o.nslices, o.sptr, o.col, (const V*)o.val, 0};
+  sell_rows<float, MODE, V, false, XS>(A, o.x, o.b, o.dinv, o.y, 1.0f, nullptr, o.xs, nullptr,
+                                       nullptr, gw, nw);
+}
+
+// The forms a small level's operators take (TailOp::form): coarse operators with FP32
+// values (residual with the folded Jacobi start, smoothing), transfers with FP16 values
+// (restriction, prolongation onto the folded start).
+__device__ void exec(const TailOp& o, int gw, int nw) {
+  switch (o.form) {
+    case kTailDense: dense_rows<float>(o.nrows, (const float*)o.val, o.b, o.y, gw, nw); break;
+    case kTailSellResid: sell_op<kResid, float, true>(o, gw, nw); break;
+    case kTailSellSmooth: sell_op<kSmooth, float, false>(o, gw, nw); break;
+    case kTailSellRestrict: sell_op<kPlain, __half, false>(o, gw, nw); break;
+    case kTailSellProlong: sell_op<kDiagAdd, __half, false>(o, gw, nw); break;
+    case kTailCsrResid:
+      if (o.lanes == 32) csr_op<kResid, 32, float, true>(o, gw, nw);
+      else if (o.lanes == 16) csr_op<kResid, 16, float, true>(o, gw, nw);
+      else csr_op<kResid, 8, float, true>(o, gw, nw);
+      break;
+    case kTailCsrSmooth:
+      if (o.lanes == 32) csr_op<kSmooth, 32, float, false>(o, gw, nw);
+      else if (o.lanes == 16) csr_op<kSmooth, 16, float, false>(o, gw, nw);
+      else csr_op<kSmooth, 8, float, false>(o, gw, nw);
+      break;
+    case kTailCsrRestrict:
+      if (o.lanes == 32) csr_op<kPlain, 32, __half, false>(o, gw, nw);
+      else if (o.lanes == 16) csr_op<kPlain, 16, __half, false>(o, gw, nw);
+      else if (o.lanes == 8) csr_op<kPlain, 8, __half, false>(o, gw, nw);
+      else csr_op<kPlain, 4, __half, false>(o, gw, nw);
+      break;
+    case kTailCsrProlong:
+      if (o.lanes == 32) csr_op<kDiagAdd, 32, __half, false>(o, gw, nw);
+      else if (o.lanes == 16) csr_op<kDiagAdd, 16, __half, false>(o, gw, nw);
+      else if (o.lanes == 8) csr_op<kDiagAdd, 8, __half, false>(o, gw, nw);
+      else csr_op<kDiagAdd, 4, __half, false>(o, gw, nw);
+      break;
+    default: break;
+  }
+}
+
+}  // namespace tail
+
+// bar[0]: barrier arrivals, bar[1]: CTAs done; both zero between launches (the last CTA
+// to leave resets them).  A barrier that gives up stops the solve with
+// GIPB200_ERR_TIMEOUT.
+__global__ void __launch_bounds__(256) k_amg_tail(const TailOp* __restrict__ ops, int nops,
+                                                  unsigned* bar, PcgScalars* S) {
+  if (amg_enter(S)) return;
+  __shared__ int s_ok;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  bool ok = true;
+  for (int k = 0; k < nops; ++k) {
+    if (k > 0 && !tail::grid_sync(bar, (unsigned)k * gridDim.x, &s_ok)) {
+      ok = false;
+      break;
+    }
+    tail::exec(ops[k], gw, nw);
+  }
+  if (!ok) {
+    if (threadIdx.x == 0) {
+      S->status = GIPB200_ERR_TIMEOUT;
+      S->done = 1;
+    }
+    return;  // the counters stay set; the solve's start clears them
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(bar + 1, 1u) == gridDim.x - 1) {
+      bar[0] = 0u;
+      bar[1] = 0u;
+      __threadfence();
+    }
   }
 }
 
@@ -1064,8 +1210,114 @@ int AmgT<T>::build(int n, const int* rp, const int* ci, const double* v, const d
     return GIPB200_OK;
   }));
   op_complexity = nnz_all / std::max(nnz0, 1.0);
+  GIPB_TRY(build_tail(s));
   GIPB_CUDA(cudaStreamSynchronize(s));
   setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return GIPB200_OK;
+}
+
+// The coarse tail's product list: levels tail_from..L-2 down (folded residual,
+// restriction), the dense coarsest solve, then the same levels up (prolongation onto the
+// folded start, smoothing) -- the order and the data of the separate kernels.  Left off
+// (tail_from = -1) for the FP64 cycle, without folding, or when an operator has a form
+// the tail does not run (16-bit columns, FP16 coarse values, 4 threads per coarse row).
+template <typename T>
+int AmgT<T>::build_tail(cudaStream_t s) {
+  tail_from = -1;
+  tail_nops = 0;
+  if constexpr (!std::is_same<T, float>::value) {
+    return GIPB200_OK;
+  } else {
+    const int L = (int)lv.size();
+    if (getenv("GIPB200_AMG_NO_TAIL") || !fold_coarse || L < 3 || nc <= 0) return GIPB200_OK;
+    int tf = L - 1;
+    while (tf - 1 >= 1 && lv[tf - 1]->n <= kTailRows) --tf;
+    if (tf > L - 2) return GIPB200_OK;  // no level above the coarsest is small
+    for (int l = tf; l < L - 1; ++l)
+      if (!folds(l)) return GIPB200_OK;
+    std::vector<TailOp> ops;
+    const double w = sizeof(T);
+    // the operator's form for one product; false when the tail does not run it
+    auto add = [&](const SellT<T>& M, bool transfer, int sell_form, int csr_form,
+                   const float* x, const float* b, const float* dinv, const float* xs, float* y,
+                   int level, int kind, double bytes) -> bool {
+      if (M.short_cols || M.half != transfer) return false;
+      TailOp o{};
+      o.nrows = M.nrows;
+      o.nslices = M.nslices;
+      o.sptr = M.sptr.p;
+      o.rp = M.rp.p;
+      o.col = M.col.p;
+      o.val = transfer ? (const void*)M.hval.p : (const void*)M.val.p;
+      o.lanes = M.lanes;
+      if (M.lanes == 0) {
+        o.form = sell_form;
+      } else {
+        if (!transfer && M.lanes < 8) return false;
+        o.form = csr_form;
+      }
+      o.x = x;
+      o.b = b;
+      o.dinv = dinv;
+      o.xs = xs;
+      o.y = y;
+      o.level = level;
+      o.kind = kind;
+      o.bytes = bytes;
+      ops.push_back(o);
+      return true;
+    };
+    for (int l = tf; l < L - 1; ++l) {
+      const AmgLevel<T>& V = *lv[l];
+      const double n = V.n, nn = lv[l + 1]->n;
+      if (!add(V.A, false, kTailSellResid, kTailCsrResid, V.b.p, V.b.p, nullptr, V.dinv.p, V.t.p,
+               l, GIPB200_CYCLE_RESIDUAL, stream_bytes(V.A) + 3.0 * n * w) ||
+          !add(V.R, true, kTailSellRestrict, kTailCsrRestrict, V.t.p, nullptr, nullptr, nullptr,
+               lv[l + 1]->b.p, l, GIPB200_CYCLE_RESTRICT, stream_bytes(V.R) + (n + nn) * w))
+        return GIPB200_OK;
+    }
+    {
+      TailOp o{};
+      o.form = kTailDense;
+      o.nrows = nc;
+      o.val = cinv.p;
+      o.b = lv[L - 1]->b.p;
+      o.y = lv[L - 1]->x.p;
+      o.level = L - 1;
+      o.kind = GIPB200_CYCLE_DENSE;
+      o.bytes = ((double)nc * nc + 2.0 * nc) * w;
+      ops.push_back(o);
+    }
+    for (int l = L - 2; l >= tf; --l) {
+      const AmgLevel<T>& V = *lv[l];
+      const double n = V.n, nn = lv[l + 1]->n;
+      const float* xc = (l + 1 == L - 1) ? lv[l + 1]->x.p : lv[l + 1]->t.p;
+      if (!add(V.P, true, kTailSellProlong, kTailCsrProlong, xc, V.b.p, V.dinv.p, nullptr,
+               V.x.p, l, GIPB200_CYCLE_PROLONG, stream_bytes(V.P) + (nn + 3.0 * n) * w) ||
+          !add(V.A, false, kTailSellSmooth, kTailCsrSmooth, V.x.p, V.b.p, V.dinv.p, nullptr,
+               V.t.p, l, GIPB200_CYCLE_SMOOTH, stream_bytes(V.A) + 4.0 * n * w))
+        return GIPB200_OK;
+    }
+    DeviceInfo di;
+    GIPB_TRY(device_info(&di));
+    int per_sm = 0;
+    GIPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_amg_tail, 256, 0));
+    if (per_sm < 1) return GIPB200_OK;
+    tail_grid = std::min(per_sm, 2) * di.nsm;
+    GIPB_TRY(tail_ops.upload(ops.data(), ops.size(), s));
+    GIPB_TRY(tail_bar.alloc(2));
+    GIPB_TRY(tail_bar.zero(s));
+    tail_bytes = 0.0;
+    for (const TailOp& o : ops) tail_bytes += o.bytes;
+    tail_nops = (int)ops.size();
+    tail_from = tf;
+    return GIPB200_OK;
+  }
+}
+
+template <typename T>
+int AmgT<T>::reset_tail(cudaStream_t s) const {
+  if (tail_from >= 0) GIPB_CUDA(cudaMemsetAsync(tail_bar.p, 0, 2 * sizeof(unsigned), s));
   return GIPB200_OK;
 }
 
@@ -1101,9 +1353,10 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     return tr ? tr->mark(s, l, kind, by) : GIPB200_OK;
   };
   auto a_bytes = [&](int l) { return l == 0 ? a0_stream_bytes : stream_bytes(lv[l]->A); };
-  // downward: pre-smooth from zero, residual, restriction
+  // downward: pre-smooth from zero, residual, restriction (levels below the coarse tail)
   const bool u0 = unit0;  // level 0 never forms x0 = omega0 r
-  for (int l = 0; l < L - 1; ++l) {
+  const int tf = tail_from;
+  for (int l = 0; l < L - 1 && (tf < 0 || l < tf); ++l) {
     const AmgLevel<T>& V = *lv[l];
     const T* b = l == 0 ? r : V.b.p;
     const double n = V.n, nn = lv[l + 1]->n;
@@ -1134,11 +1387,26 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     amg_mv<T, kPlain>(V.R, V.t.p, (const T*)nullptr, (const T*)nullptr, lv[l + 1]->b.p, S, s);
   }
   const AmgLevel<T>& C = *lv[L - 1];
-  GIPB_TRY(mark(L - 1, GIPB200_CYCLE_DENSE, ((double)nc * nc + 2.0 * nc) * w));
-  launch_dep(k_amg_dense<T>, std::min(kMaxReduceBlocks, (nc + 7) / 8), 256, s, nc,
-             (const T*)cinv.p, (const T*)C.b.p, C.x.p, S);
+  if (tf >= 0) {  // the small levels and the coarsest in one cooperative launch
+    GIPB_TRY(mark(tf, GIPB200_CYCLE_TAIL, tail_bytes));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)tail_grid);
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    GIPB_CUDA(cudaLaunchKernelEx(&cfg, k_amg_tail, (const TailOp*)tail_ops.p, tail_nops,
+                                 tail_bar.p, S));
+  } else {
+    GIPB_TRY(mark(L - 1, GIPB200_CYCLE_DENSE, ((double)nc * nc + 2.0 * nc) * w));
+    launch_dep(k_amg_dense<T>, std::min(kMaxReduceBlocks, (nc + 7) / 8), 256, s, nc,
+               (const T*)cinv.p, (const T*)C.b.p, C.x.p, S);
+  }
   // upward: prolongation, post-smoothing (level 0 also reduces r.z)
-  for (int l = L - 2; l >= 0; --l) {
+  for (int l = std::min(L - 2, tf >= 0 ? tf - 1 : L - 2); l >= 0; --l) {
     const AmgLevel<T>& V = *lv[l];
     const T* xc = (l + 1 == L - 1) ? lv[l + 1]->x.p : lv[l + 1]->t.p;
     const double n = V.n, nn = lv[l + 1]->n;

@@ -38,6 +38,35 @@ struct SellT {
   SellView<__half> hview() const { return {nrows, nslices, sptr.p, col.p, hval.p}; }
 };
 
+// One product of the FP32 cycle's small levels as the coarse-tail kernel runs it.
+enum {
+  kTailDense = 0,
+  kTailSellResid,
+  kTailSellSmooth,
+  kTailSellRestrict,
+  kTailSellProlong,
+  kTailCsrResid,
+  kTailCsrSmooth,
+  kTailCsrRestrict,
+  kTailCsrProlong
+};
+struct TailOp {
+  int form;        // kTail*
+  int lanes;       // CSR threads per row
+  int nrows, nslices;
+  const long long* sptr;
+  const int* rp;
+  const int* col;
+  const void* val;  // float or __half (dense: float)
+  const float* x;
+  const float* b;
+  const float* dinv;
+  const float* xs;
+  float* y;
+  int level, kind;  // cycle position (profiling)
+  double bytes;
+};
+
 // The mixed form's packed FP32 operator (see CompressedOp), for the V-cycle's level-0
 // products.  on = false: use the plain sliced view.
 struct PackedView {
@@ -96,6 +125,16 @@ struct AmgT {
   // Level 0's residual position in aggregate order (empty: written in row order); the
   // level-0 restriction's columns are numbered in that order.
   DevBuf<int> perm0;
+  // Coarse tail (FP32 cycle): levels tail_from.. (at most kTailRows unknowns each, all
+  // folding their Jacobi starts) run as one cooperative launch of tail_grid CTAs
+  // (GIPB200_AMG_NO_TAIL=1: one kernel per product); tail_from < 0: no tail.
+  static constexpr int kTailRows = 1 << 19;
+  int tail_from = -1, tail_grid = 0, tail_nops = 0;
+  DevBuf<TailOp> tail_ops;
+  DevBuf<unsigned> tail_bar;
+  double tail_bytes = 0.0;
+  int build_tail(cudaStream_t s);
+  int reset_tail(cudaStream_t s) const;
 
   // Hierarchy of the n x n operator (host CSR, FP64 values; columns < n), near-null
   // vector z.  singular: the operator annihilates z (pinned-Neumann inner system), so the

@@ -1265,6 +1265,7 @@ int Pcg::enqueue_mixed_graph(const double* b, double* x, const double* x0, cudaS
   GIPB_TRY(make_handle(s, 0, 0, &hl));
   if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
+  if (amg) GIPB_TRY(amg->reset_tail(s));
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 1, hl));
   if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s, &pk0));
   cudaGraph_t loop_body;
@@ -1395,6 +1396,7 @@ int Pcg::enqueue_mixed(const double* b, double* x, const double* x0, cudaStream_
   const PackedView pk0 = packed();
   if (x != x0) GIPB_CUDA(cudaMemcpyAsync(x, x0, (size_t)n_all * 8, cudaMemcpyDeviceToDevice, s));
   GIPB_CUDA(cudaMemsetAsync(sc.p, 0, sizeof(PcgScalars), s));
+  if (amg) GIPB_TRY(amg->reset_tail(s));
   GIPB_TRY(launch_mixed_residual(b, x, 1, s, 0, 0));
   if (amg) GIPB_TRY(amg->enqueue(a32(), r32.p, z32.p, sc.p, rs, 0, s, &pk0));
   const int poll = host_poll_interval();
@@ -1513,6 +1515,7 @@ int Pcg::profile_vcycle(int reps, cudaStream_t s, int cap, int* n_kernels, int* 
   DevBuf<PcgScalars> tsc;
   GIPB_TRY(tsc.alloc(1));
   GIPB_TRY(tsc.zero(s));
+  if (amg) GIPB_TRY(amg->reset_tail(s));
   const PackedView pk0 = packed();
   const double plain32 = (double)L->nslots * 8.0 + (L->nslices + 1.0) * 8.0;
   const double a0 = amg ? (cop.enabled ? cop.bytes_per_launch - 16.0 * n : plain32)

@@ -177,7 +177,7 @@ def pcg_params(mode: str = "fixed", maxit: int = 100, tol: float = 1e-6,
                        PRECONDS[precond])
 
 
-CYCLE_KINDS = ("jacobi0", "residual", "restrict", "dense", "prolong", "smooth")
+CYCLE_KINDS = ("jacobi0", "residual", "restrict", "dense", "prolong", "smooth", "tail")
 
 
 def _vcycle_profile(fn: str, handle, reps: int, stream) -> list:

@@ -230,7 +230,8 @@ enum {
   GIPB200_CYCLE_RESTRICT = 2,  /* b_coarse = R t                                 */
   GIPB200_CYCLE_DENSE = 3,     /* coarsest level: x = A^-1 b (dense inverse)     */
   GIPB200_CYCLE_PROLONG = 4,   /* x += P x_coarse                                */
-  GIPB200_CYCLE_SMOOTH = 5     /* x + D^-1 (b - A x) (level 0: with r.z)         */
+  GIPB200_CYCLE_SMOOTH = 5,    /* x + D^-1 (b - A x) (level 0: with r.z)         */
+  GIPB200_CYCLE_TAIL = 6       /* the small levels and the coarsest, one launch  */
 };
 int gipb200_pcg_vcycle_profile(gipb200_pcg S, int reps, void* stream, int cap, int* n_kernels,
                                int* h_level, int* h_kind, double* h_ms, double* h_bytes);

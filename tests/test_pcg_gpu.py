@@ -254,3 +254,25 @@ def test_amg_compact_coarse_operators(gpu, monkeypatch, coarse_half):
         assert abs(its["0"] - its["1"]) <= max(2, its["1"] // 10), its
     else:  # 16-bit columns alone change nothing
         assert its["0"] == its["1"], its
+
+
+def test_amg_coarse_tail_is_exact(gpu, monkeypatch):
+    # the small levels run as one cooperative launch: every row is still summed by one warp
+    # with the separate kernels' row functions, so the solve is identical, bit for bit
+    from gip_b200 import device as dv
+    L, b = cavity.poisson_problem(48, seed=4)
+    A = dv.DeviceMatrix(L)
+    out = {}
+    for tail in (True, False):
+        if not tail:
+            monkeypatch.setenv("GIPB200_AMG_NO_TAIL", "1")
+        S = dv.PcgSolver(A, mode="mixed", maxit=2000, tol=1e-9, inner_tol=1e-2, max_outer=100,
+                         precond="amg")
+        x = _t(np.zeros(L.nrows))
+        res = S.solve(_t(b), x, _t(np.zeros(L.nrows)))
+        assert res["status"] == 0, (tail, res)
+        prof = S.vcycle_profile(reps=2)
+        out[tail] = (x.cpu().numpy(), res["iterations"], [c["kind"] for c in prof])
+    assert "tail" in out[True][2] and "tail" not in out[False][2]
+    assert out[True][1] == out[False][1]
+    assert np.array_equal(out[True][0], out[False][0])
