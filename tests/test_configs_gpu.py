@@ -58,9 +58,10 @@ def _batch_set(seed=1234):
 @pytest.mark.slow
 def test_config5_batch_32_uneven_cavities(gpu, oracle_mod):
     """The 32 seeded cavities (edges from {24..96}, Re log-uniform on [100, 1000]) advance 10
-    mixed steps (AMG, tol 1e-8) in one batch: every instance keeps massr < 1e-6 and its
-    velocity within 1e-6 (of its velocity scale) of the FP64 form solved to 1e-10; the
-    instances of edge <= 32 are checked against the FP64 oracle directly as well."""
+    mixed steps (tol 1e-8) in one batch, with AMG in the graph branches and with GIP's
+    Jacobi in one persistent launch: every instance keeps massr < 1e-6 and its velocity
+    within 1e-6 (of its velocity scale) of the FP64 form solved to 1e-10; the instances of
+    edge <= 32 are checked against the FP64 oracle directly as well."""
     from gip_b200.device import DnsBatch, DnsEngine, dns_params
     edges, res = _batch_set()
     assert sorted(set(edges)) <= [24, 32, 48, 64, 80, 96] and len(edges) == 32
@@ -70,11 +71,20 @@ def test_config5_batch_32_uneven_cavities(gpu, oracle_mod):
     B = DnsBatch(cases, params)
     steps = 10
     B.advance(steps)
+    # the same batch with GIP's Jacobi, every pressure solve in one persistent launch
+    pj = [dns_params(gamma=1.0 / r, pcg_mode="mixed", precond="jacobi",
+                     **dict(kw, inner_tol=0.3)) for r in res]
+    P = DnsBatch(cases, pj)
+    P.set_solver(True, 256, 64, 1536)
+    P.advance(steps)
     torch.cuda.synchronize()
+    assert P.solver_status() == 0
     checked_oracle = 0
-    for c, n, r, e in zip(cases, edges, res, B.instances):
+    for c, n, r, e, ep in zip(cases, edges, res, B.instances, P.instances):
         h = e.history()
         assert len(h["massr"]) == steps and np.all(h["massr"] < 1e-6), (n, r, h["massr"])
+        hp = ep.history()
+        assert len(hp["massr"]) == steps and np.all(hp["massr"] < 1e-6), (n, r, hp["massr"])
         F = DnsEngine(c, gamma=1.0 / r, pcg_mode="tol", precond="amg",
                       **dict(kw, tol=1e-10))
         F.advance(steps)
@@ -82,6 +92,8 @@ def test_config5_batch_32_uneven_cavities(gpu, oracle_mod):
         for k in ("u", "v", "w"):
             err = np.abs(e.field(k) - F.field(k)).max() / scale
             assert err < 1e-6, (n, r, k, err)
+            err = np.abs(ep.field(k) - F.field(k)).max() / scale
+            assert err < 1e-6, ("persistent", n, r, k, err)
         del F
         if n <= 32:
             d = oracle_mod.OracleDNS(c, gamma=1.0 / r, cg_maxit=20000, cg_mode=1, cg_tol=1e-10)
