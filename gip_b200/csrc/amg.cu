@@ -365,9 +365,12 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool c
   S->nnz = A.nnz();
   S->nslices = (A.nr + 31) / 32;
   const double avg = (double)A.nnz() / std::max(A.nr, 1);
-  // rows of at least kCsrRows entries on average are CSR (GIPB200_AMG_CSR_ROWS overrides)
+  // Rows of at least 32 entries on average are CSR, shorter ones sliced (a lane per row,
+  // eight slots in flight): on the 256^3 cavity the level-1 operator (21 per row) and the
+  // level-0 restriction (29) ran 72 and 124 us sliced against 91 and 128 us in CSR.
+  // GIPB200_AMG_CSR_ROWS overrides the threshold.
   const char* csr_env = getenv("GIPB200_AMG_CSR_ROWS");
-  const double csr_rows = csr_env ? atof(csr_env) : 12.0;
+  const double csr_rows = csr_env ? atof(csr_env) : 32.0;
   if (avg >= csr_rows) {  // long rows: CSR, 4 to 32 threads per row
     // FP32 cycle's transfer operators (FP16 values): as few threads per row as cover its
     // entries in one pass (4 threads x 8 entries, 8 x 4, ...), so that a warp works on more
@@ -1229,7 +1232,11 @@ int AmgT<T>::build_tail(cudaStream_t s) {
     return GIPB200_OK;
   } else {
     const int L = (int)lv.size();
-    if (getenv("GIPB200_AMG_NO_TAIL") || !fold_coarse || L < 3 || nc <= 0) return GIPB200_OK;
+    // GIPB200_AMG_TAIL=<CTAs per SM>: on (measured no faster than the separate kernels in
+    // the step's graph: its grid barriers cost what the launches did)
+    const char* tail_env = getenv("GIPB200_AMG_TAIL");
+    const int tail_per_sm = tail_env ? atoi(tail_env) : 0;
+    if (tail_per_sm <= 0 || !fold_coarse || L < 3 || nc <= 0) return GIPB200_OK;
     int tf = L - 1;
     while (tf - 1 >= 1 && lv[tf - 1]->n <= kTailRows) --tf;
     if (tf > L - 2) return GIPB200_OK;  // no level above the coarsest is small
@@ -1303,7 +1310,7 @@ int AmgT<T>::build_tail(cudaStream_t s) {
     int per_sm = 0;
     GIPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_amg_tail, 256, 0));
     if (per_sm < 1) return GIPB200_OK;
-    tail_grid = std::min(per_sm, 2) * di.nsm;
+    tail_grid = std::min(per_sm, tail_per_sm) * di.nsm;
     GIPB_TRY(tail_ops.upload(ops.data(), ops.size(), s));
     GIPB_TRY(tail_bar.alloc(2));
     GIPB_TRY(tail_bar.zero(s));

@@ -125,9 +125,9 @@ struct AmgT {
   // Level 0's residual position in aggregate order (empty: written in row order); the
   // level-0 restriction's columns are numbered in that order.
   DevBuf<int> perm0;
-  // Coarse tail (FP32 cycle): levels tail_from.. (at most kTailRows unknowns each, all
-  // folding their Jacobi starts) run as one cooperative launch of tail_grid CTAs
-  // (GIPB200_AMG_NO_TAIL=1: one kernel per product); tail_from < 0: no tail.
+  // Coarse tail (FP32 cycle, GIPB200_AMG_TAIL=<CTAs per SM>): levels tail_from.. (at most
+  // kTailRows unknowns each, all folding their Jacobi starts) run as one cooperative launch
+  // of tail_grid CTAs; tail_from < 0: one kernel per product (the default).
   static constexpr int kTailRows = 1 << 19;
   int tail_from = -1, tail_grid = 0, tail_nops = 0;
   DevBuf<TailOp> tail_ops;

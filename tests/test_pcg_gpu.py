@@ -264,8 +264,10 @@ def test_amg_coarse_tail_is_exact(gpu, monkeypatch):
     A = dv.DeviceMatrix(L)
     out = {}
     for tail in (True, False):
-        if not tail:
-            monkeypatch.setenv("GIPB200_AMG_NO_TAIL", "1")
+        if tail:
+            monkeypatch.setenv("GIPB200_AMG_TAIL", "2")
+        else:
+            monkeypatch.delenv("GIPB200_AMG_TAIL", raising=False)
         S = dv.PcgSolver(A, mode="mixed", maxit=2000, tol=1e-9, inner_tol=1e-2, max_outer=100,
                          precond="amg")
         x = _t(np.zeros(L.nrows))
