@@ -407,6 +407,80 @@ __global__ void __launch_bounds__(256) k_mx_residual(SellView<double> L, const d
                                        scale, r32, p32, use_cond, loop_cond, amg});
 }
 
+// The same residual from the packed operator's columns with L's FP64 values from a 4-bit
+// table (each row's inner entries in column order) against b' = b - L_ghost x_ghost,
+// which the solve forms once (x's ghost entries do not change during a solve); slices
+// stored plain use L's own row against b.  Streams 24 instead of ~100 bytes per row.
+__global__ void __launch_bounds__(256, 8) k_mx_residual_packed(
+    SellView<double> L, const uint4* __restrict__ delta, const int* __restrict__ base,
+    const unsigned char* __restrict__ plain, const unsigned* __restrict__ lidx,
+    const double* __restrict__ ltable, const double* __restrict__ bp,
+    const double* __restrict__ x, const double* __restrict__ b,
+    const double* __restrict__ scale, float* __restrict__ r32, float* __restrict__ p32,
+    float* __restrict__ y32, PcgScalars* S, ReduceScratch rs, int first, double tol,
+    double delta_f, int maxit, int max_updates, int pin_row, double pin_val, int use_cond,
+    cudaGraphConditionalHandle loop_cond, int amg) {
+  mx_enter(S, 0, 0);
+  if (!first && (!S->upd || S->done)) return;
+  __shared__ double tab[16];
+  if (threadIdx.x < 16) tab[threadIdx.x] = ltable[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int s = gw; s < L.nslices; s += nw) {
+    const int i = s * 32 + lane;
+    const int pl = __ldg(plain + s);
+    const uint4 d = ld_stream(delta + i);
+    const unsigned w = ld_stream(lidx + i);
+    int c[8];
+    packed_cols(base, s, d, c);
+    double sum = 0.0;
+    if (pl) {
+      bool any = false;
+      sell_row_f64(L, x, s, lane, sum, any);
+    } else {
+      double xv[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) xv[j] = __ldg(x + c[j]);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) sum = dadd(sum, dmul(xv[j], tab[(w >> (4 * j)) & 15u]));
+    }
+    if (i < L.nrows) {
+      const double bi = b[i];
+      const double ri = (pl ? bi : bp[i]) - sum;
+      const float rh = (float)(ri * scale[i]);
+      r32[i] = rh;
+      if (first) {
+        p32[i] = rh;
+        y32[i] = 0.f;
+      }
+      acc[0] += ri * ri;
+      acc[1] += (double)rh * (double)rh;
+      acc[2] += bi * bi;
+      acc[3] += ri;
+    }
+  }
+  grid_reduce<SumOp, 4>(acc, rs,
+                        ResidualFinish{S, first, tol, delta_f, maxit, max_updates, pin_row,
+                                       pin_val, scale, r32, p32, use_cond, loop_cond, amg});
+}
+
+// b' = b - L_ghost x for the rows with ghost columns (b' = b elsewhere, copied before)
+__global__ void k_mx_ghost_rhs(int ng, const int* __restrict__ rows, const int* __restrict__ rp,
+                               const int* __restrict__ col, const double* __restrict__ val,
+                               const double* __restrict__ x, const double* __restrict__ b,
+                               double* __restrict__ bp) {
+  dep_begin();
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += gridDim.x * blockDim.x) {
+    double sum = 0.0;
+    for (int k = rp[g]; k < rp[g + 1]; ++k) sum = dadd(sum, dmul(x[col[k]], val[k]));
+    const int i = rows[g];
+    bp[i] = b[i] - sum;
+  }
+}
+
 struct AlphaFinish32 {
   PcgScalars* S;
   __device__ void operator()(const double* t) const {
@@ -934,31 +1008,77 @@ int Pcg::sort_fp32_rows(cudaStream_t s) {
   std::vector<long long> sptr((size_t)ns + 1);
   std::vector<int> col((size_t)nslots);
   std::vector<float> val((size_t)nslots);
+  std::vector<double> lval((size_t)nslots);
   GIPB_CUDA(cudaMemcpyAsync(sptr.data(), L->sptr.p, sptr.size() * 8, cudaMemcpyDeviceToHost, s));
   GIPB_CUDA(cudaMemcpyAsync(col.data(), L->col.p, col.size() * 4, cudaMemcpyDeviceToHost, s));
   GIPB_CUDA(cudaMemcpyAsync(val.data(), lhat.p, val.size() * 4, cudaMemcpyDeviceToHost, s));
+  GIPB_CUDA(cudaMemcpyAsync(lval.data(), L->val.p, lval.size() * 8, cudaMemcpyDeviceToHost, s));
   GIPB_CUDA(cudaStreamSynchronize(s));
   const int nu = n;
+  // ghost entries (columns >= n) per row, for the packed FP64 residual's constant part:
+  // counted and listed from the original slots, before the rows are sorted
+  const int nr = L->nrows;
+  std::vector<int> gcount((size_t)nr + 1, 0);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < nr; ++i) {
+    const int sl = i >> 5, l = i & 31;
+    const long long b0 = sptr[sl];
+    const int len = (int)((sptr[sl + 1] - b0) >> 5);
+    int g = 0;
+    for (int j = 0; j < len; ++j) g += col[b0 + 32LL * j + l] >= nu ? 1 : 0;
+    gcount[(size_t)i + 1] = g;
+  }
+  ghost_rows.clear();
+  ghost_rp.assign(1, 0);
+  for (int i = 0; i < nr; ++i)
+    if (gcount[(size_t)i + 1] > 0) {
+      ghost_rows.push_back(i);
+      ghost_rp.push_back(ghost_rp.back() + gcount[(size_t)i + 1]);
+    }
+  ghost_col.assign((size_t)ghost_rp.back(), 0);
+  ghost_val.assign((size_t)ghost_rp.back(), 0.0);
+#pragma omp parallel for schedule(static)
+  for (int g = 0; g < (int)ghost_rows.size(); ++g) {
+    const int i = ghost_rows[g], sl = i >> 5, l = i & 31;
+    const long long b0 = sptr[sl];
+    const int len = (int)((sptr[sl + 1] - b0) >> 5);
+    int o = ghost_rp[g];
+    for (int j = 0; j < len; ++j) {
+      const long long k = b0 + 32LL * j + l;
+      if (col[k] >= nu) {
+        ghost_col[(size_t)o] = col[k];
+        ghost_val[(size_t)o] = lval[k];
+        ++o;
+      }
+    }
+  }
+  // each row's inner entries sorted by column; L's FP64 values follow in lval_sorted (the
+  // packed FP64 residual reads them in this order)
+  lval_sorted.assign((size_t)nslots, 0.0);
 #pragma omp parallel for schedule(static)
   for (int sl = 0; sl < ns; ++sl) {
     const long long b0 = sptr[sl];
     const int len = (int)((sptr[sl + 1] - b0) >> 5);
-    std::vector<std::pair<int, float>> row((size_t)len);
+    struct E {
+      int c;
+      float v;
+      double lv;
+    };
+    std::vector<E> row((size_t)len);
     for (int l = 0; l < 32; ++l) {
       int m = 0;
       for (int j = 0; j < len; ++j) {
         const long long k = b0 + 32LL * j + l;
         const int c = col[k];
-        if (c >= 0 && c < nu) row[m++] = {c, val[k]};
+        if (c >= 0 && c < nu) row[m++] = {c, val[k], lval[k]};
       }
       std::stable_sort(row.begin(), row.begin() + m,
-                       [](const std::pair<int, float>& x, const std::pair<int, float>& y) {
-                         return x.first < y.first;
-                       });
+                       [](const E& x, const E& y) { return x.c < y.c; });
       for (int j = 0; j < len; ++j) {
         const long long k = b0 + 32LL * j + l;
-        col[k] = j < m ? row[j].first : -1;
-        val[k] = j < m ? row[j].second : 0.0f;
+        col[k] = j < m ? row[j].c : -1;
+        val[k] = j < m ? row[j].v : 0.0f;
+        lval_sorted[k] = j < m ? row[j].lv : 0.0;
       }
     }
   }
@@ -1072,6 +1192,69 @@ int Pcg::build_compressed(cudaStream_t s) {
                          (double)plain_slots * 8.0 + (double)(ns - packed_slices) * 16.0 +
                          (double)ns + (double)L->nrows * 16.0;
   cop.enabled = true;
+  // The FP64 residual from the same packed columns: a 4-bit index per slot into a table of
+  // L's (at most 15 distinct nonzero) values in the sorted slot order.  Left off when L has
+  // more values, or a slot the FP32 packing dropped (a stored zero of S L S) holds a
+  // nonzero of L.
+  lpacked = false;
+  if (!getenv("GIPB200_NO_PACKED_RESIDUAL") && lval_sorted.size() == (size_t)nslots) {
+    std::vector<unsigned long long> lkeys;
+    bool ok = true;
+    for (long long k = 0; k < nslots && ok; ++k) {
+      if (col[k] < 0) continue;
+      const double v = lval_sorted[(size_t)k];
+      if (val[k] == 0.0f) {
+        ok = v == 0.0;
+        continue;
+      }
+      unsigned long long bits;
+      memcpy(&bits, &v, 8);
+      if (v != 0.0 && std::find(lkeys.begin(), lkeys.end(), bits) == lkeys.end()) {
+        if (lkeys.size() >= 15) ok = false;
+        else lkeys.push_back(bits);
+      }
+    }
+    if (ok) {
+      std::sort(lkeys.begin(), lkeys.end());
+      std::vector<double> ltab(16, 0.0);
+      for (size_t t = 0; t < lkeys.size(); ++t) memcpy(&ltab[t + 1], &lkeys[t], 8);
+      std::vector<unsigned> lidx(nrow_pad, 0u);
+#pragma omp parallel for schedule(static)
+      for (int sl = 0; sl < ns; ++sl) {
+        if (plain[sl]) continue;
+        const long long b0 = sptr[sl];
+        const int len = (int)((sptr[sl + 1] - b0) >> 5);
+        for (int l = 0; l < 32; ++l) {
+          unsigned w = 0u;
+          for (int j = 0; j < len; ++j) {
+            const long long k = b0 + 32LL * j + l;
+            if (col[k] < 0 || val[k] == 0.0f) continue;
+            const double v = lval_sorted[(size_t)k];
+            unsigned long long bits;
+            memcpy(&bits, &v, 8);
+            const unsigned t =
+                v == 0.0 ? 0u
+                         : 1u + (unsigned)(std::lower_bound(lkeys.begin(), lkeys.end(), bits) -
+                                           lkeys.begin());
+            w |= t << (4 * j);
+          }
+          lidx[(size_t)sl * 32 + l] = w;
+        }
+      }
+      GIPB_TRY(lidx4.upload(lidx.data(), lidx.size(), s));
+      GIPB_TRY(ltable.upload(ltab.data(), ltab.size(), s));
+      const int ng = (int)ghost_rows.size();
+      GIPB_TRY(d_ghost_rows.upload(ghost_rows.data(), std::max(ng, 1), s));
+      GIPB_TRY(d_ghost_rp.upload(ghost_rp.data(), ghost_rp.size(), s));
+      GIPB_TRY(d_ghost_col.upload(ghost_col.data(), std::max<size_t>(ghost_col.size(), 1), s));
+      GIPB_TRY(d_ghost_val.upload(ghost_val.data(), std::max<size_t>(ghost_val.size(), 1), s));
+      GIPB_TRY(bprime.alloc((size_t)std::max(n, 1)));
+      GIPB_CUDA(cudaStreamSynchronize(s));
+      lpacked = true;
+    }
+  }
+  lval_sorted.clear();
+  lval_sorted.shrink_to_fit();
   return GIPB200_OK;
 }
 
@@ -1097,6 +1280,9 @@ double Pcg::iteration_bytes() const {
 double Pcg::replacement_bytes() const {
   if (prm.mode != GIPB200_PCG_MIXED) return 0.0;
   const double nn = n;
+  if (lpacked)  // packed columns, value indices, slot bases, b', scale read, r^ written, fold
+    return (16.0 + 4.0 + 8.0 + 8.0 + 4.0) * nn + 32.0 * L->nslices + 8.0 * n_all +
+           (16.0 + 8.0 + 4.0 + 4.0) * nn;
   // FP64 r = b - L x with the FP32 restart (L, x gathered, b, scale read, r^ written) and
   // the fold x += S y + kappa, y = 0
   return 12.0 * L->nnz + (L->nslices + 1.0) * 8.0 + 8.0 * n_all + 16.0 * nn + 4.0 * nn +
@@ -1383,6 +1569,30 @@ static void launch_mx_spmv(const Pcg& P, const float* pin, float* pout, const fl
 
 int Pcg::launch_mixed_residual(const double* b, const double* x, int first, cudaStream_t s,
                                int use_cond, cudaGraphConditionalHandle h) {
+  if (lpacked) {
+    if (first) {  // b' = b - L_ghost x for this solve (x's ghost entries stay fixed)
+      GIPB_CUDA(cudaMemcpyAsync(bprime.p, b, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                s));
+      const int ng = (int)ghost_rows.size();
+      if (ng > 0) {
+        int gb = 1;
+        GIPB_TRY(grid_blocks(256, ng, 1, 0, &gb));
+        k_mx_ghost_rhs<<<gb, 256, 0, s>>>(ng, d_ghost_rows.p, d_ghost_rp.p, d_ghost_col.p,
+                                          d_ghost_val.p, x, b, bprime.p);
+        launches += 1;
+      }
+    }
+    launch_dep(k_mx_residual_packed, blocks_spmv, 256, s, L->view(),
+               (const uint4*)cop.delta.p, (const int*)cop.base.p,
+               (const unsigned char*)cop.plain.p, (const unsigned*)lidx4.p,
+               (const double*)ltable.p, (const double*)bprime.p, (const double*)x, b,
+               (const double*)scale.p, r32.p, p32.p, y32.p, sc.p, rs, first, prm.tol,
+               prm.inner_tol, prm.maxit, prm.max_outer, pin_row, pin_val, use_cond, h,
+               amg ? 1 : 0);
+    GIPB_LAUNCH_CHECK();
+    launches += 1;
+    return GIPB200_OK;
+  }
   launch_dep(k_mx_residual, blocks_spmv, 256, s, L->view(), (const double*)x, b,
              (const double*)scale.p, r32.p, p32.p, y32.p, sc.p, rs, first, prm.tol, prm.inner_tol,
              prm.maxit, prm.max_outer, pin_row, pin_val, use_cond, h, amg ? 1 : 0);

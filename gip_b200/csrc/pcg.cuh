@@ -86,6 +86,19 @@ struct Pcg {
   double iteration_bytes() const;
   double replacement_bytes() const;
   int sort_fp32_rows(cudaStream_t s);
+  // Packed FP64 residual of the mixed form (r = b - L x from the packed operator's columns
+  // and a table of L's values): L's inner values in the sorted slot order and its ghost
+  // entries (host, set-up only), then on the device the value indices, the table, the
+  // ghost rows and the right-hand side less the ghost part (constant during a solve).
+  std::vector<double> lval_sorted;
+  std::vector<int> ghost_rows, ghost_rp, ghost_col;
+  std::vector<double> ghost_val;
+  bool lpacked = false;
+  DevBuf<unsigned> lidx4;      // per row, 8 x 4 bits into ltable
+  DevBuf<double> ltable;       // 16 entries, index 0 = 0.0
+  DevBuf<int> d_ghost_rows, d_ghost_rp, d_ghost_col;
+  DevBuf<double> d_ghost_val;
+  DevBuf<double> bprime;       // b - L_ghost x_ghost
   void launch_pcg_update(double* x, cudaStream_t s);
   int build_compressed(cudaStream_t s);
   SellView<float> a32() const {

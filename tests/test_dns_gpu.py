@@ -291,3 +291,27 @@ def test_merged_face_operators_are_exact(gpu, monkeypatch, general):
     P.advance(3)
     for k in ("u", "v", "w", "p", "mf"):
         assert np.array_equal(E.field(k), P.field(k)), k
+
+
+@pytest.mark.parametrize("precond", ["amg", "jacobi"])
+def test_packed_fp64_residual_matches_sliced(gpu, monkeypatch, precond):
+    # the mixed form's FP64 residual from the packed operator's columns (L's values from a
+    # table, the ghost part of b - L x formed once per solve) against the sliced FP64 L: the
+    # same solve to rounding, the same iteration counts to within one
+    from gip_b200.device import DnsEngine
+    case, _ = cavity.generate(20, re=400.0, permute_seed=3)
+    kw = dict(gamma=1.0 / 400, pcg_mode="mixed", maxit=4000, tol=1e-9,
+              inner_tol=0.01 if precond == "amg" else 0.3, max_outer=200, reorder=True,
+              precond=precond)
+    E = DnsEngine(case, **kw)
+    monkeypatch.setenv("GIPB200_NO_PACKED_RESIDUAL", "1")
+    F = DnsEngine(case, **kw)
+    E.advance(4)
+    F.advance(4)
+    he, hf = E.history(), F.history()
+    assert np.all(np.abs(he["iters"] - hf["iters"]) <= 1), (he["iters"], hf["iters"])
+    assert np.all(he["massr"] < 1e-8)
+    scale = np.abs(F.field("u")).max()
+    for k in ("u", "v", "w"):
+        assert np.abs(E.field(k) - F.field(k)).max() / scale < 1e-8, k
+    assert np.abs(E.field("p") - F.field("p")).max() / np.abs(F.field("p")).max() < 1e-7
