@@ -51,7 +51,8 @@ class DnsParams(C.Structure):
 class PcgInfo(C.Structure):
     _fields_ = [("pin_row", C.c_int), ("compressed", C.c_int), ("value_table", C.c_int),
                 ("compressed_fraction", C.c_double), ("amg_levels", C.c_int),
-                ("amg_complexity", C.c_double), ("amg_setup_s", C.c_double)]
+                ("amg_complexity", C.c_double), ("amg_setup_s", C.c_double),
+                ("packed_residual", C.c_int)]
 
 
 class DnsInfo(C.Structure):
@@ -59,7 +60,8 @@ class DnsInfo(C.Structure):
                 ("value_table", C.c_int), ("compressed_fraction", C.c_double),
                 ("slots_L", C.c_longlong), ("nnz_L", C.c_longlong), ("amg_levels", C.c_int),
                 ("amg_complexity", C.c_double), ("amg_setup_s", C.c_double),
-                ("iteration_bytes", C.c_double), ("replacement_bytes", C.c_double)]
+                ("iteration_bytes", C.c_double), ("replacement_bytes", C.c_double),
+                ("packed_residual", C.c_int)]
 
 
 class CgScalars(C.Structure):

@@ -1408,6 +1408,7 @@ int gipb200_dns_get_info(gipb200_dns Dh, gipb200_dns_info* info) {
   info->amg_setup_s = amg ? amg->setup_s : amg64 ? amg64->setup_s : 0.0;
   info->iteration_bytes = E.pcg.iteration_bytes();
   info->replacement_bytes = E.pcg.replacement_bytes();
+  info->packed_residual = E.pcg.lpacked ? 1 : 0;
   return GIPB200_OK;
 }
 

@@ -1841,6 +1841,7 @@ int gipb200_pcg_get_info(gipb200_pcg S, gipb200_pcg_info* info) {
   info->amg_levels = amg ? (int)amg->lv.size() : amg64 ? (int)amg64->lv.size() : 0;
   info->amg_complexity = amg ? amg->op_complexity : amg64 ? amg64->op_complexity : 0.0;
   info->amg_setup_s = amg ? amg->setup_s : amg64 ? amg64->setup_s : 0.0;
+  info->packed_residual = lpacked ? 1 : 0;
   return GIPB200_OK;
 }
 

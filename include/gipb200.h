@@ -208,6 +208,7 @@ typedef struct {
   int amg_levels;              /* AMG: levels of the hierarchy (0: no AMG)                */
   double amg_complexity;       /* AMG: operator nonzeros of all levels / of the finest     */
   double amg_setup_s;          /* AMG: host setup time                                    */
+  int packed_residual;         /* MIXED: FP64 residual from the packed columns (1) or L   */
 } gipb200_pcg_info;
 int gipb200_pcg_get_info(gipb200_pcg S, gipb200_pcg_info* info);
 /* No counterpart in the reference: times `reps` launches of the solver's SpMV-dot kernel
@@ -362,6 +363,7 @@ typedef struct {
   double amg_setup_s;          /* AMG: host setup time                                   */
   double iteration_bytes;      /* algorithmic bytes of one PCG iteration (with V-cycle)   */
   double replacement_bytes;    /* MIXED: bytes of one FP64 residual replacement           */
+  int packed_residual;         /* MIXED: FP64 residual from the packed columns (1) or L   */
 } gipb200_dns_info;
 int gipb200_dns_get_info(gipb200_dns E, gipb200_dns_info* info);
 

@@ -306,6 +306,7 @@ def test_packed_fp64_residual_matches_sliced(gpu, monkeypatch, precond):
     E = DnsEngine(case, **kw)
     monkeypatch.setenv("GIPB200_NO_PACKED_RESIDUAL", "1")
     F = DnsEngine(case, **kw)
+    assert E.info()["packed_residual"] == 1 and F.info()["packed_residual"] == 0
     E.advance(4)
     F.advance(4)
     he, hf = E.history(), F.history()
