@@ -1244,10 +1244,11 @@ int Pcg::build_compressed(cudaStream_t s) {
       GIPB_TRY(lidx4.upload(lidx.data(), lidx.size(), s));
       GIPB_TRY(ltable.upload(ltab.data(), ltab.size(), s));
       const int ng = (int)ghost_rows.size();
-      GIPB_TRY(d_ghost_rows.upload(ghost_rows.data(), std::max(ng, 1), s));
+      // (an empty list uploads nothing: the buffer keeps its one-element minimum)
+      GIPB_TRY(d_ghost_rows.upload(ghost_rows.data(), (size_t)ng, s));
       GIPB_TRY(d_ghost_rp.upload(ghost_rp.data(), ghost_rp.size(), s));
-      GIPB_TRY(d_ghost_col.upload(ghost_col.data(), std::max<size_t>(ghost_col.size(), 1), s));
-      GIPB_TRY(d_ghost_val.upload(ghost_val.data(), std::max<size_t>(ghost_val.size(), 1), s));
+      GIPB_TRY(d_ghost_col.upload(ghost_col.data(), ghost_col.size(), s));
+      GIPB_TRY(d_ghost_val.upload(ghost_val.data(), ghost_val.size(), s));
       GIPB_TRY(bprime.alloc((size_t)std::max(n, 1)));
       GIPB_CUDA(cudaStreamSynchronize(s));
       lpacked = true;
@@ -1841,7 +1842,7 @@ int gipb200_pcg_get_info(gipb200_pcg S, gipb200_pcg_info* info) {
   info->amg_levels = amg ? (int)amg->lv.size() : amg64 ? (int)amg64->lv.size() : 0;
   info->amg_complexity = amg ? amg->op_complexity : amg64 ? amg64->op_complexity : 0.0;
   info->amg_setup_s = amg ? amg->setup_s : amg64 ? amg64->setup_s : 0.0;
-  info->packed_residual = lpacked ? 1 : 0;
+  info->packed_residual = S->P.lpacked ? 1 : 0;
   return GIPB200_OK;
 }
 
