@@ -412,6 +412,16 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool c
     GIPB_CUDA(cudaStreamSynchronize(s));
     return GIPB200_OK;
   }
+  // The FP32 cycle's sliced operators with rows of two or more 8-slot batches on average
+  // run software-pipelined (k_amg_spmv_pf at 4 CTAs per SM): the 256^3 cavity's level-0
+  // restriction (29 entries per row) 114.9 against 123.1 us.  Rows of one batch lose more
+  // to the halved occupancy than the overlap gains (its level-0 prolongation: 209.5 against
+  // 143.2 us).  GIPB200_AMG_PIPE=0: never; =1: every sliced FP32 operator (read per call).
+  {
+    const char* pe = getenv("GIPB200_AMG_PIPE");
+    const bool f32 = std::is_same<T, float>::value;
+    S->pipe = f32 && (pe ? atoi(pe) == 1 : avg >= 16.0) ? 1 : 0;
+  }
   std::vector<long long> sptr((size_t)S->nslices + 1, 0);
   for (int sl = 0; sl < S->nslices; ++sl) {
     int len = 0;
@@ -617,6 +627,105 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? 6 : 8) k_amg_spmv(SellVi
                                  (gridDim.x * blockDim.x) >> 5);
 }
 
+// The sliced products software-pipelined over each warp's sequence of 8-slot batches: the
+// loads of the next batch (in this slice, or in the warp's next slice, whose slot range is
+// read one slice ahead) are issued before the gathers of the current one, and a slice's
+// row operands (b, dinv, x, y, yperm) before its first gathers, so a warp always has
+// operator words in flight.  The same fused multiply-adds in the same order as sell_rows
+// (batches of 8 slots from slot 0), so the results are identical.  OCC: resident CTAs per
+// SM it is compiled for (the second batch in registers lowers the CTAs that fit: 64
+// registers a thread at 4, no spills).
+template <typename V>
+__device__ __forceinline__ void sell_batch(const SellView<V>& A, long long base, int len, int j0,
+                                           int lane, int (&c)[8], V (&v)[8]) {
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const bool in = j0 + t < len;
+    c[t] = in ? ld_stream(A.col + base + 32LL * (j0 + t) + lane) : -1;
+    v[t] = in ? ld_stream(A.val + base + 32LL * (j0 + t) + lane) : V(0.0f);
+  }
+}
+
+template <typename T, int MODE, typename V, bool XS, int OCC>
+__global__ void __launch_bounds__(256, OCC) k_amg_spmv_pf(SellView<V> A, const T* __restrict__ x,
+                                                          const T* __restrict__ b,
+                                                          const T* __restrict__ dinv,
+                                                          T* __restrict__ y, PcgScalars* S, T w,
+                                                          const int* __restrict__ yperm,
+                                                          const T* __restrict__ xs) {
+  if (amg_enter(S)) return;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (s >= A.nslices) return;
+  long long base, nbase = 0;
+  int len, nlen = 0;
+  slice_range(A, s, base, len);
+  int sn = s + nw;
+  if (sn < A.nslices) slice_range(A, sn, nbase, nlen);
+  // row operands of slice s (the writes below need them; loaded ahead of the gathers)
+  T rb = T(0), rd = T(0), rx = T(0);
+  int ri = 0;
+  auto row_ops = [&](int sl) {
+    const int i = sl * 32 + lane;
+    if (i < A.nrows) {
+      if (MODE != kPlain && MODE != kAdd) rb = b[i];
+      if (MODE == kAdd) rb = y[i];
+      if (MODE == kDiagAdd || MODE == kSmooth) rd = dinv[i];
+      if (MODE == kSmooth) rx = x[i];
+      if (MODE == kResid) ri = yperm ? yperm[i] : i;
+    }
+  };
+  row_ops(s);
+  int c[8];
+  V v[8];
+  sell_batch(A, base, len, 0, lane, c, v);
+  int j0 = 0;
+  T sum = T(0);
+  while (true) {
+    const bool last = j0 + 8 >= len;
+    const bool more = !last || sn < A.nslices;
+    int cn[8];
+    V vn[8];
+    if (more) {
+      sell_batch(A, last ? nbase : base, last ? nlen : len, last ? 0 : j0 + 8, lane, cn, vn);
+    } else {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) cn[t] = -1, vn[t] = V(0.0f);
+    }
+    T xv[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      xv[t] = (c[t] >= 0) ? (XS ? mulr(__ldg(xs + c[t]), __ldg(x + c[t])) : __ldg(x + c[t])) : T(0);
+#pragma unroll
+    for (int t = 0; t < 8; ++t) sum = fmat(xv[t], (T)to_arith(v[t]), sum);
+    if (last) {
+      const int i = s * 32 + lane;
+      if (i < A.nrows) {
+        if (MODE == kResid) y[ri] = (w == T(1)) ? rb - sum : fmat(-w, sum, rb);
+        else if (MODE == kPlain) y[i] = sum;
+        else if (MODE == kAdd) y[i] = rb + sum;
+        else if (MODE == kScaleAdd) y[i] = fmat(w, rb, sum);
+        else if (MODE == kDiagAdd) y[i] = addr(mulr(rd, rb), sum);
+        else y[i] = fmat(rd, rb - sum, rx);
+      }
+      if (!more) break;
+      s = sn;
+      base = nbase;
+      len = nlen;
+      sn = s + nw;
+      if (sn < A.nslices) slice_range(A, sn, nbase, nlen);
+      row_ops(s);
+      sum = T(0);
+      j0 = 0;
+    } else {
+      j0 += 8;
+    }
+#pragma unroll
+    for (int t = 0; t < 8; ++t) c[t] = cn[t], v[t] = vn[t];
+  }
+}
+
 // The same products from the CSR form: LANES threads per row, each summing a strided part
 // of the row, combined by a fixed shuffle tree (deterministic).  The row loop is uniform
 // across the warp (32 / LANES rows per warp per pass), so every lane takes part in the
@@ -709,6 +818,17 @@ template <typename T, int MODE, typename V, bool XS>
 void amg_mv_vx(const SellT<T>& M, SellView<V> view, const V* v, const T* x, const T* b,
                const T* dinv, T* y, PcgScalars* S, cudaStream_t s, T w, const T* xs) {
   if (M.lanes == 0) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (M.pipe > 0 && !M.short_cols) {
+        constexpr int kOcc = 4;
+        DeviceInfo di;
+        const int nsm = device_info(&di) == GIPB200_OK ? di.nsm : 1;
+        const int nb = std::min(vec_blocks(M.nslices * 32), nsm * kOcc);
+        launch_dep(k_amg_spmv_pf<T, MODE, V, XS, kOcc>, nb, 256, s, view, x, b, dinv, y, S, w,
+                   (const int*)nullptr, xs);
+        return;
+      }
+    }
     if (M.short_cols)
       launch_dep(k_amg_spmv<T, MODE, V, true, XS>, vec_blocks(M.nslices * 32), 256, s, view, x,
                  b, dinv, y, S, w, (const int*)nullptr, xs, (const unsigned short*)M.dcol.p,

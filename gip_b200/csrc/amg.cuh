@@ -31,6 +31,7 @@ struct SellT {
   DevBuf<__half> hval;
   // 16-bit columns: column = cbase[row] + dcol[k], cbase the row's smallest column (every
   // row's columns span at most 65536; in the sliced form 0xffff marks padding slots)
+  int pipe = 0;                // sliced FP32 form: 1 = software-pipelined product (k_amg_spmv_pf)
   bool short_cols = false;
   DevBuf<unsigned short> dcol;
   DevBuf<int> cbase;

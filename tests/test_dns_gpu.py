@@ -219,6 +219,26 @@ def test_amg_packed_level0_is_exact(gpu, monkeypatch):
         assert np.array_equal(E.field(k), P.field(k)), k
 
 
+@pytest.mark.parametrize("pipe", ["0", "1"])
+def test_amg_pipelined_products_are_exact(gpu, monkeypatch, pipe):
+    """The software-pipelined sliced V-cycle products (next batch loaded before the current
+    one's gathers) compute the same sums in the same order: identical steps whether no
+    sliced operator (0), the long-row ones (default) or all of them (1) run pipelined.
+    64^3 has more slices than warps at level 0, so warps walk several slices and batches."""
+    from gip_b200.device import DnsEngine
+    case, _ = cavity.generate(64, re=400.0, permute_seed=3)
+    kw = dict(gamma=1.0 / 400, pcg_mode="mixed", maxit=3000, tol=1e-8, inner_tol=1e-2,
+              max_outer=100, reorder=True, precond="amg")
+    E = DnsEngine(case, **kw)
+    monkeypatch.setenv("GIPB200_AMG_PIPE", pipe)
+    P = DnsEngine(case, **kw)
+    E.advance(2)
+    P.advance(2)
+    assert E.history()["iters"].tolist() == P.history()["iters"].tolist()
+    for k in ("u", "v", "w", "p"):
+        assert np.array_equal(E.field(k), P.field(k)), k
+
+
 def test_step_phases_report_and_advance_like_a_step(gpu):
     # the per-phase report times a real step: same state as a graph-launched step
     from gip_b200.device import DnsEngine
