@@ -61,7 +61,7 @@ class DnsInfo(C.Structure):
                 ("slots_L", C.c_longlong), ("nnz_L", C.c_longlong), ("amg_levels", C.c_int),
                 ("amg_complexity", C.c_double), ("amg_setup_s", C.c_double),
                 ("iteration_bytes", C.c_double), ("replacement_bytes", C.c_double),
-                ("packed_residual", C.c_int)]
+                ("packed_residual", C.c_int), ("value_tables", C.c_int)]
 
 
 class CgScalars(C.Structure):

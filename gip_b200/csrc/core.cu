@@ -201,6 +201,100 @@ int sell_add_fp32(Sell* S, cudaStream_t stream) {
   return GIPB200_OK;
 }
 
+// ------------------------------------------------------------------ value tables
+bool value_table(const double* v, long long n, int cap, std::vector<double>* tab) {
+  std::vector<unsigned long long> keys;
+  bool ok = true;
+#pragma omp parallel
+  {
+    std::vector<unsigned long long> loc;
+    bool lok = true;
+    unsigned long long last = 0;
+    bool have_last = false;
+#pragma omp for schedule(static) nowait
+    for (long long k = 0; k < n; ++k) {
+      if (!lok) continue;
+      unsigned long long b;
+      memcpy(&b, v + k, 8);
+      if (have_last && b == last) continue;
+      if (std::find(loc.begin(), loc.end(), b) == loc.end()) {
+        if ((int)loc.size() >= cap) {
+          lok = false;
+          continue;
+        }
+        loc.push_back(b);
+      }
+      last = b;
+      have_last = true;
+    }
+#pragma omp critical
+    {
+      if (!lok) ok = false;
+      for (unsigned long long b : loc)
+        if (std::find(keys.begin(), keys.end(), b) == keys.end()) keys.push_back(b);
+    }
+  }
+  if (!ok || (int)keys.size() > cap) return false;
+  std::sort(keys.begin(), keys.end());
+  tab->resize(keys.size());
+  for (size_t t = 0; t < keys.size(); ++t) memcpy(&(*tab)[t], &keys[t], 8);
+  return true;
+}
+
+// idx[k] = position of val[k]'s bit pattern in the sorted keys (padding slots: 0); miss
+// counts stored slots whose value the table does not hold.
+__global__ void k_value_index(long long nslots, const double* __restrict__ val,
+                              const int* __restrict__ col, const unsigned long long* __restrict__ keys,
+                              int nkeys, unsigned char* __restrict__ idx, unsigned* miss) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nslots;
+       k += (long long)gridDim.x * blockDim.x) {
+    int t = 0;
+    if (col[k] >= 0) {
+      const unsigned long long b = (unsigned long long)__double_as_longlong(val[k]);
+      int lo = 0, hi = nkeys - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (keys[mid] < b) lo = mid + 1;
+        else hi = mid;
+      }
+      if (keys[lo] != b) atomicAdd(miss, 1u);
+      t = lo;
+    }
+    idx[k] = (unsigned char)t;
+  }
+}
+
+int sell_add_value_table(Sell* S, const double* h_val, long long nnz, cudaStream_t stream) {
+  S->ntab = 0;
+  if (S->nslots == 0 || nnz <= 0 || !h_val || getenv("GIPB200_NO_VALUE_TABLE")) return GIPB200_OK;
+  std::vector<double> tab;
+  if (!value_table(h_val, nnz, 256, &tab) || tab.empty()) return GIPB200_OK;
+  std::vector<unsigned long long> keys(tab.size());
+  for (size_t t = 0; t < tab.size(); ++t) memcpy(&keys[t], &tab[t], 8);
+  DevBuf<unsigned long long> dkeys;
+  DevBuf<unsigned> miss;
+  GIPB_TRY(dkeys.upload(keys.data(), keys.size(), stream));
+  GIPB_TRY(miss.alloc(1));
+  GIPB_TRY(miss.zero(stream));
+  GIPB_TRY(S->vidx.alloc((size_t)S->nslots));
+  int blocks;
+  GIPB_TRY(grid_blocks(256, (int)std::min<long long>(S->nslots, 1 << 30), 1, 0, &blocks));
+  k_value_index<<<blocks, 256, 0, stream>>>(S->nslots, S->val.p, S->col.p, dkeys.p,
+                                            (int)keys.size(), S->vidx.p, miss.p);
+  GIPB_LAUNCH_CHECK();
+  unsigned h_miss = 0;
+  GIPB_CUDA(cudaMemcpyAsync(&h_miss, miss.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+  GIPB_CUDA(cudaStreamSynchronize(stream));
+  if (h_miss) {  // slot values that are not the CSR values: keep the direct layout only
+    S->vidx.release();
+    return GIPB200_OK;
+  }
+  GIPB_TRY(S->vtab.upload(tab.data(), tab.size(), stream));
+  GIPB_CUDA(cudaStreamSynchronize(stream));
+  S->ntab = (int)tab.size();
+  return GIPB200_OK;
+}
+
 // ------------------------------------------------------------------ SpMV kernels
 // mode 0: y = Ax; mode 1: y = alpha Ax + beta y.  Rows without nonzeros keep y.
 __global__ void __launch_bounds__(256) k_sell_spmv(SellView<double> A, const double* __restrict__ x,
@@ -234,6 +328,36 @@ __global__ void __launch_bounds__(256) k_csr_spmv(int nrows, const int* __restri
     const int o = ypos ? ypos[r] : r;
     y[o] = mode ? dadd(dmul(alpha, sum), dmul(beta, y[o])) : sum;
   }
+}
+
+// k_csr_spmv with the stored values read through a value table (vidx, vtab)
+__global__ void __launch_bounds__(256) k_csr_spmv_tab(int nrows, const int* __restrict__ rp,
+                                                      const int* __restrict__ col,
+                                                      const unsigned char* __restrict__ vidx,
+                                                      const double* __restrict__ vtab,
+                                                      const double* __restrict__ x, double* y,
+                                                      const int* __restrict__ ypos, double alpha,
+                                                      double beta, int mode) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
+    const int jb = rp[r], je = rp[r + 1];
+    if (jb == je) continue;
+    double sum = 0.0;
+    for (int j = jb; j < je; ++j) sum = dadd(sum, dmul(__ldg(x + col[j]), __ldg(vtab + vidx[j])));
+    const int o = ypos ? ypos[r] : r;
+    y[o] = mode ? dadd(dmul(alpha, sum), dmul(beta, y[o])) : sum;
+  }
+}
+
+int launch_csr_spmv_tab(int nrows, const int* rowptr, const int* col, const unsigned char* vidx,
+                        const double* vtab, const double* x, double* y, const int* ypos,
+                        double alpha, double beta, int mode, cudaStream_t s) {
+  if (nrows == 0) return GIPB200_OK;
+  int blocks;
+  GIPB_TRY(grid_blocks(256, nrows, 1, 0, &blocks));
+  k_csr_spmv_tab<<<blocks, 256, 0, s>>>(nrows, rowptr, col, vidx, vtab, x, y, ypos, alpha, beta,
+                                        mode);
+  GIPB_LAUNCH_CHECK();
+  return GIPB200_OK;
 }
 
 int launch_sell_spmv(const Sell& A, const double* vals, const double* x, double* y, double alpha,

@@ -160,16 +160,26 @@ __device__ __forceinline__ unsigned packed_index(const PackedWords& w, int j) {
   return (NIB == 4) ? (w.w0 >> (4 * j)) & 15u : ((j < 4 ? w.w0 : w.w1) >> (8 * (j & 3))) & 255u;
 }
 
+// Stored value of slot k: through the operator's value table (TAB: one byte per slot into
+// vtab, the same doubles) or read directly.  A compile-time choice, like every switch in a
+// gather loop.
+template <bool TAB, typename V>
+__device__ __forceinline__ V sell_value(const SellView<V>& A, long long k) {
+  if constexpr (TAB)
+    return __ldg(A.vtab + ld_stream(A.vidx + k));
+  else
+    return ld_stream(A.val + k);
+}
+
 // One row of a SELL-32 matrix, summed slot by slot in CSR order with GIP's rounding.
 // `any` reports whether the row has at least one stored nonzero.
-template <typename V, typename X, int CH = 8>
+template <typename V, typename X, int CH = 8, bool TAB = false>
 __device__ __forceinline__ void sell_row_f64(const SellView<V>& A, const X* __restrict__ x,
                                              int s, int lane, double& sum, bool& any) {
   long long base;
   int len;
   slice_range(A, s, base, len);
   const int* cp = A.col + base + lane;
-  const V* vp = A.val + base + lane;
   for (int j0 = 0; j0 < len; j0 += CH) {
     int c[CH];
     V v[CH];
@@ -177,7 +187,7 @@ __device__ __forceinline__ void sell_row_f64(const SellView<V>& A, const X* __re
     for (int t = 0; t < CH; ++t) {
       if (j0 + t < len) {
         c[t] = ld_stream(cp + (size_t)(j0 + t) * 32);
-        v[t] = ld_stream(vp + (size_t)(j0 + t) * 32);
+        v[t] = sell_value<TAB>(A, base + (long long)(j0 + t) * 32 + lane);
       } else {
         c[t] = -1;
         v[t] = V(0);
@@ -240,6 +250,7 @@ __device__ __forceinline__ void sell_row_f64_pair(const SellView<V>& A, const do
 // by slot with GIP's rounding, any_k = the row has a stored nonzero): the slot loads of all
 // three and then their gathers are in flight at once, three dependent round trips per row
 // instead of nine.  The same results as three sell_row_f64 calls.
+template <bool TAB = false>
 __device__ __forceinline__ void sell_rows3_f64(const SellView<double> (&M)[3],
                                                const double* const (&x)[3], int s, int lane,
                                                double (&sum)[3], bool (&any)[3]) {
@@ -263,7 +274,7 @@ __device__ __forceinline__ void sell_rows3_f64(const SellView<double> (&M)[3],
       for (int t = 0; t < 2; ++t) {
         const int j = j0 + t;
         c[k][t] = (j < len[k]) ? ld_stream(M[k].col + base[k] + 32LL * j + lane) : -1;
-        v[k][t] = (j < len[k]) ? ld_stream(M[k].val + base[k] + 32LL * j + lane) : 0.0;
+        v[k][t] = (j < len[k]) ? sell_value<TAB>(M[k], base[k] + 32LL * j + lane) : 0.0;
       }
 #pragma unroll
     for (int k = 0; k < 3; ++k)

@@ -25,6 +25,7 @@ namespace gipb200 {
 // ------------------------------------------------------------------ row helpers
 // D and C share D's sparsity (GIP loads C from D's file, GIP_DNS.h:150-151): one pass
 // over the slots yields D u, D v, D w, C u, C v, C w, each summed in CSR order.
+template <bool TAB>
 __device__ __forceinline__ void dc_row(const SellView<double>& D, const double* __restrict__ cval,
                                        const double* __restrict__ u, const double* __restrict__ v,
                                        const double* __restrict__ w, int s, int lane,
@@ -42,7 +43,7 @@ __device__ __forceinline__ void dc_row(const SellView<double>& D, const double* 
       const bool in = j0 + t < len;
       const long long k = base + 32LL * (j0 + t) + lane;
       c[t] = in ? ld_stream(D.col + k) : -1;
-      dv[t] = in ? ld_stream(D.val + k) : 0.0;
+      dv[t] = in ? sell_value<TAB>(D, k) : 0.0;
       cv[t] = in ? ld_stream(cval + k) : 0.0;
     }
     double xu[2], xv[2], xw[2];
@@ -73,6 +74,7 @@ __device__ __forceinline__ double axpby_row(double alpha, double sum, double bet
 
 // ------------------------------------------------------------------ PredictorVelocity
 // ax = D u; ax = -C u + ax  (and v, w)   -- GIP_DNS.h:313-318
+template <bool TAB>
 __global__ void __launch_bounds__(256) k_dns_convdiff(SellView<double> D,
                                                       const double* __restrict__ cval,
                                                       const double* __restrict__ u,
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(256) k_dns_convdiff(SellView<double> D,
   for (int s = gw; s < D.nslices; s += nw) {
     double sd[3] = {0.0, 0.0, 0.0}, sc[3] = {0.0, 0.0, 0.0};
     bool any = false;
-    dc_row(D, cval, u, v, w, s, lane, sd, sc, any);
+    dc_row<TAB>(D, cval, u, v, w, s, lane, sd, sc, any);
     const int i = s * 32 + lane;
     if (i < D.nrows && any) {
       ax[i] = axpby_row(-1.0, sc[0], 1.0, sd[0]);
@@ -119,6 +121,7 @@ __global__ void __launch_bounds__(256) k_dns_ab2(int n, double* __restrict__ u, 
 
 // ------------------------------------------------------------------ PoissonEquation rhs
 // rhs = Mx u; rhs = My v + rhs; rhs = sigma Mz w + sigma rhs   -- GIP_DNS.h:343-345
+template <bool TAB>
 __global__ void __launch_bounds__(256) k_dns_rhs(SellView<double> Mx, SellView<double> My,
                                                  SellView<double> Mz, const double* __restrict__ u,
                                                  const double* __restrict__ v,
@@ -135,7 +138,7 @@ __global__ void __launch_bounds__(256) k_dns_rhs(SellView<double> Mx, SellView<d
     const double* const X[3] = {u, v, w};
     double sm[3] = {0, 0, 0};
     bool an[3] = {false, false, false};
-    sell_rows3_f64(M, X, s, lane, sm, an);
+    sell_rows3_f64<TAB>(M, X, s, lane, sm, an);
     const double sx = sm[0], sy = sm[1], sz = sm[2];
     bool ax = an[0], ay = an[1], az = an[2];
     ax = ax && i < Mx.nrows;
@@ -163,6 +166,7 @@ __global__ void k_dns_pcopy(int n_inner, int n_owned, double* __restrict__ p, do
 
 // ------------------------------------------------------------------ VelocityCorrection
 // gp = G p (x,y,z); u -= gp/(rho sigma) over the inner cells   -- GIP_DNS.h:359-370
+template <bool TAB>
 __global__ void __launch_bounds__(256) k_dns_gradcorr(SellView<double> Gx, SellView<double> Gy,
                                                       SellView<double> Gz, const double* __restrict__ p,
                                                       double* __restrict__ gpx, double* __restrict__ gpy,
@@ -180,7 +184,7 @@ __global__ void __launch_bounds__(256) k_dns_gradcorr(SellView<double> Gx, SellV
     const double* const X[3] = {p, p, p};
     double sm[3] = {0, 0, 0};
     bool an[3] = {false, false, false};
-    sell_rows3_f64(G, X, s, lane, sm, an);
+    sell_rows3_f64<TAB>(G, X, s, lane, sm, an);
     const double sx = sm[0], sy = sm[1], sz = sm[2];
     const bool ax = an[0], ay = an[1], az = an[2];
     if (ax && i < Gx.nrows) gpx[i] = sx;
@@ -293,6 +297,7 @@ __global__ void __launch_bounds__(256) k_dns_massflux3(
 // operator only (a structured grid's face is an x, y or z face): one gradient and one
 // velocity sum per face, so the kernel fits the registers of six blocks per SM.  The
 // updates keep their order: mf = fact1 SO p (a0), then fact2 SF_d gp_d, then rho SF_d u_d.
+template <bool TAB>
 __global__ void __launch_bounds__(256, 5) k_dns_massflux1(
     SellView<double> SO, SellView<double> SF, const unsigned short* __restrict__ cnt,
     const double* __restrict__ p, const double* __restrict__ gpx, const double* __restrict__ gpy,
@@ -332,9 +337,9 @@ __global__ void __launch_bounds__(256, 5) k_dns_massflux1(
       for (int t = 0; t < 2; ++t) {
         const int j = j0 + t;
         oc[t] = (j < ol) ? ld_stream(SO.col + ob + 32LL * j + lane) : -1;
-        ov[t] = (j < ol) ? ld_stream(SO.val + ob + 32LL * j + lane) : 0.0;
+        ov[t] = (j < ol) ? sell_value<TAB>(SO, ob + 32LL * j + lane) : 0.0;
         fc[t] = (j < fl) ? ld_stream(SF.col + fb + 32LL * j + lane) : -1;
-        fv[t] = (j < fl) ? ld_stream(SF.val + fb + 32LL * j + lane) : 0.0;
+        fv[t] = (j < fl) ? sell_value<TAB>(SF, fb + 32LL * j + lane) : 0.0;
       }
       double op[2], a[2], b[2];
 #pragma unroll
@@ -430,6 +435,7 @@ struct MassrFinish {
 };
 
 // temp = Mres mf; massr = max |temp| over the inner cells   -- GIP_DNS.h:399-400
+template <bool TAB>
 __global__ void __launch_bounds__(256) k_dns_massr(SellView<double> Mres, const double* __restrict__ mf,
                                                    double* __restrict__ temp, int n_inner,
                                                    const DnsScalars* S, DnsHistory H,
@@ -443,7 +449,7 @@ __global__ void __launch_bounds__(256) k_dns_massr(SellView<double> Mres, const 
     const int i = s * 32 + lane;
     double sum = 0;
     bool any = false;
-    if (s < Mres.nslices) sell_row_f64(Mres, mf, s, lane, sum, any);
+    if (s < Mres.nslices) sell_row_f64<double, double, 8, TAB>(Mres, mf, s, lane, sum, any);
     any = any && i < Mres.nrows;
     if (any) temp[i] = sum;
     if (i < n_inner) {
@@ -586,20 +592,31 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync, int part) {
   if (part != 2) {
     mark(0);
     // PredictorVelocity: C's values from the face fluxes, then D/C products and AB2
-    if (ec_slot)
+    if (ec_slot && ec_ntab)
+      GIPB_TRY(launch_csr_spmv_tab(ec_rows, ec_rp.p, ec_col.p, ec_vidx.p, ec_vtab.p, mf.p, cval.p,
+                                   nullptr, 0.0, 0.0, 0, s));
+    else if (ec_slot)
       GIPB_TRY(launch_csr_spmv(ec_rows, ec_rp.p, ec_col.p, ec_val.p, mf.p, cval.p, nullptr, 0.0,
                                0.0, 0, s));
     else
       GIPB_TRY(launch_csr_spmv(Ec.nrows, Ec.rowptr.p, Ec.csr_col.p, Ec.csr_val.p, mf.p, cval.p,
                                D.pos.p, 0.0, 0.0, 0, s));
-    k_dns_convdiff<<<grid.convdiff, 256, 0, s>>>(D.view(), cval.p, u.p, v.p, w.p, ax.p, ay.p,
-                                                 az.p);
+    if (tab_d())
+      k_dns_convdiff<true><<<grid.convdiff, 256, 0, s>>>(D.view(), cval.p, u.p, v.p, w.p, ax.p,
+                                                         ay.p, az.p);
+    else
+      k_dns_convdiff<false><<<grid.convdiff, 256, 0, s>>>(D.view(), cval.p, u.p, v.p, w.p, ax.p,
+                                                          ay.p, az.p);
     k_dns_ab2<<<grid.ab2, 256, 0, s>>>(N, u.p, v.p, w.p, ax.p, ay.p, az.p, ax0.p, ay0.p, az0.p,
                                        sc.p);
     mark(1);
     // PoissonEquation
-    k_dns_rhs<<<grid.rhs, 256, 0, s>>>(Mx.view(), My.view(), Mz.view(), u.p, v.p, w.p, rhs.p,
-                                       sc.p);
+    if (tab_m())
+      k_dns_rhs<true><<<grid.rhs, 256, 0, s>>>(Mx.view(), My.view(), Mz.view(), u.p, v.p, w.p,
+                                               rhs.p, sc.p);
+    else
+      k_dns_rhs<false><<<grid.rhs, 256, 0, s>>>(Mx.view(), My.view(), Mz.view(), u.p, v.p, w.p,
+                                                rhs.p, sc.p);
     GIPB_LAUNCH_CHECK();
     mark(2);
   }
@@ -611,14 +628,24 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync, int part) {
     GIPB_TRY(launch_sell_spmv(Lb, Lb.val.p, p0.p, p.p, 1.0, 1.0, 1, s));
     mark(4);
     // VelocityCorrection
-    k_dns_gradcorr<<<grid.gradcorr, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p, gpx.p,
-                                                 gpy.p, gpz.p, u.p, v.p, w.p, N, prm.rho, sc.p);
+    if (tab_g())
+      k_dns_gradcorr<true><<<grid.gradcorr, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p,
+                                                         gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, N,
+                                                         prm.rho, sc.p);
+    else
+      k_dns_gradcorr<false><<<grid.gradcorr, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p,
+                                                          gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, N,
+                                                          prm.rho, sc.p);
     mark(5);
     // MassFluxes
-    if (SF3.on && SF3.single)
-      k_dns_massflux1<<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p, p.p,
-                                                    gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p,
-                                                    prm.rho, sc.p);
+    if (SF3.on && SF3.single && tab_f())
+      k_dns_massflux1<true><<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p,
+                                                          p.p, gpx.p, gpy.p, gpz.p, u.p, v.p,
+                                                          w.p, mf.p, prm.rho, sc.p);
+    else if (SF3.on && SF3.single)
+      k_dns_massflux1<false><<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p,
+                                                           p.p, gpx.p, gpy.p, gpz.p, u.p, v.p,
+                                                           w.p, mf.p, prm.rho, sc.p);
     else if (SF3.on)
       k_dns_massflux3<<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p, p.p,
                                                     gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p,
@@ -629,7 +656,10 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync, int part) {
                                                    prm.rho, sc.p);
     mark(6);
     // CFLCondition
-    k_dns_massr<<<grid.massr, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
+    if (Mres.ntab)
+      k_dns_massr<true><<<grid.massr, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
+    else
+      k_dns_massr<false><<<grid.massr, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
     k_dns_cfl<<<grid.cfl, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p, H,
                                           pcg.sc.p, 1, prm.pcg.mode == GIPB200_PCG_MIXED,
                                           dt_seq.p, dt_seq_len, rs);
@@ -646,10 +676,14 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync, int part) {
 // Compulsory traffic: every stored value and index once, slice offsets, each gathered
 // vector once, each written vector once (a row without stored nonzeros writes nothing).
 void Dns::phase_bytes(double out[7]) const {
-  auto op = [](const Sell& M) { return 12.0 * M.nnz + 8.0 * (M.nslices + 1.0); };
+  // a tabled operator streams a 4-byte column and a 1-byte value index per nonzero
+  auto op = [](const Sell& M) {
+    return (M.ntab ? 5.0 : 12.0) * M.nnz + 8.0 * (M.nslices + 1.0) + 8.0 * M.ntab;
+  };
   const double n = N, no = NO, nf = NF;
   // predictor: C's values = Ec mf (CSR, rows scattered into C's slots), D/C products, AB2
-  const double ec = ec_slot ? 12.0 * Ec.nnz + 4.0 * (ec_rows + 1.0) + 8.0 * nf + 8.0 * Ec.nrows
+  const double ec = ec_slot ? (ec_ntab ? 5.0 : 12.0) * Ec.nnz + 4.0 * (ec_rows + 1.0) + 8.0 * nf +
+                                  8.0 * Ec.nrows
                             : 12.0 * Ec.nnz + 4.0 * (Ec.nrows + 1.0) + 4.0 * Ec.nrows + 8.0 * nf +
                                   8.0 * Ec.nrows;
   const double cd = op(D) + 8.0 * D.nnz + 24.0 * no + 24.0 * n;
@@ -795,8 +829,12 @@ static int check_op(const gipb200_host_csr& m, const char* name, int rows_max, i
 
 // The engine's sliced operators keep only what it reads: D its CSR columns and slot map
 // (C's values, the adjoint), L everything (the solver's set-up), the others nothing.
-static int build_op(Sell* S, const gipb200_host_csr& m, unsigned keep = 0) {
-  return sell_build(S, m.nrows, m.ncols, m.nnz, m.rowptr, m.col, m.val, 0, keep);
+// table: the phase kernels read the values through a value table where the operator's
+// values allow one (a uniform mesh's operators hold a handful of distinct values).
+static int build_op(Sell* S, const gipb200_host_csr& m, unsigned keep = 0, bool table = false) {
+  GIPB_TRY(sell_build(S, m.nrows, m.ncols, m.nnz, m.rowptr, m.col, m.val, 0, keep));
+  if (table) GIPB_TRY(sell_add_value_table(S, m.val, m.nnz, 0));
+  return GIPB200_OK;
 }
 
 // Sizes of an operator whose sliced layout is never read (phase byte counts only).
@@ -848,7 +886,27 @@ static int build_ec_slot(Dns& E, const gipb200_host_csr& D, const gipb200_host_c
   }
   GIPB_TRY(E.ec_rp.upload(rp.data(), rp.size(), 0));
   GIPB_TRY(E.ec_col.upload(col.data(), std::max<size_t>(col.size(), 1), 0));
-  GIPB_TRY(E.ec_val.upload(val.data(), std::max<size_t>(val.size(), 1), 0));
+  // C's values through a value table of Ec's (few) distinct values where they allow one
+  std::vector<double> tab;
+  E.ec_ntab = 0;
+  if (!getenv("GIPB200_NO_VALUE_TABLE") && !val.empty() &&
+      value_table(val.data(), (long long)val.size(), 256, &tab)) {
+    std::vector<unsigned long long> keys(tab.size());
+    for (size_t t = 0; t < tab.size(); ++t) memcpy(&keys[t], &tab[t], 8);
+    std::vector<unsigned char, NoInitAlloc<unsigned char>> idx(val.size());
+#pragma omp parallel for schedule(static)
+    for (long long e = 0; e < (long long)val.size(); ++e) {
+      unsigned long long b;
+      memcpy(&b, &val[(size_t)e], 8);
+      idx[(size_t)e] =
+          (unsigned char)(std::lower_bound(keys.begin(), keys.end(), b) - keys.begin());
+    }
+    GIPB_TRY(E.ec_vidx.upload(idx.data(), idx.size(), 0));
+    GIPB_TRY(E.ec_vtab.upload(tab.data(), tab.size(), 0));
+    E.ec_ntab = (int)tab.size();
+  } else {
+    GIPB_TRY(E.ec_val.upload(val.data(), std::max<size_t>(val.size(), 1), 0));
+  }
   GIPB_CUDA(cudaStreamSynchronize(0));
   E.ec_rows = (int)nslots;
   E.ec_slot = true;
@@ -899,6 +957,7 @@ static int build_face3(FaceOps3* F, const gipb200_host_csr* const op[3], int NF,
     }
   }
   GIPB_TRY(sell_build(&F->S, NF, NO, (int)col.size(), rp.data(), col.data(), val.data(), 0, 0u));
+  GIPB_TRY(sell_add_value_table(&F->S, val.data(), (long long)val.size(), 0));
   GIPB_TRY(F->cnt.upload(cnt.data(), cnt.size(), 0));
   GIPB_CUDA(cudaStreamSynchronize(0));
   F->on = true;
@@ -1050,7 +1109,7 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     E.setup_s[0] = since(t_begin);  // checks and renumbering
     const auto t_ops = std::chrono::steady_clock::now();
     const gipb200_dns_ops* bops = &rops;
-    GIPB_TRY(build_op(&E.D, bops->D, kKeepDeviceCsr | kKeepPos));
+    GIPB_TRY(build_op(&E.D, bops->D, kKeepDeviceCsr | kKeepPos, true));
     trace("sliced D");
     // Ec is only ever read row by row in CSR form (C's values, the adjoint's convective
     // term): no sliced copy
@@ -1060,19 +1119,19 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     trace("sliced L");
     GIPB_TRY(build_op(&E.Lb, bops->Lb));
     trace("sliced Lb");
-    GIPB_TRY(build_op(&E.Mx, bops->Mx));
+    GIPB_TRY(build_op(&E.Mx, bops->Mx, 0, true));
     trace("sliced Mx");
-    GIPB_TRY(build_op(&E.My, bops->My));
+    GIPB_TRY(build_op(&E.My, bops->My, 0, true));
     trace("sliced My");
-    GIPB_TRY(build_op(&E.Mz, bops->Mz));
+    GIPB_TRY(build_op(&E.Mz, bops->Mz, 0, true));
     trace("sliced Mz");
-    GIPB_TRY(build_op(&E.Mres, bops->Mres));
+    GIPB_TRY(build_op(&E.Mres, bops->Mres, 0, true));
     trace("sliced Mres");
-    GIPB_TRY(build_op(&E.Gx, bops->Gx));
+    GIPB_TRY(build_op(&E.Gx, bops->Gx, 0, true));
     trace("sliced Gx");
-    GIPB_TRY(build_op(&E.Gy, bops->Gy));
+    GIPB_TRY(build_op(&E.Gy, bops->Gy, 0, true));
     trace("sliced Gy");
-    GIPB_TRY(build_op(&E.Gz, bops->Gz));
+    GIPB_TRY(build_op(&E.Gz, bops->Gz, 0, true));
     trace("sliced Gz");
     {
       // SFx, SFy, SFz merged per face where they fit; their own layouts only otherwise
@@ -1089,7 +1148,7 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
       }
     }
     trace("face operators");
-    GIPB_TRY(build_op(&E.SO, bops->SO));
+    GIPB_TRY(build_op(&E.SO, bops->SO, 0, true));
     trace("sliced SO");
     GIPB_TRY(build_ec_slot(E, bops->D, bops->Ec));
     trace("Ec in C's slot order");
@@ -1122,17 +1181,22 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     GIPB_TRY(grid_blocks(256, std::max(NF, 1), 1, kMaxReduceBlocks, &E.blocks_faces));
     GIPB_TRY(grid_blocks(256, NO, 1, kMaxReduceBlocks, &E.blocks_owned));
     GIPB_TRY(grid_blocks(256, N, 4, kMaxReduceBlocks, &E.blocks_vec));
-    GIPB_TRY(one_wave(k_dns_convdiff, E.blocks_cells, &E.grid.convdiff));
+    GIPB_TRY(E.tab_d() ? one_wave(k_dns_convdiff<true>, E.blocks_cells, &E.grid.convdiff)
+                       : one_wave(k_dns_convdiff<false>, E.blocks_cells, &E.grid.convdiff));
     GIPB_TRY(one_wave(k_dns_ab2, E.blocks_vec, &E.grid.ab2));
-    GIPB_TRY(one_wave(k_dns_rhs, E.blocks_cells, &E.grid.rhs));
-    GIPB_TRY(one_wave(k_dns_gradcorr, E.blocks_owned, &E.grid.gradcorr));
+    GIPB_TRY(E.tab_m() ? one_wave(k_dns_rhs<true>, E.blocks_cells, &E.grid.rhs)
+                       : one_wave(k_dns_rhs<false>, E.blocks_cells, &E.grid.rhs));
+    GIPB_TRY(E.tab_g() ? one_wave(k_dns_gradcorr<true>, E.blocks_owned, &E.grid.gradcorr)
+                       : one_wave(k_dns_gradcorr<false>, E.blocks_owned, &E.grid.gradcorr));
     if (E.SF3.on && E.SF3.single)
-      GIPB_TRY(one_wave(k_dns_massflux1, E.blocks_faces, &E.grid.massflux));
+      GIPB_TRY(E.tab_f() ? one_wave(k_dns_massflux1<true>, E.blocks_faces, &E.grid.massflux)
+                         : one_wave(k_dns_massflux1<false>, E.blocks_faces, &E.grid.massflux));
     else if (E.SF3.on)
       GIPB_TRY(one_wave(k_dns_massflux3, E.blocks_faces, &E.grid.massflux));
     else
       GIPB_TRY(one_wave(k_dns_massflux, E.blocks_faces, &E.grid.massflux));
-    GIPB_TRY(one_wave(k_dns_massr, E.blocks_cells, &E.grid.massr));
+    GIPB_TRY(E.Mres.ntab ? one_wave(k_dns_massr<true>, E.blocks_cells, &E.grid.massr)
+                         : one_wave(k_dns_massr<false>, E.blocks_cells, &E.grid.massr));
     GIPB_TRY(one_wave(k_dns_cfl, E.blocks_vec, &E.grid.cfl));
     GIPB_CUDA(cudaStreamCreateWithFlags(&E.cap_stream, cudaStreamNonBlocking));
     GIPB_CUDA(cudaDeviceSynchronize());
@@ -1409,6 +1473,7 @@ int gipb200_dns_get_info(gipb200_dns Dh, gipb200_dns_info* info) {
   info->iteration_bytes = E.pcg.iteration_bytes();
   info->replacement_bytes = E.pcg.replacement_bytes();
   info->packed_residual = E.pcg.lpacked ? 1 : 0;
+  info->value_tables = E.value_tables();
   return GIPB200_OK;
 }
 

@@ -149,6 +149,10 @@ struct SellView {
   const int* __restrict__ col;
   const V* __restrict__ val;
   int uslots;  // > 0: every slice has this many slots (slice s starts at 32 * uslots * s)
+  // optional value table (operators with at most 256 distinct stored values): slot k holds
+  // vtab[vidx[k]], the same double as val[k], in one byte instead of eight
+  const unsigned char* __restrict__ vidx = nullptr;
+  const V* __restrict__ vtab = nullptr;
 };
 
 // Slot range of slice s: computed when the slices are uniform, else read from sptr.
@@ -178,7 +182,14 @@ struct Sell {
   DevBuf<int> csr_col;
   DevBuf<double> csr_val;
   std::vector<int> h_rowptr, h_col;  // host CSR structure (setup only)
-  SellView<double> view() const { return {nrows, nslices, sptr.p, col.p, val.p, uslots}; }
+  // value table (sell_add_value_table): ntab > 0 distinct stored values, vidx per slot
+  int ntab = 0;
+  DevBuf<unsigned char> vidx;
+  DevBuf<double> vtab;
+  SellView<double> view() const {
+    return {nrows, nslices, sptr.p, col.p, val.p, uslots, ntab ? vidx.p : nullptr,
+            ntab ? vtab.p : nullptr};
+  }
   SellView<double> view_vals(const double* v) const {
     return {nrows, nslices, sptr.p, col.p, v, uslots};
   }
@@ -196,6 +207,13 @@ int csr_build(Sell* S, int nrows, int ncols, int nnz, const int* h_rowptr, const
               const double* h_val, cudaStream_t stream);
 // Adds an FP32 value copy.
 int sell_add_fp32(Sell* S, cudaStream_t stream);
+// Adds a value table when the operator's stored values (h_val, its nnz CSR values) take at
+// most 256 distinct doubles (bitwise); else leaves ntab = 0.  Lossless: the table holds
+// the values themselves.
+int sell_add_value_table(Sell* S, const double* h_val, long long nnz, cudaStream_t stream);
+// The table of the distinct doubles (bitwise, sorted by bit pattern) among v[0..n), or
+// false when there are more than `cap`.
+bool value_table(const double* v, long long n, int cap, std::vector<double>* tab);
 int validate_csr(int nrows, int ncols, int nnz, const int* rowptr, const int* col,
                  int col_bound, const char* name);
 
@@ -205,6 +223,10 @@ int launch_sell_spmv(const Sell& A, const double* vals, const double* x, double*
 int launch_csr_spmv(int nrows, const int* rowptr, const int* col, const double* val,
                     const double* x, double* y, const int* ypos, double alpha, double beta,
                     int mode, cudaStream_t s);
+// The same product with the values read through a value table (vtab[vidx[j]]).
+int launch_csr_spmv_tab(int nrows, const int* rowptr, const int* col, const unsigned char* vidx,
+                        const double* vtab, const double* x, double* y, const int* ypos,
+                        double alpha, double beta, int mode, cudaStream_t s);
 int grid_blocks(int threads, int work_items, int per_thread, int max_blocks, int* blocks);
 
 }  // namespace gipb200

@@ -219,6 +219,27 @@ def test_amg_packed_level0_is_exact(gpu, monkeypatch):
         assert np.array_equal(E.field(k), P.field(k)), k
 
 
+@pytest.mark.parametrize("mode", ["fixed", "mixed"])
+def test_value_tables_are_exact(gpu, monkeypatch, mode):
+    """The phase kernels reading their operators' values through 8-bit value tables produce
+    the same doubles as reading them directly: identical steps, every field equal."""
+    from gip_b200.device import DnsEngine
+    case, _ = cavity.generate(24, re=400.0, permute_seed=5)
+    kw = dict(gamma=1.0 / 400, pcg_mode=mode, maxit=400 if mode == "fixed" else 3000, tol=1e-8,
+              inner_tol=0.1, max_outer=100, reorder=True)
+    E = DnsEngine(case, **kw)
+    assert E.info()["value_tables"] == 6
+    monkeypatch.setenv("GIPB200_NO_VALUE_TABLE", "1")
+    P = DnsEngine(case, **kw)
+    assert P.info()["value_tables"] == 0
+    E.advance(4)
+    P.advance(4)
+    assert E.history()["iters"].tolist() == P.history()["iters"].tolist()
+    assert np.array_equal(E.history()["massr"], P.history()["massr"])
+    for k in ("u", "v", "w", "p", "mf", "ax0", "rhs", "gpx", "gpy", "gpz", "temp"):
+        assert np.array_equal(E.field(k), P.field(k)), k
+
+
 @pytest.mark.parametrize("pipe", ["0", "1"])
 def test_amg_pipelined_products_are_exact(gpu, monkeypatch, pipe):
     """The software-pipelined sliced V-cycle products (next batch loaded before the current
