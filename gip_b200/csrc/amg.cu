@@ -412,15 +412,17 @@ int upload(const HCsr& A, SellT<T>* S, cudaStream_t s, bool half = false, bool c
     GIPB_CUDA(cudaStreamSynchronize(s));
     return GIPB200_OK;
   }
-  // The FP32 cycle's sliced operators with rows of two or more 8-slot batches on average
-  // run software-pipelined (k_amg_spmv_pf at 4 CTAs per SM): the 256^3 cavity's level-0
-  // restriction (29 entries per row) 114.9 against 123.1 us.  Rows of one batch lose more
-  // to the halved occupancy than the overlap gains (its level-0 prolongation: 209.5 against
-  // 143.2 us).  GIPB200_AMG_PIPE=0: never; =1: every sliced FP32 operator (read per call).
+  // The FP32 cycle's sliced transfer operators with rows of two or more 8-slot batches on
+  // average run software-pipelined (k_amg_spmv_pf at 4 CTAs per SM): the 256^3 cavity's
+  // level-0 restriction (29 entries per row) 116.5 against 123.1 us.  Rows of one batch
+  // lose more to the halved occupancy than the overlap gains (its level-0 prolongation:
+  // 209.5 against 143.2 us), and the level-1 operator (21 per row) gained nothing (73.2
+  // against 71.9 us).  GIPB200_AMG_PIPE=0: never; =1: every sliced FP32 operator (read per
+  // call).
   {
     const char* pe = getenv("GIPB200_AMG_PIPE");
     const bool f32 = std::is_same<T, float>::value;
-    S->pipe = f32 && (pe ? atoi(pe) == 1 : avg >= 16.0) ? 1 : 0;
+    S->pipe = f32 && (pe ? atoi(pe) == 1 : transfer && avg >= 16.0) ? 1 : 0;
   }
   std::vector<long long> sptr((size_t)S->nslices + 1, 0);
   for (int sl = 0; sl < S->nslices; ++sl) {
