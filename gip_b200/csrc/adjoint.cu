@@ -163,6 +163,7 @@ struct Adjoint {
   int N = 0, NO = 0, NF = 0, nnzD = 0, n_lid = 0;
   std::vector<double> u0, v0, w0;          // initial fields (host)
   DevBuf<double> dval0;                    // D_given in D's sliced layout
+  DevBuf<double> dtab0;                    // D_given's value table (when D has one)
   DevBuf<double> cval0;                    // C's initial values (= D_given, CSR order)
   DevBuf<double> vol;
   DevBuf<int> lid;
@@ -391,6 +392,11 @@ int gipb200_adjoint_create(const gipb200_dns_ops* ops, const double* h_u0, const
     A.w0.assign(h_w0, h_w0 + NO);
     GIPB_TRY(A.dval0.alloc(A.E.D.val.n));
     GIPB_CUDA(cudaMemcpy(A.dval0.p, A.E.D.val.p, A.E.D.val.n * 8, cudaMemcpyDeviceToDevice));
+    if (A.E.D.ntab) {  // the forward kernels read D through its table: scaled with it
+      GIPB_TRY(A.dtab0.alloc((size_t)A.E.D.ntab));
+      GIPB_CUDA(cudaMemcpy(A.dtab0.p, A.E.D.vtab.p, (size_t)A.E.D.ntab * 8,
+                           cudaMemcpyDeviceToDevice));
+    }
     GIPB_TRY(A.cval0.upload(ops->D.val, std::max(ops->D.nnz, 1)));
     GIPB_TRY(A.vol.upload(h_volume, N));
     GIPB_TRY(A.lid.upload(h_lid_cells, std::max(n_lid, 1)));
@@ -480,6 +486,11 @@ int gipb200_adjoint_forward(gipb200_adjoint H, const double* h_lid, double nu_sc
     GIPB_TRY(grid_blocks(256, (int)std::min<size_t>(A.dval0.n, 1u << 30), 4, 0, &b));
     k_scale_copy<<<b, 256, 0, s>>>((long long)A.dval0.n, A.dval0.p, nu_scale, A.E.D.val.p);
     GIPB_LAUNCH_CHECK();
+    // the same product of the same doubles: every slot's table value equals its scaled value
+    if (A.E.D.ntab) {
+      k_scale_copy<<<1, 256, 0, s>>>((long long)A.E.D.ntab, A.dtab0.p, nu_scale, A.E.D.vtab.p);
+      GIPB_LAUNCH_CHECK();
+    }
   }
   if (dt_given) {
     GIPB_TRY(A.E.dt_seq.upload(h_dt, nsteps));
