@@ -166,7 +166,6 @@ __global__ void k_dns_pcopy(int n_inner, int n_owned, double* __restrict__ p, do
 
 // ------------------------------------------------------------------ VelocityCorrection
 // gp = G p (x,y,z); u -= gp/(rho sigma) over the inner cells   -- GIP_DNS.h:359-370
-template <bool TAB>
 __global__ void __launch_bounds__(256) k_dns_gradcorr(SellView<double> Gx, SellView<double> Gy,
                                                       SellView<double> Gz, const double* __restrict__ p,
                                                       double* __restrict__ gpx, double* __restrict__ gpy,
@@ -184,7 +183,7 @@ __global__ void __launch_bounds__(256) k_dns_gradcorr(SellView<double> Gx, SellV
     const double* const X[3] = {p, p, p};
     double sm[3] = {0, 0, 0};
     bool an[3] = {false, false, false};
-    sell_rows3_f64<TAB>(G, X, s, lane, sm, an);
+    sell_rows3_f64(G, X, s, lane, sm, an);
     const double sx = sm[0], sy = sm[1], sz = sm[2];
     const bool ax = an[0], ay = an[1], az = an[2];
     if (ax && i < Gx.nrows) gpx[i] = sx;
@@ -297,7 +296,6 @@ __global__ void __launch_bounds__(256) k_dns_massflux3(
 // operator only (a structured grid's face is an x, y or z face): one gradient and one
 // velocity sum per face, so the kernel fits the registers of six blocks per SM.  The
 // updates keep their order: mf = fact1 SO p (a0), then fact2 SF_d gp_d, then rho SF_d u_d.
-template <bool TAB>
 __global__ void __launch_bounds__(256, 5) k_dns_massflux1(
     SellView<double> SO, SellView<double> SF, const unsigned short* __restrict__ cnt,
     const double* __restrict__ p, const double* __restrict__ gpx, const double* __restrict__ gpy,
@@ -337,9 +335,9 @@ __global__ void __launch_bounds__(256, 5) k_dns_massflux1(
       for (int t = 0; t < 2; ++t) {
         const int j = j0 + t;
         oc[t] = (j < ol) ? ld_stream(SO.col + ob + 32LL * j + lane) : -1;
-        ov[t] = (j < ol) ? sell_value<TAB>(SO, ob + 32LL * j + lane) : 0.0;
+        ov[t] = (j < ol) ? ld_stream(SO.val + ob + 32LL * j + lane) : 0.0;
         fc[t] = (j < fl) ? ld_stream(SF.col + fb + 32LL * j + lane) : -1;
-        fv[t] = (j < fl) ? sell_value<TAB>(SF, fb + 32LL * j + lane) : 0.0;
+        fv[t] = (j < fl) ? ld_stream(SF.val + fb + 32LL * j + lane) : 0.0;
       }
       double op[2], a[2], b[2];
 #pragma unroll
@@ -628,24 +626,14 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync, int part) {
     GIPB_TRY(launch_sell_spmv(Lb, Lb.val.p, p0.p, p.p, 1.0, 1.0, 1, s));
     mark(4);
     // VelocityCorrection
-    if (tab_g())
-      k_dns_gradcorr<true><<<grid.gradcorr, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p,
-                                                         gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, N,
-                                                         prm.rho, sc.p);
-    else
-      k_dns_gradcorr<false><<<grid.gradcorr, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p,
-                                                          gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, N,
-                                                          prm.rho, sc.p);
+    k_dns_gradcorr<<<grid.gradcorr, 256, 0, s>>>(Gx.view(), Gy.view(), Gz.view(), p.p, gpx.p,
+                                                 gpy.p, gpz.p, u.p, v.p, w.p, N, prm.rho, sc.p);
     mark(5);
     // MassFluxes
-    if (SF3.on && SF3.single && tab_f())
-      k_dns_massflux1<true><<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p,
-                                                          p.p, gpx.p, gpy.p, gpz.p, u.p, v.p,
-                                                          w.p, mf.p, prm.rho, sc.p);
-    else if (SF3.on && SF3.single)
-      k_dns_massflux1<false><<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p,
-                                                           p.p, gpx.p, gpy.p, gpz.p, u.p, v.p,
-                                                           w.p, mf.p, prm.rho, sc.p);
+    if (SF3.on && SF3.single)
+      k_dns_massflux1<<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p, p.p,
+                                                    gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p,
+                                                    prm.rho, sc.p);
     else if (SF3.on)
       k_dns_massflux3<<<grid.massflux, 256, 0, s>>>(SO.view(), SF3.S.view(), SF3.cnt.p, p.p,
                                                     gpx.p, gpy.p, gpz.p, u.p, v.p, w.p, mf.p,
@@ -829,8 +817,11 @@ static int check_op(const gipb200_host_csr& m, const char* name, int rows_max, i
 
 // The engine's sliced operators keep only what it reads: D its CSR columns and slot map
 // (C's values, the adjoint), L everything (the solver's set-up), the others nothing.
-// table: the phase kernels read the values through a value table where the operator's
-// values allow one (a uniform mesh's operators hold a handful of distinct values).
+// table: the phase kernel reads the values through a value table where the operator's
+// values allow one (a uniform mesh's operators hold a handful of distinct values).  Used
+// for D (C/D products), Mx/My/Mz (right-hand side) and Mres (massr), whose kernels gained
+// 115, 16 and 53 us on the 256^3 cavity; the correction (G) gained nothing and the mass
+// fluxes (SO, merged SF) lost 33 us to the dependent table read, so those read directly.
 static int build_op(Sell* S, const gipb200_host_csr& m, unsigned keep = 0, bool table = false) {
   GIPB_TRY(sell_build(S, m.nrows, m.ncols, m.nnz, m.rowptr, m.col, m.val, 0, keep));
   if (table) GIPB_TRY(sell_add_value_table(S, m.val, m.nnz, 0));
@@ -957,7 +948,6 @@ static int build_face3(FaceOps3* F, const gipb200_host_csr* const op[3], int NF,
     }
   }
   GIPB_TRY(sell_build(&F->S, NF, NO, (int)col.size(), rp.data(), col.data(), val.data(), 0, 0u));
-  GIPB_TRY(sell_add_value_table(&F->S, val.data(), (long long)val.size(), 0));
   GIPB_TRY(F->cnt.upload(cnt.data(), cnt.size(), 0));
   GIPB_CUDA(cudaStreamSynchronize(0));
   F->on = true;
@@ -1127,11 +1117,11 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     trace("sliced Mz");
     GIPB_TRY(build_op(&E.Mres, bops->Mres, 0, true));
     trace("sliced Mres");
-    GIPB_TRY(build_op(&E.Gx, bops->Gx, 0, true));
+    GIPB_TRY(build_op(&E.Gx, bops->Gx));
     trace("sliced Gx");
-    GIPB_TRY(build_op(&E.Gy, bops->Gy, 0, true));
+    GIPB_TRY(build_op(&E.Gy, bops->Gy));
     trace("sliced Gy");
-    GIPB_TRY(build_op(&E.Gz, bops->Gz, 0, true));
+    GIPB_TRY(build_op(&E.Gz, bops->Gz));
     trace("sliced Gz");
     {
       // SFx, SFy, SFz merged per face where they fit; their own layouts only otherwise
@@ -1148,7 +1138,7 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
       }
     }
     trace("face operators");
-    GIPB_TRY(build_op(&E.SO, bops->SO, 0, true));
+    GIPB_TRY(build_op(&E.SO, bops->SO));
     trace("sliced SO");
     GIPB_TRY(build_ec_slot(E, bops->D, bops->Ec));
     trace("Ec in C's slot order");
@@ -1186,11 +1176,9 @@ int dns_init(Dns& E, const gipb200_dns_ops* ops, const double* h_u, const double
     GIPB_TRY(one_wave(k_dns_ab2, E.blocks_vec, &E.grid.ab2));
     GIPB_TRY(E.tab_m() ? one_wave(k_dns_rhs<true>, E.blocks_cells, &E.grid.rhs)
                        : one_wave(k_dns_rhs<false>, E.blocks_cells, &E.grid.rhs));
-    GIPB_TRY(E.tab_g() ? one_wave(k_dns_gradcorr<true>, E.blocks_owned, &E.grid.gradcorr)
-                       : one_wave(k_dns_gradcorr<false>, E.blocks_owned, &E.grid.gradcorr));
+    GIPB_TRY(one_wave(k_dns_gradcorr, E.blocks_owned, &E.grid.gradcorr));
     if (E.SF3.on && E.SF3.single)
-      GIPB_TRY(E.tab_f() ? one_wave(k_dns_massflux1<true>, E.blocks_faces, &E.grid.massflux)
-                         : one_wave(k_dns_massflux1<false>, E.blocks_faces, &E.grid.massflux));
+      GIPB_TRY(one_wave(k_dns_massflux1, E.blocks_faces, &E.grid.massflux));
     else if (E.SF3.on)
       GIPB_TRY(one_wave(k_dns_massflux3, E.blocks_faces, &E.grid.massflux));
     else

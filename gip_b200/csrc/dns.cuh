@@ -61,11 +61,8 @@ struct Dns {
   // the phase kernels' operators all tabled (each kernel reads its operators one way)
   bool tab_d() const { return D.ntab > 0; }
   bool tab_m() const { return Mx.ntab > 0 && My.ntab > 0 && Mz.ntab > 0; }
-  bool tab_g() const { return Gx.ntab > 0 && Gy.ntab > 0 && Gz.ntab > 0; }
-  bool tab_f() const { return SO.ntab > 0 && SF3.S.ntab > 0; }
   int value_tables() const {
-    return (tab_d() ? 1 : 0) + (tab_m() ? 1 : 0) + (tab_g() ? 1 : 0) + (tab_f() ? 1 : 0) +
-           (Mres.ntab > 0 ? 1 : 0) + (ec_ntab > 0 ? 1 : 0);
+    return (tab_d() ? 1 : 0) + (tab_m() ? 1 : 0) + (Mres.ntab > 0 ? 1 : 0) + (ec_ntab > 0 ? 1 : 0);
   }
   DevBuf<double> cval;
   DevBuf<double> u, v, w, dxs, ax, ay, az, ax0, ay0, az0, rhs, p, p0, gpx, gpy, gpz, temp, mf;

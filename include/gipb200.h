@@ -364,8 +364,9 @@ typedef struct {
   double iteration_bytes;      /* algorithmic bytes of one PCG iteration (with V-cycle)   */
   double replacement_bytes;    /* MIXED: bytes of one FP64 residual replacement           */
   int packed_residual;         /* MIXED: FP64 residual from the packed columns (1) or L   */
-  int value_tables;            /* phase kernels (of 6: D/C, M, G, SO+SF, Mres, Ec) reading */
-                               /* their operators' values through 8-bit value tables      */
+  int value_tables;            /* phase kernels (of 4: D/C products, right-hand side,     */
+                               /* massr, C's values) reading their operators' values      */
+                               /* through 8-bit value tables                              */
 } gipb200_dns_info;
 int gipb200_dns_get_info(gipb200_dns E, gipb200_dns_info* info);
 

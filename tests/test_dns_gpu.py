@@ -228,7 +228,7 @@ def test_value_tables_are_exact(gpu, monkeypatch, mode):
     kw = dict(gamma=1.0 / 400, pcg_mode=mode, maxit=400 if mode == "fixed" else 3000, tol=1e-8,
               inner_tol=0.1, max_outer=100, reorder=True)
     E = DnsEngine(case, **kw)
-    assert E.info()["value_tables"] == 6
+    assert E.info()["value_tables"] == 4
     monkeypatch.setenv("GIPB200_NO_VALUE_TABLE", "1")
     P = DnsEngine(case, **kw)
     assert P.info()["value_tables"] == 0
