@@ -161,6 +161,8 @@ _SIGNATURES = {
     "gipb200_dns_setup_profile": (_I, [_VP, _VP]),
     "gipb200_dns_vcycle_profile": (_I, [_VP, _I, _VP, _I, C.POINTER(_I), _VP, _VP, _VP, _VP]),
     "gipb200_pcg_vcycle_profile": (_I, [_VP, _I, _VP, _I, C.POINTER(_I), _VP, _VP, _VP, _VP]),
+    "gipb200_dns_vcycle_forms": (_I, [_VP, _I, C.POINTER(_I), _VP]),
+    "gipb200_pcg_vcycle_forms": (_I, [_VP, _I, C.POINTER(_I), _VP]),
     "gipb200_dns_set_field": (_I, [_VP, C.c_char_p, _VP, _I, _I, _VP]),
     "gipb200_dns_launch_count": (_I, [_VP, C.POINTER(C.c_longlong)]),
     "gipb200_dns_kernel_time": (_I, [_VP, _I, _I, _VP, C.POINTER(_D), C.POINTER(_D)]),

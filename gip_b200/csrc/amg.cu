@@ -1450,10 +1450,11 @@ int AmgT<T>::reset_tail(cudaStream_t s) const {
   return GIPB200_OK;
 }
 
-int CycleTrace::mark(cudaStream_t s, int lvl, int knd, double by) {
+int CycleTrace::mark(cudaStream_t s, int lvl, int knd, double by, int frm) {
   GIPB_TRY(close(s));
   level.push_back(lvl);
   kind.push_back(knd);
+  form.push_back(frm);
   bytes.push_back(by);
   return GIPB200_OK;
 }
@@ -1478,8 +1479,8 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
   const int L = (int)lv.size();
   const double w = sizeof(T);
   // bytes of each kernel as cycle_bytes counts them (profiling marks only)
-  auto mark = [&](int l, int kind, double by) -> int {
-    return tr ? tr->mark(s, l, kind, by) : GIPB200_OK;
+  auto mark = [&](int l, int kind, double by, int form) -> int {
+    return tr ? tr->mark(s, l, kind, by, form) : GIPB200_OK;
   };
   auto a_bytes = [&](int l) { return l == 0 ? a0_stream_bytes : stream_bytes(lv[l]->A); };
   // downward: pre-smooth from zero, residual, restriction (levels below the coarse tail)
@@ -1493,11 +1494,13 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     // small levels >= 1 gather D^-1 b where they would gather the Jacobi start x = D^-1 b
     const bool fold = folds(l);
     if (!skip && !fold) {
-      GIPB_TRY(mark(l, GIPB200_CYCLE_JACOBI0, 3.0 * n * w));
+      GIPB_TRY(mark(l, GIPB200_CYCLE_JACOBI0, 3.0 * n * w, GIPB200_FORM_VECTOR));
       launch_dep(k_amg_jacobi0<T>, vec_blocks(V.n), 256, s, V.n, (const T*)V.dinv.p, b, V.x.p, S);
     }
-    GIPB_TRY(mark(l, GIPB200_CYCLE_RESIDUAL, a_bytes(l) + (skip ? 2.0 : 3.0) * n * w +
-                                                 (l == 0 && perm0.p ? 4.0 * n : 0.0)));
+    GIPB_TRY(mark(l, GIPB200_CYCLE_RESIDUAL,
+                  a_bytes(l) + (skip ? 2.0 : 3.0) * n * w + (l == 0 && perm0.p ? 4.0 * n : 0.0),
+                  l == 0 ? (packed ? GIPB200_FORM_PACKED : GIPB200_FORM_SLICED)
+                         : product_form(V.A)));
     if (l == 0) {
       const int bs = vec_blocks(A0.nslices * 32);
       if (packed)
@@ -1512,12 +1515,13 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     } else {  // t = b - A x
       amg_mv<T, kResid>(V.A, V.x.p, b, (const T*)nullptr, V.t.p, S, s);
     }
-    GIPB_TRY(mark(l, GIPB200_CYCLE_RESTRICT, stream_bytes(V.R) + (n + nn) * w));
+    GIPB_TRY(mark(l, GIPB200_CYCLE_RESTRICT, stream_bytes(V.R) + (n + nn) * w,
+                  product_form(V.R)));
     amg_mv<T, kPlain>(V.R, V.t.p, (const T*)nullptr, (const T*)nullptr, lv[l + 1]->b.p, S, s);
   }
   const AmgLevel<T>& C = *lv[L - 1];
   if (tf >= 0) {  // the small levels and the coarsest in one cooperative launch
-    GIPB_TRY(mark(tf, GIPB200_CYCLE_TAIL, tail_bytes));
+    GIPB_TRY(mark(tf, GIPB200_CYCLE_TAIL, tail_bytes, GIPB200_FORM_TAIL));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)tail_grid);
     cfg.blockDim = dim3(256);
@@ -1530,7 +1534,8 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     GIPB_CUDA(cudaLaunchKernelEx(&cfg, k_amg_tail, (const TailOp*)tail_ops.p, tail_nops,
                                  tail_bar.p, S));
   } else {
-    GIPB_TRY(mark(L - 1, GIPB200_CYCLE_DENSE, ((double)nc * nc + 2.0 * nc) * w));
+    GIPB_TRY(mark(L - 1, GIPB200_CYCLE_DENSE, ((double)nc * nc + 2.0 * nc) * w,
+                  GIPB200_FORM_DENSE));
     launch_dep(k_amg_dense<T>, std::min(kMaxReduceBlocks, (nc + 7) / 8), 256, s, nc,
                (const T*)cinv.p, (const T*)C.b.p, C.x.p, S);
   }
@@ -1541,15 +1546,17 @@ int AmgT<T>::enqueue(SellView<T> A0, const T* r, T* z0, PcgScalars* S, ReduceScr
     const double n = V.n, nn = lv[l + 1]->n;
     const bool skip = l == 0 && u0;
     const bool fold = folds(l);
-    GIPB_TRY(mark(l, GIPB200_CYCLE_PROLONG,
-                  stream_bytes(V.P) + (nn + (fold ? 3.0 : 2.0) * n) * w));
+    GIPB_TRY(mark(l, GIPB200_CYCLE_PROLONG, stream_bytes(V.P) + (nn + (fold ? 3.0 : 2.0) * n) * w,
+                  product_form(V.P)));
     if (skip)  // x0 = omega0 r + P x1
       amg_mv<T, kScaleAdd>(V.P, xc, r, (const T*)nullptr, V.x.p, S, s, (T)omega0);
     else if (fold)  // x = D^-1 b + P x_coarse
       amg_mv<T, kDiagAdd>(V.P, xc, V.b.p, V.dinv.p, V.x.p, S, s);
     else
       amg_mv<T, kAdd>(V.P, xc, (const T*)nullptr, (const T*)nullptr, V.x.p, S, s);
-    GIPB_TRY(mark(l, GIPB200_CYCLE_SMOOTH, a_bytes(l) + (skip ? 3.0 : 4.0) * n * w));
+    GIPB_TRY(mark(l, GIPB200_CYCLE_SMOOTH, a_bytes(l) + (skip ? 3.0 : 4.0) * n * w,
+                  l == 0 ? (packed ? GIPB200_FORM_PACKED : GIPB200_FORM_SMOOTH_DOT)
+                         : product_form(V.A)));
     if (l == 0) {
       const int bs = vec_blocks(A0.nslices * 32);
       if (packed)

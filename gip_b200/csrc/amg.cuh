@@ -85,10 +85,10 @@ struct PackedView {
 // (GIPB200_CYCLE_*) and its algorithmic bytes.
 struct CycleTrace {
   std::vector<cudaEvent_t> ev;
-  std::vector<int> level, kind;
+  std::vector<int> level, kind, form;
   std::vector<double> bytes;
   bool captured = false;  // record into a graph being captured (external event nodes)
-  int mark(cudaStream_t s, int lvl, int knd, double by);  // before a kernel
+  int mark(cudaStream_t s, int lvl, int knd, double by, int frm);  // before a kernel
   int close(cudaStream_t s);                              // after the last one
   ~CycleTrace();
 };
@@ -157,6 +157,13 @@ struct AmgT {
 };
 
 // Stored bytes one product streams from an AMG operator.
+// The kernel form of a product with operator M (GIPB200_FORM_*).
+template <typename T>
+int product_form(const SellT<T>& M) {
+  if (M.lanes > 0) return GIPB200_FORM_CSR;
+  return (M.pipe && !M.short_cols) ? GIPB200_FORM_PIPELINED : GIPB200_FORM_SLICED;
+}
+
 template <typename T>
 double stream_bytes(const SellT<T>& M) {
   const double w = M.half ? 2.0 : (double)sizeof(T);

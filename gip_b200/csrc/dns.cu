@@ -1532,6 +1532,11 @@ int gipb200_dns_vcycle_profile(gipb200_dns Dh, int reps, void* stream, int cap, 
                                   h_bytes);
 }
 
+int gipb200_dns_vcycle_forms(gipb200_dns Dh, int cap, int* n_kernels, int* h_form) {
+  if (!Dh) return fail(GIPB200_ERR_ARG, "null engine");
+  return Dh->E.pcg.vcycle_forms(cap, n_kernels, h_form);
+}
+
 int gipb200_dns_set_time(gipb200_dns Dh, double time, void* stream) {
   if (!Dh) return fail(GIPB200_ERR_ARG, "null engine");
   if (!std::isfinite(time)) return fail(GIPB200_ERR_ARG, "time must be finite");

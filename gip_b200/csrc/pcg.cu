@@ -1770,6 +1770,7 @@ int Pcg::profile_vcycle(int reps, cudaStream_t s, int cap, int* n_kernels, int* 
   }
   cudaGraphExecDestroy(ex);
   GIPB_TRY(st);
+  cycle_forms = tr.form;
   *n_kernels = nk;
   for (int j = 0; j < std::min(nk, cap); ++j) {
     if (level) level[j] = tr.level[j];
@@ -1777,6 +1778,14 @@ int Pcg::profile_vcycle(int reps, cudaStream_t s, int cap, int* n_kernels, int* 
     if (bytes) bytes[j] = tr.bytes[j];
     if (ms) ms[j] = sum[j] / reps;
   }
+  return GIPB200_OK;
+}
+
+int Pcg::vcycle_forms(int cap, int* n_kernels, int* h_form) const {
+  if (cap < 0 || !n_kernels || (cap > 0 && !h_form)) return fail(GIPB200_ERR_ARG, "bad arguments");
+  if (cycle_forms.empty()) return fail(GIPB200_ERR_STATE, "no V-cycle has been profiled");
+  *n_kernels = (int)cycle_forms.size();
+  for (int k = 0; k < std::min(cap, (int)cycle_forms.size()); ++k) h_form[k] = cycle_forms[(size_t)k];
   return GIPB200_OK;
 }
 
@@ -1858,6 +1867,11 @@ int gipb200_pcg_vcycle_profile(gipb200_pcg S, int reps, void* stream, int cap, i
   if (!S) return fail(GIPB200_ERR_ARG, "null solver");
   return S->P.profile_vcycle(reps, as_stream(stream), cap, n_kernels, h_level, h_kind, h_ms,
                              h_bytes);
+}
+
+int gipb200_pcg_vcycle_forms(gipb200_pcg S, int cap, int* n_kernels, int* h_form) {
+  if (!S) return fail(GIPB200_ERR_ARG, "null solver");
+  return S->P.vcycle_forms(cap, n_kernels, h_form);
 }
 
 int gipb200_pcg_solve(gipb200_pcg S, const double* b, double* x, const double* x0, void* stream,

@@ -148,6 +148,8 @@ struct Pcg {
   // Per-kernel profile of `reps` V-cycles on the current residual (scratch scalars).
   int profile_vcycle(int reps, cudaStream_t s, int cap, int* n_kernels, int* level, int* kind,
                      double* ms, double* bytes);
+  std::vector<int> cycle_forms;  // kernel forms of the last profiled cycle (GIPB200_FORM_*)
+  int vcycle_forms(int cap, int* n_kernels, int* h_form) const;
 
  private:
   int enqueue_fp64(const double* b, double* x, const double* x0, cudaStream_t s, bool host_sync);

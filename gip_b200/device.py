@@ -178,6 +178,9 @@ def pcg_params(mode: str = "fixed", maxit: int = 100, tol: float = 1e-6,
 
 
 CYCLE_KINDS = ("jacobi0", "residual", "restrict", "dense", "prolong", "smooth", "tail")
+# the kernel each product form runs as (GIPB200_FORM_*)
+FORM_KERNELS = ("k_amgp_spmv", "k_amg_spmv", "k_amg_spmv_pf", "k_amg_csr", "k_amg_dense",
+                "k_amg_jacobi0", "k_amg_tail", "k_amg_smooth_dot")
 
 
 def _vcycle_profile(fn: str, handle, reps: int, stream) -> list:
@@ -189,8 +192,12 @@ def _vcycle_profile(fn: str, handle, reps: int, stream) -> list:
     by = np.zeros(cap)
     L.call(fn, handle, reps, _stream(stream), cap, C.byref(nk), _hptr(lvl), _hptr(kind),
            _hptr(ms), _hptr(by))
+    form = np.zeros(cap, np.int32)
+    nf = C.c_int()
+    L.call(fn.replace("_profile", "_forms"), handle, cap, C.byref(nf), _hptr(form))
     return [{"level": int(lvl[k]), "kind": CYCLE_KINDS[kind[k]], "ms": float(ms[k]),
-             "bytes": float(by[k])} for k in range(min(nk.value, cap))]
+             "bytes": float(by[k]), "kernel": FORM_KERNELS[form[k]]}
+            for k in range(min(nk.value, cap))]
 
 
 class PcgSolver:

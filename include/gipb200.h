@@ -236,6 +236,20 @@ enum {
 };
 int gipb200_pcg_vcycle_profile(gipb200_pcg S, int reps, void* stream, int cap, int* n_kernels,
                                int* h_level, int* h_kind, double* h_ms, double* h_bytes);
+/* The form each kernel of the last profiled cycle ran its product in (GIPB200_FORM_*), in
+ * the same order; at most `cap` written, *n_kernels = kernels per cycle.
+ * GIPB200_ERR_STATE before a profile. */
+enum {
+  GIPB200_FORM_PACKED = 0,     /* level 0 from the packed FP32 operator (k_amgp_spmv)     */
+  GIPB200_FORM_SLICED = 1,     /* sliced, a lane per row (k_amg_spmv)                     */
+  GIPB200_FORM_PIPELINED = 2,  /* sliced, software-pipelined (k_amg_spmv_pf)              */
+  GIPB200_FORM_CSR = 3,        /* CSR, several lanes per row (k_amg_csr)                  */
+  GIPB200_FORM_DENSE = 4,      /* dense inverse of the coarsest level (k_amg_dense)       */
+  GIPB200_FORM_VECTOR = 5,     /* element-wise (k_amg_jacobi0)                            */
+  GIPB200_FORM_TAIL = 6,       /* the coarse tail in one launch (k_amg_tail)              */
+  GIPB200_FORM_SMOOTH_DOT = 7  /* level-0 smoothing with r.z, plain layout                */
+};
+int gipb200_pcg_vcycle_forms(gipb200_pcg S, int cap, int* n_kernels, int* h_form);
 
 /* No counterpart in the reference.  A Jacobi-PCG solve for callers that cannot allocate
  * device memory at solve time (a framework-owned arena or caching allocator, code that
@@ -393,6 +407,8 @@ int gipb200_dns_setup_profile(gipb200_dns E, double* h_seconds);
 /* gipb200_pcg_vcycle_profile for the engine's pressure solver (precond = AMG). */
 int gipb200_dns_vcycle_profile(gipb200_dns E, int reps, void* stream, int cap, int* n_kernels,
                                int* h_level, int* h_kind, double* h_ms, double* h_bytes);
+/* gipb200_pcg_vcycle_forms for the engine's pressure solver. */
+int gipb200_dns_vcycle_forms(gipb200_dns E, int cap, int* n_kernels, int* h_form);
 
 /* Number of this library's kernels the engine has launched so far (a graph launch counts
  * the kernels it holds). */

@@ -275,6 +275,10 @@ def test_amg_coarse_tail_is_exact(gpu, monkeypatch):
         assert res["status"] == 0, (tail, res)
         prof = S.vcycle_profile(reps=2)
         out[tail] = (x.cpu().numpy(), res["iterations"], [c["kind"] for c in prof])
+        # each kernel names the form it ran in: the tail launch, the packed level 0
+        kern = [c["kernel"] for c in prof]
+        assert ("k_amg_tail" in kern) == tail, kern
+        assert prof[0]["kernel"] == "k_amgp_spmv" and prof[-1]["kernel"] == "k_amgp_spmv", kern
     assert "tail" in out[True][2] and "tail" not in out[False][2]
     assert out[True][1] == out[False][1]
     assert np.array_equal(out[True][0], out[False][0])
