@@ -180,6 +180,7 @@ struct Adjoint {
     DevBuf<double> u, v, w, mf, ax0, ay0, az0, p0;
   };
   std::vector<Ckpt*> ckpts;
+  DevBuf<double> lid_dev;                     // the lid values of the current forward
   DevBuf<double> seg_u, seg_mf;               // per-step u,v,w (3*NO) and mf (NF)
   int seg_cap = 0;
   // adjoint vectors
@@ -201,6 +202,15 @@ struct Adjoint {
 
 static int blocks_for(int n, int* b) { return grid_blocks(256, std::max(n, 1), 4, kMaxReduceBlocks, b); }
 
+// The engine's prescribed dt sequence: copied into its buffer, which grows only when a run
+// is longer than any before (no allocation per forward or backward call).
+static int put_dt_seq(Dns& E, const double* h, int n) {
+  if (!E.dt_seq.p || E.dt_seq.n < (size_t)n) GIPB_TRY(E.dt_seq.alloc((size_t)n));
+  GIPB_CUDA(cudaMemcpy(E.dt_seq.p, h, (size_t)n * 8, cudaMemcpyHostToDevice));
+  E.dt_seq_len = n;
+  return GIPB200_OK;
+}
+
 int Adjoint::reset_state(cudaStream_t s) {
   // the engine restarts from the initial fields with the lid values applied
   std::vector<double> uu(u0);
@@ -208,11 +218,12 @@ int Adjoint::reset_state(cudaStream_t s) {
   GIPB_CUDA(cudaMemcpyAsync(E.v.p, v0.data(), (size_t)NO * 8, cudaMemcpyHostToDevice, s));
   GIPB_CUDA(cudaMemcpyAsync(E.w.p, w0.data(), (size_t)NO * 8, cudaMemcpyHostToDevice, s));
   if (n_lid) {
-    DevBuf<double> lv;
-    GIPB_TRY(lv.upload(lid_vals.data(), n_lid, s));
+    if (!lid_dev.p) GIPB_TRY(lid_dev.alloc((size_t)n_lid));
+    GIPB_CUDA(cudaMemcpyAsync(lid_dev.p, lid_vals.data(), (size_t)n_lid * 8,
+                              cudaMemcpyHostToDevice, s));
     int b;
     GIPB_TRY(blocks_for(n_lid, &b));
-    k_scatter_idx<<<b, 256, 0, s>>>(n_lid, lid.p, lv.p, E.u.p);
+    k_scatter_idx<<<b, 256, 0, s>>>(n_lid, lid.p, lid_dev.p, E.u.p);
     GIPB_LAUNCH_CHECK();
     GIPB_CUDA(cudaStreamSynchronize(s));
   }
@@ -493,11 +504,9 @@ int gipb200_adjoint_forward(gipb200_adjoint H, const double* h_lid, double nu_sc
     }
   }
   if (dt_given) {
-    GIPB_TRY(A.E.dt_seq.upload(h_dt, nsteps));
-    A.E.dt_seq_len = nsteps;
+    GIPB_TRY(put_dt_seq(A.E, h_dt, nsteps));
   } else {
-    A.E.dt_seq.release();
-    A.E.dt_seq_len = 0;
+    A.E.dt_seq_len = 0;  // dt from the CFL condition (the buffer is kept for the backward)
   }
   // a new dt source changes the captured step: capture again
   if (A.E.exec) {
@@ -509,13 +518,18 @@ int gipb200_adjoint_forward(gipb200_adjoint H, const double* h_lid, double nu_sc
     A.E.graph = nullptr;
   }
   GIPB_TRY(A.reset_state(s));
-  for (auto* c : A.ckpts) delete c;
-  A.ckpts.clear();
+  // the checkpoints are kept from call to call (their device buffers are reused: a forward
+  // allocates only when it needs more segments than the last one)
   const int K = A.prm.checkpoint_every;
-  for (int n0 = 0; n0 < nsteps; n0 += K) {
-    Adjoint::Ckpt* c = new Adjoint::Ckpt();
+  const int nck = (nsteps + K - 1) / K;
+  while ((int)A.ckpts.size() > nck) {
+    delete A.ckpts.back();
+    A.ckpts.pop_back();
+  }
+  while ((int)A.ckpts.size() < nck) A.ckpts.push_back(new Adjoint::Ckpt());
+  for (int n0 = 0, ci = 0; n0 < nsteps; n0 += K, ++ci) {
+    Adjoint::Ckpt* c = A.ckpts[(size_t)ci];
     c->step = n0;
-    A.ckpts.push_back(c);
     if (n0 == 0) {
       // the first step's dt comes from the initial CFL (or the prescribed list)
       GIPB_TRY(A.E.grow_history(nsteps, s));
@@ -558,8 +572,7 @@ int gipb200_adjoint_backward(gipb200_adjoint H, double* h_grad_lid, double* h_gr
     A.seg_cap = K;
   }
   // the backward replays each segment with the recorded steps
-  GIPB_TRY(A.E.dt_seq.upload(A.dts.data(), A.nsteps));
-  A.E.dt_seq_len = A.nsteps;
+  GIPB_TRY(put_dt_seq(A.E, A.dts.data(), A.nsteps));
   if (A.E.exec) {
     cudaGraphExecDestroy(A.E.exec);
     A.E.exec = nullptr;

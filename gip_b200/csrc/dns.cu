@@ -601,7 +601,8 @@ int Dns::grow_history(int need, cudaStream_t s) {
 
 int Dns::enqueue_initial_dt(cudaStream_t s) {
   k_dns_cfl<<<grid.cfl, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p,
-                                        history(), pcg.sc.p, 0, 0, dt_seq.p, dt_seq_len, rs);
+                                        history(), pcg.sc.p, 0, 0,
+                                        dt_seq_len > 0 ? dt_seq.p : nullptr, dt_seq_len, rs);
   GIPB_LAUNCH_CHECK();
   launches += 1;
   return GIPB200_OK;
@@ -677,7 +678,7 @@ int Dns::enqueue_step(cudaStream_t s, bool host_sync, int part) {
       k_dns_massr<false><<<grid.massr, 256, 0, s>>>(Mres.view(), mf.p, temp.p, N, sc.p, H, rs);
     k_dns_cfl<<<grid.cfl, 256, 0, s>>>(N, u.p, v.p, w.p, dxs.p, prm.gamma, prm.rho, sc.p, H,
                                           pcg.sc.p, 1, prm.pcg.mode == GIPB200_PCG_MIXED,
-                                          dt_seq.p, dt_seq_len, rs);
+                                          dt_seq_len > 0 ? dt_seq.p : nullptr, dt_seq_len, rs);
     GIPB_LAUNCH_CHECK();
     mark(7);
   }
