@@ -70,3 +70,28 @@ def test_peaks_and_traffic_helpers(tmp_path, monkeypatch):
     monkeypatch.setattr(bench, "REPO", str(tmp_path))
     assert bench.peaks() == {"hbm_gbs": 6650.0, "source": "fallback"}
     assert bench.ncu_traffic("k_mxp_spmv_dot", 1000) is None
+
+
+def test_other_configs_record_errors_and_keep_the_line(monkeypatch):
+    """A configuration that fails records its error under other_configs; the others still
+    run and the cavity line is still printed (each entry also carries its wall time)."""
+    import argparse
+
+    sys.path.insert(0, REPO)
+    import torch
+
+    import bench
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda: None)
+
+    def boom(*a, **k):
+        raise RuntimeError("no device")
+
+    monkeypatch.setattr(bench, "poisson_results", boom)
+    monkeypatch.setattr(bench, "adjoint_results",
+                        lambda a, n, nd: {"results": {"n": n, "dirs": nd}})
+    monkeypatch.setattr(bench, "batch_results", lambda a, full: {"results": {"full": full}})
+    out = bench.other_configs(argparse.Namespace())
+    assert out["poisson_128"]["error"] == "RuntimeError: no device"
+    assert out["adjoint_64"]["results"] == {"n": 64, "dirs": 4}
+    assert out["batch_32"]["results"] == {"full": False}
+    assert all("wall_s" in v for v in out.values())
